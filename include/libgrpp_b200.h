@@ -1,0 +1,107 @@
+/*
+ * Batched C-ABI of the B200 GRPP integral engine.
+ *
+ * libgrpp (aoleynichenko/libgrpp) evaluates one shell pair x one potential
+ * centre per call (libgrpp/libgrpp.h:123-231) and leaves parallelism to the
+ * caller (test_libgrpp_c/eval_integrals.c:78-83). This header adds batched
+ * entry points with no counterpart in libgrpp: a whole list of
+ * (shell A, shell B, centre C) tasks is described once in flat arrays
+ * (plain pointers and sizes, host memory) and evaluated on the GPU in one
+ * call. The single-task libgrpp_* functions of libgrpp.h are implemented on
+ * top of these with a batch of one.
+ *
+ * Task semantics are those of libgrpp_full_grpp_integrals
+ * (libgrpp/full_grpp_integrals.c:27-104): for task t the four output blocks
+ * hold arep, so_x, so_y, so_z of <A| U_GRPP(C) |B>, row-major
+ * cart_size(A) x cart_size(B), stored consecutively in task order:
+ * block t starts at sum_{s<t} cart_size(A_s) * cart_size(B_s).
+ */
+#ifndef LIBGRPP_B200_BATCH_H
+#define LIBGRPP_B200_BATCH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    /* ---- shells: basis shells and outercore shells share one table ----
+     * coefficients are the raw contraction coefficients a caller passes to
+     * libgrpp_new_shell (no normalisation folded in). */
+    int n_shells;
+    const int *shell_L;          /* [n_shells] */
+    const int *shell_nprim;      /* [n_shells] */
+    const int *shell_prim_off;   /* [n_shells] offset into prim_coef / prim_alpha */
+    const double *prim_coef;
+    const double *prim_alpha;
+    const double *shell_origin;  /* [3*n_shells]; ignored for outercore shells */
+    const int *shell_cart_off;   /* [n_shells] offset (in components) into cart_list */
+    const int *cart_list;        /* 3 ints (x,y,z powers) per Cartesian component */
+
+    /* ---- potentials sum_k c_k r^(n_k-2) exp(-zeta_k r^2) ---- */
+    int n_pots;
+    const int *pot_L;
+    const int *pot_J;            /* 2j for outercore potentials, 0 otherwise */
+    const int *pot_nprim;
+    const int *pot_prim_off;
+    const int *pot_powers;       /* n_k in {0,1,2} */
+    const double *pot_coef;
+    const double *pot_alpha;
+
+    /* ---- GRPP operators (one per element) ---- */
+    int n_grpps;
+    const int *grpp_UL;          /* [n_grpps] potential index of U_L, -1 if none */
+    const int *grpp_arep_off;    /* into grpp_pot_list */
+    const int *grpp_n_arep;
+    const int *grpp_so_off;      /* into grpp_pot_list */
+    const int *grpp_n_so;
+    const int *grpp_oc_off;      /* into grpp_oc_pot / grpp_oc_shell */
+    const int *grpp_n_oc;
+    const int *grpp_pot_list;
+    const int *grpp_oc_pot;
+    const int *grpp_oc_shell;
+
+    /* ---- potential centres ---- */
+    int n_centres;
+    const double *centre_origin; /* [3*n_centres] */
+    const int *centre_grpp;      /* [n_centres] */
+
+    /* ---- tasks ---- */
+    int64_t n_tasks;
+    const int *task_a;           /* bra shell */
+    const int *task_b;           /* ket shell */
+    const int *task_c;           /* centre */
+} libgrpp_b200_batch_t;
+
+/* status codes */
+enum {
+    LIBGRPP_B200_OK = 0,
+    LIBGRPP_B200_ERR_INVALID = 1,    /* input outside the supported limits */
+    LIBGRPP_B200_ERR_CUDA = 2,       /* a CUDA runtime call failed */
+    LIBGRPP_B200_ERR_TIMEOUT = 3,    /* a bounded device-side wait gave up */
+    LIBGRPP_B200_ERR_NOT_INIT = 4    /* libgrpp_init() was not called */
+};
+
+/* radial quadrature modes */
+enum {
+    LIBGRPP_B200_RADIAL_PLAIN = 0,   /* level-by-level nested Log3 doubling */
+    LIBGRPP_B200_RADIAL_LEARNED = 1  /* MLP-predicted level + one check level, plain fallback */
+};
+
+/* last error of the calling thread: code and message */
+int libgrpp_b200_last_error(void);
+const char *libgrpp_b200_last_error_message(void);
+
+/* total number of doubles of one output array for this batch */
+int64_t libgrpp_b200_batch_output_size(const libgrpp_b200_batch_t *batch);
+
+/* Full GRPP integrals for every task (host in, host out). Returns a status code. */
+int libgrpp_b200_full_grpp_batch(const libgrpp_b200_batch_t *batch, int radial_mode, double *arep,
+                                 double *so_x, double *so_y, double *so_z);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LIBGRPP_B200_BATCH_H */

@@ -1,0 +1,213 @@
+"""ctypes binding of the libgrpp C API.
+
+One binding serves every library that exports libgrpp's C interface
+(libgrpp/libgrpp.h:33-231): the CUDA engine ``libgrpp_b200/libgrpp_b200.so``,
+and, for tests only, the CPU oracle and the compiled reference. Objects are
+built through the library's own constructors, exactly as a C caller would.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+
+from .system import GRPP, Potential, Shell, ncart
+
+_D = ct.POINTER(ct.c_double)
+_I = ct.POINTER(ct.c_int)
+_V = ct.c_void_p
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PRODUCT_LIB = os.path.join(ROOT, "libgrpp_b200", "libgrpp_b200.so")
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_I)
+
+
+class LibGRPP:
+    """A loaded library exporting the libgrpp C API."""
+
+    def __init__(self, path: str):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built")
+        self.path = path
+        self.lib = ct.CDLL(path, mode=getattr(os, "RTLD_LOCAL", 0) | getattr(os, "RTLD_NOW", 2))
+        L = self.lib
+        proto = {
+            "libgrpp_init": (None, []),
+            "libgrpp_finalize": (None, []),
+            "libgrpp_is_initialized": (ct.c_int, []),
+            "libgrpp_set_cartesian_order": (None, [ct.c_int]),
+            "libgrpp_new_shell": (_V, [_D, ct.c_int, ct.c_int, _D, _D]),
+            "libgrpp_delete_shell": (None, [_V]),
+            "libgrpp_get_shell_size": (ct.c_int, [_V]),
+            "libgrpp_new_potential": (_V, [ct.c_int, ct.c_int, ct.c_int, _I, _D, _D]),
+            "libgrpp_delete_potential": (None, [_V]),
+            "libgrpp_potential_value": (ct.c_double, [_V, ct.c_double]),
+            "libgrpp_new_grpp": (_V, []),
+            "libgrpp_grpp_set_local_potential": (None, [_V, _V]),
+            "libgrpp_grpp_add_averaged_potential": (None, [_V, _V]),
+            "libgrpp_grpp_add_spin_orbit_potential": (None, [_V, _V]),
+            "libgrpp_grpp_add_outercore_potential": (None, [_V, _V, _V]),
+            "libgrpp_delete_grpp": (None, [_V]),
+            "libgrpp_type1_integrals": (None, [_V, _V, _D, _V, _D]),
+            "libgrpp_type2_integrals": (None, [_V, _V, _D, _V, _D]),
+            "libgrpp_spin_orbit_integrals": (None, [_V, _V, _D, _V, _D, _D, _D]),
+            "libgrpp_outercore_potential_integrals": (None, [_V, _V, _D, ct.c_int, ct.POINTER(_V), ct.POINTER(_V), _D, _D, _D, _D]),
+            "libgrpp_full_grpp_integrals": (None, [_V, _V, _V, _D, _D, _D, _D, _D]),
+            "libgrpp_full_grpp_integrals_gradient": (None, [_V, _V, _V, _D, _D, ct.POINTER(_D), ct.POINTER(_D), ct.POINTER(_D), ct.POINTER(_D)]),
+            "libgrpp_type1_integrals_gradient": (None, [_V, _V, _D, _V, _D, ct.POINTER(_D)]),
+            "libgrpp_type2_integrals_gradient": (None, [_V, _V, _D, _V, _D, ct.POINTER(_D)]),
+            "libgrpp_spin_orbit_integrals_gradient": (None, [_V, _V, _D, _V, _D, ct.POINTER(_D), ct.POINTER(_D), ct.POINTER(_D)]),
+        }
+        for name, (res, args) in proto.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        self._opt("grpp_driver_full_batch", ct.c_int, [_V, ct.c_int64, ct.c_int64, ct.c_int, _D, _D, _D, _D])
+        self._opt("grpp_driver_term", ct.c_int, [_V, ct.c_int64, ct.c_int, ct.c_int, _D, _D, _D])
+        self._opt("grpp_driver_grad_contract", ct.c_int, [_V, ct.c_int64, ct.c_int64, ct.c_int, _I, _I, _D, ct.c_int, _I, ct.c_int, _D, _D])
+        self._opt("grpp_driver_num_threads", ct.c_int, [])
+        self._opt("libgrpp_b200_last_error", ct.c_int, [])
+        self._opt("libgrpp_b200_last_error_message", ct.c_char_p, [])
+        self._opt("libgrpp_b200_full_grpp_batch", ct.c_int, [_V, ct.c_int, _D, _D, _D, _D])
+        self.lib.libgrpp_init()
+
+    def _opt(self, name, res, args):
+        f = getattr(self.lib, name, None)
+        if f is not None:
+            f.restype = res
+            f.argtypes = args
+
+    def has(self, name: str) -> bool:
+        return getattr(self.lib, name, None) is not None
+
+    # ------------------------------------------------------------ objects
+    def set_cartesian_order(self, order: int):
+        self.lib.libgrpp_set_cartesian_order(order)
+
+    def new_shell(self, s: Shell) -> int:
+        o = np.ascontiguousarray(s.origin, dtype=np.float64)
+        c = np.ascontiguousarray(s.coeffs, dtype=np.float64)
+        a = np.ascontiguousarray(s.alpha, dtype=np.float64)
+        return self.lib.libgrpp_new_shell(_dp(o), int(s.L), len(a), _dp(c), _dp(a))
+
+    def new_potential(self, p: Potential) -> int:
+        pw = np.ascontiguousarray(p.powers, dtype=np.int32)
+        c = np.ascontiguousarray(p.coeffs, dtype=np.float64)
+        a = np.ascontiguousarray(p.alpha, dtype=np.float64)
+        return self.lib.libgrpp_new_potential(int(p.L), int(p.J), len(a), _ip(pw), _dp(c), _dp(a))
+
+    def new_grpp(self, g: GRPP) -> int:
+        h = self.lib.libgrpp_new_grpp()
+        if g.UL is not None:
+            self.lib.libgrpp_grpp_set_local_potential(h, self.new_potential(g.UL))
+        for p in g.arep:
+            self.lib.libgrpp_grpp_add_averaged_potential(h, self.new_potential(p))
+        for p in g.so:
+            self.lib.libgrpp_grpp_add_spin_orbit_potential(h, self.new_potential(p))
+        for p, s in g.oc:
+            self.lib.libgrpp_grpp_add_outercore_potential(h, self.new_potential(p), self.new_shell(s))
+        return h
+
+    # ------------------------------------------------------------ integrators
+    def type1(self, hA, hB, C, hpot, nA, nB):
+        out = np.zeros(nA * nB)
+        self.lib.libgrpp_type1_integrals(hA, hB, _dp(np.ascontiguousarray(C, dtype=np.float64)), hpot, _dp(out))
+        return out.reshape(nA, nB)
+
+    def type2(self, hA, hB, C, hpot, nA, nB):
+        out = np.zeros(nA * nB)
+        self.lib.libgrpp_type2_integrals(hA, hB, _dp(np.ascontiguousarray(C, dtype=np.float64)), hpot, _dp(out))
+        return out.reshape(nA, nB)
+
+    def spin_orbit(self, hA, hB, C, hpot, nA, nB):
+        o = [np.zeros(nA * nB) for _ in range(3)]
+        self.lib.libgrpp_spin_orbit_integrals(hA, hB, _dp(np.ascontiguousarray(C, dtype=np.float64)), hpot,
+                                              _dp(o[0]), _dp(o[1]), _dp(o[2]))
+        return [x.reshape(nA, nB) for x in o]
+
+    def full(self, hA, hB, hg, C, nA, nB):
+        o = [np.zeros(nA * nB) for _ in range(4)]
+        self.lib.libgrpp_full_grpp_integrals(hA, hB, hg, _dp(np.ascontiguousarray(C, dtype=np.float64)),
+                                             *[_dp(x) for x in o])
+        return [x.reshape(nA, nB) for x in o]
+
+    def full_gradient(self, hA, hB, hg, C, D, nA, nB):
+        g = np.zeros((4, 3, nA * nB))
+        ptrs = [(_D * 3)(*[g[m, k].ctypes.data_as(_D) for k in range(3)]) for m in range(4)]
+        self.lib.libgrpp_full_grpp_integrals_gradient(
+            hA, hB, hg, _dp(np.ascontiguousarray(C, dtype=np.float64)), _dp(np.ascontiguousarray(D, dtype=np.float64)),
+            *ptrs)
+        return g.reshape(4, 3, nA, nB)
+
+    # ------------------------------------------------------------ batched (CPU drivers)
+    def driver_full_batch(self, batch, t0=0, t1=None, nthreads=1):
+        if t1 is None:
+            t1 = len(batch.task_a)
+        off = batch.block_offsets()
+        n = int(off[t1] - off[t0])
+        outs = [np.zeros(max(n, 1)) for _ in range(4)]
+        self.lib.grpp_driver_full_batch(ct.byref(batch.struct), t0, t1, nthreads, *[_dp(x) for x in outs])
+        return [x[:n] for x in outs]
+
+    def driver_grad_contract(self, system, batch, D, t0=0, t1=None, nthreads=1):
+        if t1 is None:
+            t1 = len(batch.task_a)
+        nat = len(system.atoms)
+        g = np.zeros((4, nat, 3))
+        sa = np.ascontiguousarray(system.shell_atom, dtype=np.int32)
+        ca = np.ascontiguousarray(system.centre_atom, dtype=np.int32)
+        xyz = np.ascontiguousarray(system.atoms, dtype=np.float64)
+        bo = np.ascontiguousarray(system.basis_offsets()[:-1], dtype=np.int32)
+        Dm = np.ascontiguousarray(D, dtype=np.float64)
+        self.lib.grpp_driver_grad_contract(ct.byref(batch.struct), t0, t1, nthreads, _ip(sa), _ip(ca), _dp(xyz), nat,
+                                           _ip(bo), int(Dm.shape[0]), _dp(Dm), _dp(g))
+        return g
+
+    def num_threads(self) -> int:
+        return int(self.lib.grpp_driver_num_threads())
+
+    # ------------------------------------------------------------ batched (GPU engine)
+    def full_grpp_batch(self, batch, radial_mode=0):
+        n = int(batch.block_offsets()[-1])
+        outs = [np.zeros(max(n, 1)) for _ in range(4)]
+        rc = self.lib.libgrpp_b200_full_grpp_batch(ct.byref(batch.struct), radial_mode, *[_dp(x) for x in outs])
+        if rc != 0:
+            raise RuntimeError(f"libgrpp_b200_full_grpp_batch failed ({rc}): {self.last_error_message()}")
+        return [x[:n] for x in outs]
+
+    def last_error(self) -> int:
+        return int(self.lib.libgrpp_b200_last_error())
+
+    def last_error_message(self) -> str:
+        m = self.lib.libgrpp_b200_last_error_message()
+        return m.decode() if m else ""
+
+
+def shells_handles(lib: LibGRPP, system):
+    return [lib.new_shell(s) for s in system.shells]
+
+
+def dense_full(lib: LibGRPP, system, threads=None):
+    """Dense (arep, so_x, so_y, so_z) matrices of a system through the single-task
+    API, serially in the C driver's order (test_libgrpp_c/eval_integrals.c:78-123)."""
+    lib.set_cartesian_order(system.cart_order)
+    hs = shells_handles(lib, system)
+    hg = [lib.new_grpp(g) for g in system.grpps]
+    off = system.basis_offsets()
+    n = int(off[-1])
+    M = np.zeros((4, n, n))
+    for i, si in enumerate(system.shells):
+        for j, sj in enumerate(system.shells):
+            for C, gi in system.centres:
+                blocks = lib.full(hs[i], hs[j], hg[gi], C, ncart(si.L), ncart(sj.L))
+                for m in range(4):
+                    M[m, off[i]:off[i + 1], off[j]:off[j + 1]] += blocks[m]
+    return M
