@@ -1,0 +1,628 @@
+// Angular part of the semilocal (type 2) and spin-orbit integrals, outercore
+// assembly and the final per-task combination of all GRPP terms.
+//
+// Reference algorithm: libgrpp/type2_integrals.c:34-243,
+// libgrpp/spin_orbit_integrals.c:41-288, libgrpp/angular_integrals.c:63-130,
+// libgrpp/outercore_integrals.c:83-390, libgrpp/full_grpp_integrals.c:27-104.
+//
+// Restructuring (same sums, same order, same skip rules):
+//  * the type 2 angular integral
+//      omega(l,L,m,a,b,c; k) = sum_mu S_{l mu}(k) sum_uvw y_{Lm,uvw} sum_rst y_{l mu,rst} I(a+r+u, b+s+v, c+t+w)
+//    is split into the k-independent tensor Atab[l,mu,L,m,abc] (the inner two
+//    sums, built once per (L, l_shell) and cached on the device) and the sum
+//    over mu done per shell and centre;
+//  * the reference's inner quantity for one binomial term (a..f),
+//      V[abc][def] = sum_{l1,l2} Q[l1][l2][|abc|+|def|] sum_m omega_A omega_B,
+//    depends only on (abc, def): it is computed once per task and potential
+//    and reused by every Cartesian pair (i, j), which then only forms
+//      gamma_ij = 16 pi^2 sum_{abc<=i, def<=j} C(..) CA^(..) CB^(..) V[abc][def].
+// Threshold skips of the reference (|factor| < 1e-13, |Q| < 1e-16,
+// |omega_1| < 1e-16 for type 2; 1e-14 everywhere for spin-orbit;
+// |S_{l mu}|, |y| < 1e-14 inside omega) are applied at the same places.
+#pragma once
+
+#include "grpp_common.cuh"
+#include "specfunc.cuh"
+
+namespace grpp {
+
+// lexicographic index of (a, b, c), a+b+c <= l (a outer, then b, then c)
+__host__ __device__ inline int abc_index(int l, int a, int b, int c)
+{
+    // triples with first component < a
+    int idx = 0;
+    for (int q = 0; q < a; q++) idx += (l - q + 1) * (l - q + 2) / 2;
+    // with first a and second < b
+    idx += b * (l - a + 1) - b * (b - 1) / 2;
+    return idx + c;
+}
+__host__ __device__ inline int n_abc(int l) { return (l + 1) * (l + 2) * (l + 3) / 6; }
+
+// lambda slots for |abc| = n: lambda = lo, lo+2, ..., L+n
+__host__ __device__ inline int lam_lo(int L, int n) { return L - n >= 0 ? L - n : ((L + n) & 1); }
+__host__ __device__ inline int lam_count(int L, int n) { return (L + n - lam_lo(L, n)) / 2 + 1; }
+__host__ __device__ inline int lam_slots(int L, int l)
+{
+    int m = 0;
+    for (int n = 0; n <= l; n++) m = m > lam_count(L, n) ? m : lam_count(L, n);
+    return m;
+}
+
+// Atab layout per (L, l): [abc][slot][mu (0..2*lmax_lam)][m (0..2L)], lmax_lam = L + l
+__host__ __device__ inline int64_t atab_size(int L, int l)
+{
+    return (int64_t)n_abc(l) * lam_slots(L, l) * (2 * (L + l) + 1) * (2 * L + 1);
+}
+
+__device__ __forceinline__ double usp_integral(int i, int j, int k)
+{
+    if ((i & 1) || (j & 1) || (k & 1)) return 0.0;
+    return 4 * kPi * dfact(i - 1) * dfact(j - 1) * dfact(k - 1) / dfact(i + j + k + 1);
+}
+
+// Atab[abc][slot][mu][m] = sum_uvw sum_rst y_{Lm,uvw} y_{lam mu,rst} I(a+r+u, ...),
+// terms skipped when |y| < 1e-14, accumulated in the reference's order
+// (angular_integrals.c:78-106: uvw outer, rst inner, y_lam * y_L * usp).
+__global__ void atab_kernel(int L, int l, double *out)
+{
+    const int nslot = lam_slots(L, l), nmu = 2 * (L + l) + 1, nm = 2 * L + 1;
+    const int64_t total = (int64_t)n_abc(l) * nslot * nmu * nm;
+    for (int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id < total; id += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = id;
+        const int m = (int)(r % nm) - L;
+        r /= nm;
+        const int mui = (int)(r % nmu);
+        r /= nmu;
+        const int slot = (int)(r % nslot);
+        const int abc = (int)(r / nslot);
+        // decode abc
+        int a = 0, b = 0, c = 0, idx = abc;
+        for (a = 0; a <= l; a++) {
+            const int cnt = (l - a + 1) * (l - a + 2) / 2;
+            if (idx < cnt) break;
+            idx -= cnt;
+        }
+        for (b = 0; b <= l - a; b++) {
+            const int cnt = l - a - b + 1;
+            if (idx < cnt) break;
+            idx -= cnt;
+        }
+        c = idx;
+        const int n = a + b + c;
+        double val = 0.0;
+        const int lam = lam_lo(L, n) + 2 * slot;
+        if (slot < lam_count(L, n) && mui <= 2 * lam) {
+            const int mu = mui - lam;
+            const int nuvw = ncart(L), nrst = ncart(lam);
+            const double *yL = c_tab.rsh_coef + c_tab.rsh_off[L] + (m + L) * nuvw;
+            const double *yl = c_tab.rsh_coef + c_tab.rsh_off[lam] + (mu + lam) * nrst;
+            const int8_t *cu = c_tab.rsh_comb + 3 * c_tab.rsh_comb_off[L];
+            const int8_t *cr = c_tab.rsh_comb + 3 * c_tab.rsh_comb_off[lam];
+            for (int iu = 0; iu < nuvw; iu++) {
+                const double y1 = yL[iu];
+                if (fabs(y1) < kZeroThresh) continue;
+                for (int ir = 0; ir < nrst; ir++) {
+                    const double y2 = yl[ir];
+                    if (fabs(y2) < kZeroThresh) continue;
+                    const double usp = usp_integral(a + cr[3 * ir] + cu[3 * iu], b + cr[3 * ir + 1] + cu[3 * iu + 1],
+                                                    c + cr[3 * ir + 2] + cu[3 * iu + 2]);
+                    val += y2 * y1 * usp;
+                }
+            }
+        }
+        out[id] = val;
+    }
+}
+
+// ---- outercore spherical projections ---------------------------------------------
+// S_sph[i][m] = sum_icart coef[m][icart] S_cart[i][icart] (outercore_integrals.c:514-525),
+// coef = spherical_to_cartesian_coef(L, m, r, s, t) / ang_norm_factor(r, s, t) (:165-177).
+struct OcProjArgs {
+    int n;                       // number of (proj, oc) blocks
+    const int *blk_shell;        // basis shell
+    const int *blk_ocshell;      // outercore shell
+    const int64_t *blk_cart_off; // offset of the n_s x ncart(oc) Cartesian block (S and U scratch)
+    const int64_t *blk_sph_off;  // offset of the n_s x (2L+1) spherical block
+    const int *shell_L, *shell_cart_off;
+    const int8_t *cart;
+    const double *S_cart, *U_cart;
+    double *S_sph, *U_sph;
+};
+
+__device__ inline double sph_coef_oc(int L, int m, int r, int s, int t)
+{
+    // find the combo (r,s,t) in the RSH table of L (lexicographic), divide by the
+    // angular norm (2 sqrt(pi))^-1 sqrt((2L+1)!!)
+    const int nc = ncart(L);
+    const int8_t *cc = c_tab.rsh_comb + 3 * c_tab.rsh_comb_off[L];
+    double y = 0.0;
+    for (int q = 0; q < nc; q++)
+        if (cc[3 * q] == r && cc[3 * q + 1] == s && cc[3 * q + 2] == t) y = c_tab.rsh_coef[c_tab.rsh_off[L] + (m + L) * nc + q];
+    const double an = 1.0 / (2.0 * sqrt(kPi)) * sqrt(dfact(2 * L + 1));
+    return y / an;
+}
+
+__global__ void oc_proj_kernel(OcProjArgs a)
+{
+    for (int blk = blockIdx.x; blk < a.n; blk += gridDim.x) {
+        const int s = a.blk_shell[blk], o = a.blk_ocshell[blk];
+        const int ns = ncart(a.shell_L[s]), L = a.shell_L[o], no = ncart(L), d = 2 * L + 1;
+        const int8_t *co = a.cart + 3 * a.shell_cart_off[o];
+        for (int e = threadIdx.x; e < ns * d; e += blockDim.x) {
+            const int i = e / d, m = e % d - L;
+            double ss = 0.0, su = 0.0;
+            for (int ic = 0; ic < no; ic++) {
+                const double u = sph_coef_oc(L, m, co[3 * ic], co[3 * ic + 1], co[3 * ic + 2]);
+                ss += u * a.S_cart[a.blk_cart_off[blk] + i * no + ic];
+                su += u * a.U_cart[a.blk_cart_off[blk] + i * no + ic];
+            }
+            a.S_sph[a.blk_sph_off[blk] + i * d + m + L] = ss;
+            a.U_sph[a.blk_sph_off[blk] + i * d + m + L] = su;
+        }
+    }
+}
+
+// ---- final per-task assembly -----------------------------------------------------
+
+constexpr int kFinThreads = 128;
+constexpr int kFinElemPerThread = 8;  // up to 1024 Cartesian pairs
+constexpr int kFinMaxLam = 24;
+constexpr int kFinMaxSl = 24;         // semilocal potentials per centre
+constexpr int kFinMaxOc = 32;         // outercore shells per centre
+
+struct FinalArgs {
+    int n_tasks;
+    const int *task_a, *task_b, *task_c;
+    const int64_t *task_out_off;
+    const uint8_t *task_has_ul;
+    const int64_t *task_q_off;        // -1 if no semilocal part
+    const int *task_proj_a, *task_proj_b; // outercore projection index of (A,C), (B,C), -1 if none
+    const int *shell_L, *shell_cart_off, *shell_prim_off;
+    const double *prim_alpha, *shell_origin;
+    const int8_t *cart;
+    const double *centre_origin;
+    const int *centre_grpp;
+    const int *grpp_sl_off, *grpp_sl_n, *grpp_n_arep, *sl_pot;
+    const int *grpp_oc_off, *grpp_n_oc, *oc_L, *oc_J;  // per outercore entry (grpp_oc_off indexing)
+    const double *oc_delta;                          // per grpp: n_oc x n_oc matrix, offset grpp_delta_off
+    const int *grpp_delta_off;
+    const int *pot_L;
+    const double *Q;
+    const int64_t *atab_off;          // [(kMaxL+2) * (kMaxL+2)] offsets of Atab per (L, l), -1 if absent
+    const double *atab;
+    const int64_t *proj_off;          // per projection: offset of its first oc block in S_sph / U_sph
+    const double *S_sph, *U_sph;
+    int raw_so;                       // 1: spin-orbit output without the 2/(2L+1) factor
+    double *arep, *so_x, *so_y, *so_z;
+    int *status;
+};
+
+// RSH values S_{l mu}(k/|k|) for l = 0..lmax (spherical_harmonics.c:227-280); out[l*(2*kFinMaxLam+1) + mu + l]
+__device__ void rsh_values(int lmax, const double *k, double *out, int tid, int nthr)
+{
+    const double len = sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
+    double ux = 0.0, uy = 0.0, uz = 0.0;
+    if (len > kZeroThresh) {
+        const double inv = 1.0 / len;
+        ux = k[0] * inv;
+        uy = k[1] * inv;
+        uz = k[2] * inv;
+    }
+    for (int e = tid; e < (lmax + 1) * (2 * kFinMaxLam + 1); e += nthr) {
+        const int l = e / (2 * kFinMaxLam + 1), mu = e % (2 * kFinMaxLam + 1) - l;
+        if (mu > l) continue;
+        const int nc = ncart(l);
+        const int8_t *cc = c_tab.rsh_comb + 3 * c_tab.rsh_comb_off[l];
+        const double *y = c_tab.rsh_coef + c_tab.rsh_off[l] + (mu + l) * nc;
+        double v = 0.0;
+        for (int q = 0; q < nc; q++) {
+            double px = 1.0, py = 1.0, pz = 1.0;
+            for (int i = 0; i < cc[3 * q]; i++) px *= ux;
+            for (int i = 0; i < cc[3 * q + 1]; i++) py *= uy;
+            for (int i = 0; i < cc[3 * q + 2]; i++) pz *= uz;
+            v += y[q] * (px * py * pz);
+        }
+        out[e] = v;
+    }
+}
+
+}  // namespace grpp
+
+namespace grpp {
+
+struct FinalSmem {
+    // offsets (in doubles) of the dynamic shared regions, computed on the host
+    int rsh_stride;  // 2*lam_max+1
+    int n_rsh;       // (lam_max+1) * rsh_stride
+    int n_omega;     // per side
+    int n_q;
+    int n_v;
+};
+
+__device__ __forceinline__ double lmat_val(int L, int comp, int m1, int m2)
+{
+    const int d = 2 * L + 1;
+    return c_tab.lmat[c_tab.lmat_off[L] + comp * d * d + (m1 + L) * d + (m2 + L)];
+}
+
+__global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSmem sm)
+{
+    extern __shared__ double dsm[];
+    __shared__ double powA[3][kMaxL + 2], powB[3][kMaxL + 2];
+    __shared__ double sCA[3], sCB[3];
+    const int tid = threadIdx.x;
+    double *rshA = dsm, *rshB = rshA + sm.n_rsh, *omA = rshB + sm.n_rsh, *omB = omA + sm.n_omega, *Qs = omB + sm.n_omega,
+           *V = Qs + sm.n_q;
+    const int rs = sm.rsh_stride;
+
+    for (int t = blockIdx.x; t < a.n_tasks; t += gridDim.x) {
+        const int sa = a.task_a[t], sb = a.task_b[t], c = a.task_c[t];
+        const int la = a.shell_L[sa], lb = a.shell_L[sb], nA = ncart(la), nB = ncart(lb), nel = nA * nB;
+        const int8_t *cA = a.cart + 3 * a.shell_cart_off[sa], *cB = a.cart + 3 * a.shell_cart_off[sb];
+        const int g = a.centre_grpp[c];
+        const int64_t oo = a.task_out_off[t];
+        __syncthreads();
+        if (tid < 3) {
+            sCA[tid] = a.centre_origin[3 * c + tid] - a.shell_origin[3 * sa + tid];
+            sCB[tid] = a.centre_origin[3 * c + tid] - a.shell_origin[3 * sb + tid];
+        }
+        __syncthreads();
+        if (tid < 3) {
+            for (int k = 0; k <= la; k++) powA[tid][k] = pow(sCA[tid], k);
+            for (int k = 0; k <= lb; k++) powB[tid][k] = pow(sCB[tid], k);
+        }
+        double acc[4][kFinElemPerThread];
+#pragma unroll
+        for (int q = 0; q < kFinElemPerThread; q++) {
+            const int e = tid + q * kFinThreads;
+            acc[0][q] = (e < nel && a.task_has_ul[t]) ? a.arep[oo + e] : 0.0;
+            acc[1][q] = acc[2][q] = acc[3][q] = 0.0;
+        }
+
+        const int nsl = a.grpp_sl_n[g];
+        if (nsl > 0 && a.task_q_off[t] >= 0) {
+            int lam_max = 0;
+            for (int p = 0; p < nsl; p++) {
+                const int Lp = a.pot_L[a.sl_pot[a.grpp_sl_off[g] + p]];
+                lam_max = max(lam_max, Lp + max(la, lb));
+            }
+            double kA[3], kB[3];
+            const double alA = a.prim_alpha[a.shell_prim_off[sa]], alB = a.prim_alpha[a.shell_prim_off[sb]];
+            for (int d = 0; d < 3; d++) {
+                kA[d] = -2.0 * (alA * (a.centre_origin[3 * c + d] - a.shell_origin[3 * sa + d]));
+                kB[d] = -2.0 * (alB * (a.centre_origin[3 * c + d] - a.shell_origin[3 * sb + d]));
+            }
+            __syncthreads();
+            // RSH values with stride rs (rsh_values uses 2*kFinMaxLam+1; use a local variant)
+            {
+                const double lenA = sqrt(kA[0] * kA[0] + kA[1] * kA[1] + kA[2] * kA[2]);
+                const double lenB = sqrt(kB[0] * kB[0] + kB[1] * kB[1] + kB[2] * kB[2]);
+                double uA[3] = {0, 0, 0}, uB[3] = {0, 0, 0};
+                if (lenA > kZeroThresh) {
+                    const double inv = 1.0 / lenA;
+                    for (int d = 0; d < 3; d++) uA[d] = kA[d] * inv;
+                }
+                if (lenB > kZeroThresh) {
+                    const double inv = 1.0 / lenB;
+                    for (int d = 0; d < 3; d++) uB[d] = kB[d] * inv;
+                }
+                for (int e = tid; e < 2 * (lam_max + 1) * rs; e += kFinThreads) {
+                    const int side = e / ((lam_max + 1) * rs), r = e % ((lam_max + 1) * rs);
+                    const int l = r / rs, mu = r % rs - l;
+                    if (mu > l) continue;
+                    const double *u = side ? uB : uA;
+                    const int nc = ncart(l);
+                    const int8_t *cc = c_tab.rsh_comb + 3 * c_tab.rsh_comb_off[l];
+                    const double *y = c_tab.rsh_coef + c_tab.rsh_off[l] + (mu + l) * nc;
+                    double v = 0.0;
+                    for (int q = 0; q < nc; q++) {
+                        double px = 1.0, py = 1.0, pz = 1.0;
+                        for (int i = 0; i < cc[3 * q]; i++) px *= u[0];
+                        for (int i = 0; i < cc[3 * q + 1]; i++) py *= u[1];
+                        for (int i = 0; i < cc[3 * q + 2]; i++) pz *= u[2];
+                        v += y[q] * (px * py * pz);
+                    }
+                    (side ? rshB : rshA)[l * rs + mu + l] = v;
+                }
+            }
+            const int64_t qbase = a.task_q_off[t];
+            int64_t qoff = 0;
+            const int n_arep = a.grpp_n_arep[g];
+            for (int p = 0; p < nsl; p++) {
+                const int L = a.pot_L[a.sl_pot[a.grpp_sl_off[g] + p]];
+                const bool so = p >= n_arep;
+                const int d1 = L + la + 1, d2 = L + lb + 1, dn = la + lb + 1, nm = 2 * L + 1;
+                const int slA = lam_slots(L, la), slB = lam_slots(L, lb);
+                const int nabA = n_abc(la), nabB = n_abc(lb);
+                const int nmuA = 2 * (L + la) + 1, nmuB = 2 * (L + lb) + 1;
+                const double *AtA = a.atab + a.atab_off[L * (kMaxL + 2) + la];
+                const double *AtB = a.atab + a.atab_off[L * (kMaxL + 2) + lb];
+                __syncthreads();
+                // omega tables: omega[abc][slot][m] = sum_mu S_{lam mu} Atab (angular_integrals.c:78-108)
+                for (int e = tid; e < nabA * slA * nm + nabB * slB * nm; e += kFinThreads) {
+                    const bool sideB = e >= nabA * slA * nm;
+                    const int r = sideB ? e - nabA * slA * nm : e;
+                    const int sl = sideB ? slB : slA, nab = sideB ? nabB : nabA, l = sideB ? lb : la;
+                    const int m = r % nm, slot = (r / nm) % sl, abc = r / (nm * sl);
+                    (void)nab;
+                    // n of abc: decode from the index
+                    int aa = 0, idx = abc;
+                    for (aa = 0; aa <= l; aa++) {
+                        const int cnt = (l - aa + 1) * (l - aa + 2) / 2;
+                        if (idx < cnt) break;
+                        idx -= cnt;
+                    }
+                    int bb = 0;
+                    for (bb = 0; bb <= l - aa; bb++) {
+                        const int cnt = l - aa - bb + 1;
+                        if (idx < cnt) break;
+                        idx -= cnt;
+                    }
+                    const int n = aa + bb + idx;
+                    double w = 0.0;
+                    if (slot < lam_count(L, n)) {
+                        const int lam = lam_lo(L, n) + 2 * slot;
+                        const double *S = (sideB ? rshB : rshA) + lam * rs;
+                        const double *At = (sideB ? AtB : AtA) + ((int64_t)(abc * sl + slot) * (sideB ? nmuB : nmuA)) * nm + m;
+                        for (int mu = -lam; mu <= lam; mu++) {
+                            const double rv = S[mu + lam];
+                            if (fabs(rv) < kZeroThresh) continue;
+                            w += At[(int64_t)(mu + lam) * nm] * rv;
+                        }
+                    }
+                    (sideB ? omB : omA)[r] = w;
+                }
+                for (int e = tid; e < d1 * d2 * dn; e += kFinThreads) Qs[e] = a.Q[qbase + qoff + e];
+                qoff += (int64_t)d1 * d2 * dn;
+                __syncthreads();
+
+                const int ncomp = so ? 3 : 1;
+                const double thrF = so ? kZeroThresh : 1e-13, thrQ = so ? kZeroThresh : 1e-16, thrW = so ? kZeroThresh : 1e-16;
+                const int rows = max(1, min(nabA, sm.n_v / (nabB * ncomp)));
+                double gam[3][kFinElemPerThread];
+#pragma unroll
+                for (int q = 0; q < kFinElemPerThread; q++) gam[0][q] = gam[1][q] = gam[2][q] = 0.0;
+
+                for (int r0 = 0; r0 < nabA; r0 += rows) {
+                    const int r1 = min(nabA, r0 + rows);
+                    __syncthreads();
+                    // V[abc][def] (type2_integrals.c:174-196, spin_orbit_integrals.c:197-224)
+                    for (int e = tid; e < (r1 - r0) * nabB; e += kFinThreads) {
+                        const int abc = r0 + e / nabB, def = e % nabB;
+                        int aa = 0, idx = abc;
+                        for (aa = 0; aa <= la; aa++) {
+                            const int cnt = (la - aa + 1) * (la - aa + 2) / 2;
+                            if (idx < cnt) break;
+                            idx -= cnt;
+                        }
+                        int bb;
+                        for (bb = 0; bb <= la - aa; bb++) {
+                            const int cnt = la - aa - bb + 1;
+                            if (idx < cnt) break;
+                            idx -= cnt;
+                        }
+                        const int n1 = aa + bb + idx;
+                        int dd = 0, jdx = def;
+                        for (dd = 0; dd <= lb; dd++) {
+                            const int cnt = (lb - dd + 1) * (lb - dd + 2) / 2;
+                            if (jdx < cnt) break;
+                            jdx -= cnt;
+                        }
+                        int ee;
+                        for (ee = 0; ee <= lb - dd; ee++) {
+                            const int cnt = lb - dd - ee + 1;
+                            if (jdx < cnt) break;
+                            jdx -= cnt;
+                        }
+                        const int n2 = dd + ee + jdx, N = n1 + n2;
+                        double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+                        const int c1 = lam_count(L, n1), c2 = lam_count(L, n2);
+                        for (int s1 = 0; s1 < c1; s1++) {
+                            const int l1 = lam_lo(L, n1) + 2 * s1;
+                            const double *w1 = omA + (abc * slA + s1) * nm;
+                            for (int s2 = 0; s2 < c2; s2++) {
+                                const int l2 = lam_lo(L, n2) + 2 * s2;
+                                const double QN = Qs[(l1 * d2 + l2) * dn + N];
+                                if (fabs(QN) < thrQ) continue;
+                                const double *w2 = omB + (def * slB + s2) * nm;
+                                if (!so) {
+                                    double sa2 = 0.0;
+                                    for (int m = 0; m < nm; m++) {
+                                        if (fabs(w1[m]) < thrW) continue;
+                                        sa2 += w1[m] * w2[m];
+                                    }
+                                    v0 += QN * sa2;
+                                } else {
+                                    double sx = 0.0, sy = 0.0, sz = 0.0;
+                                    for (int m1 = -L; m1 <= L; m1++)
+                                        for (int m2 = -L; m2 <= L; m2++) {
+                                            const double lx = lmat_val(L, 0, m1, m2), ly = lmat_val(L, 1, m1, m2),
+                                                         lz = lmat_val(L, 2, m1, m2);
+                                            if (fabs(lx) < kZeroThresh && fabs(ly) < kZeroThresh && fabs(lz) < kZeroThresh) continue;
+                                            const double o1 = w1[m1 + L];
+                                            if (fabs(o1) < kZeroThresh) continue;
+                                            const double o2 = w2[m2 + L];
+                                            sx += o1 * o2 * lx;
+                                            sy += o1 * o2 * ly;
+                                            sz += o1 * o2 * lz;
+                                        }
+                                    v0 += QN * sx;
+                                    v1 += QN * sy;
+                                    v2 += QN * sz;
+                                }
+                            }
+                        }
+                        V[e * ncomp] = v0;
+                        if (so) {
+                            V[e * ncomp + 1] = v1;
+                            V[e * ncomp + 2] = v2;
+                        }
+                    }
+                    __syncthreads();
+                    // Cartesian pairs: binomial re-centring sums over (a..f) in the reference's loop order
+#pragma unroll
+                    for (int q = 0; q < kFinElemPerThread; q++) {
+                        const int el = tid + q * kFinThreads;
+                        if (el >= nel) continue;
+                        const int i = el / nB, j = el % nB;
+                        const int ax = cA[3 * i], ay = cA[3 * i + 1], az = cA[3 * i + 2];
+                        const int bx = cB[3 * j], by = cB[3 * j + 1], bz = cB[3 * j + 2];
+                        double g0 = gam[0][q], g1 = gam[1][q], g2 = gam[2][q];
+                        for (int aa = 0; aa <= ax; aa++)
+                            for (int bb = 0; bb <= ay; bb++)
+                                for (int cc = 0; cc <= az; cc++) {
+                                    const int abc = abc_index(la, aa, bb, cc);
+                                    if (abc < r0 || abc >= r1) continue;
+                                    const double cabc = c_tab.binom[ax * kBinN + aa] * c_tab.binom[ay * kBinN + bb] *
+                                                        c_tab.binom[az * kBinN + cc];
+                                    for (int dd = 0; dd <= bx; dd++)
+                                        for (int ee = 0; ee <= by; ee++)
+                                            for (int ff = 0; ff <= bz; ff++) {
+                                                const double f = cabc * c_tab.binom[bx * kBinN + dd] * c_tab.binom[by * kBinN + ee] *
+                                                                 c_tab.binom[bz * kBinN + ff] * powA[0][ax - aa] * powA[1][ay - bb] *
+                                                                 powA[2][az - cc] * powB[0][bx - dd] * powB[1][by - ee] *
+                                                                 powB[2][bz - ff];
+                                                if (fabs(f) < thrF) continue;
+                                                const int def = abc_index(lb, dd, ee, ff);
+                                                const double *vv = V + ((abc - r0) * nabB + def) * ncomp;
+                                                g0 += f * vv[0];
+                                                if (so) {
+                                                    g1 += f * vv[1];
+                                                    g2 += f * vv[2];
+                                                }
+                                            }
+                                }
+                        gam[0][q] = g0;
+                        gam[1][q] = g1;
+                        gam[2][q] = g2;
+                    }
+                }
+                const double pi16 = 16 * kPi * kPi;
+                const double fso = a.raw_so ? 1.0 : 2.0 / (2 * L + 1);
+#pragma unroll
+                for (int q = 0; q < kFinElemPerThread; q++) {
+                    if (!so) {
+                        acc[0][q] += 1.0 * (gam[0][q] * pi16);
+                    } else {
+                        acc[1][q] += fso * (gam[0][q] * pi16);
+                        acc[2][q] += fso * (gam[1][q] * pi16);
+                        acc[3][q] += fso * (gam[2][q] * pi16);
+                    }
+                }
+            }
+        }
+
+        // ---- outercore non-local terms (outercore_integrals.c:147-390)
+        const int noc = a.grpp_n_oc[g];
+        if (noc > 0 && a.task_proj_a[t] >= 0) {
+            const int64_t pa = a.proj_off[a.task_proj_a[t]], pb = a.proj_off[a.task_proj_b[t]];
+            const int ocoff = a.grpp_oc_off[g];
+            const double *dl = a.oc_delta + a.grpp_delta_off[g];
+#pragma unroll
+            for (int q = 0; q < kFinElemPerThread; q++) {
+                const int el = tid + q * kFinThreads;
+                if (el >= nel) continue;
+                const int i = el / nB, j = el % nB;
+                double oa = 0.0, ox = 0.0, oy = 0.0, oz = 0.0;
+                // part 1
+                int64_t offA = pa, offB = pb;
+                for (int k = 0; k < noc; k++) {
+                    const int L = a.oc_L[ocoff + k], d = 2 * L + 1;
+                    const double J = a.oc_J[ocoff + k] / 2.0;
+                    const double *SA = a.S_sph + offA + i * d, *UA = a.U_sph + offA + i * d;
+                    const double *SB = a.S_sph + offB + j * d, *UB = a.U_sph + offB + j * d;
+                    const double farep = (J < L) ? (L / (2.0 * L + 1)) : ((L + 1) / (2.0 * L + 1));
+                    const double fso = (J < L) ? (-2.0 / (2 * L + 1)) : (+2.0 / (2 * L + 1));
+                    double s1 = 0.0, s2 = 0.0;
+                    for (int m = 0; m < d; m++) s1 += SA[m] * UB[m];
+                    for (int m = 0; m < d; m++) s2 += UA[m] * SB[m];
+                    double buf = 0.0;
+                    buf += s1;
+                    buf += s2;
+                    oa += farep * buf;
+                    double *oso[3] = {&ox, &oy, &oz};
+                    for (int comp = 0; comp < 3; comp++) {
+                        // so_buf = U_a (L S_b) + (S_a L) U_b
+                        double t1 = 0.0;
+                        for (int m1 = 0; m1 < d; m1++) {
+                            double tm = 0.0;
+                            for (int m2 = 0; m2 < d; m2++) tm += lmat_val(L, comp, m1 - L, m2 - L) * SB[m2];
+                            double tmp = 0.0;
+                            tmp += tm;
+                            t1 += UA[m1] * tmp;
+                        }
+                        double sob = 0.0;
+                        sob += t1;
+                        double t2 = 0.0;
+                        for (int m = 0; m < d; m++) {
+                            double tm = 0.0;
+                            for (int k2 = 0; k2 < d; k2++) tm += SA[k2] * lmat_val(L, comp, k2 - L, m - L);
+                            double tmp = 0.0;
+                            tmp += tm;
+                            t2 += tmp * UB[m];
+                        }
+                        sob += t2;
+                        *oso[comp] += fso * sob;
+                    }
+                    offA += (int64_t)nA * d;
+                    offB += (int64_t)nB * d;
+                }
+                // part 2
+                int64_t offA1 = pa;
+                for (int k1 = 0; k1 < noc; k1++) {
+                    const int L1 = a.oc_L[ocoff + k1], d = 2 * L1 + 1;
+                    int64_t offB2 = pb;
+                    for (int k2 = 0; k2 < noc; k2++) {
+                        const int L2 = a.oc_L[ocoff + k2];
+                        const int d2 = 2 * L2 + 1;
+                        if (L1 == L2 && a.oc_J[ocoff + k1] == a.oc_J[ocoff + k2]) {
+                            const double delta = dl[k1 * noc + k2];
+                            const double J = a.oc_J[ocoff + k1] / 2.0;
+                            const int L = L1;
+                            const double farep = (J < L) ? (L / (2.0 * L + 1)) : ((L + 1) / (2.0 * L + 1));
+                            const double fso = (J < L) ? (-2.0 / (2 * L + 1)) : (+2.0 / (2 * L + 1));
+                            const double *SA = a.S_sph + offA1 + i * d, *SB = a.S_sph + offB2 + j * d;
+                            double s = 0.0;
+                            for (int m = 0; m < d; m++) s += SA[m] * SB[m];
+                            double buf = 0.0;
+                            buf += s;
+                            oa += (-1.0) * delta * farep * buf;
+                            double *oso[3] = {&ox, &oy, &oz};
+                            for (int comp = 0; comp < 3; comp++) {
+                                double t1 = 0.0;
+                                for (int m1 = 0; m1 < d; m1++) {
+                                    double tm = 0.0;
+                                    for (int m2 = 0; m2 < d; m2++) tm += lmat_val(L, comp, m1 - L, m2 - L) * SB[m2];
+                                    double tmp = 0.0;
+                                    tmp += tm;
+                                    t1 += SA[m1] * tmp;
+                                }
+                                double sob = 0.0;
+                                sob += t1;
+                                *oso[comp] += (-1.0) * delta * fso * sob;
+                            }
+                        }
+                        offB2 += (int64_t)nB * d2;
+                    }
+                    offA1 += (int64_t)nA * d;
+                }
+                acc[0][q] += 1.0 * oa;
+                acc[1][q] += 1.0 * ox;
+                acc[2][q] += 1.0 * oy;
+                acc[3][q] += 1.0 * oz;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kFinElemPerThread; q++) {
+            const int e = tid + q * kFinThreads;
+            if (e < nel) {
+                a.arep[oo + e] = acc[0][q];
+                a.so_x[oo + e] = acc[1][q];
+                a.so_y[oo + e] = acc[2][q];
+                a.so_z[oo + e] = acc[3][q];
+            }
+        }
+    }
+}
+
+}  // namespace grpp

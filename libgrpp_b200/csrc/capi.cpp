@@ -1,0 +1,653 @@
+// libgrpp C API on top of the B200 engine.
+//
+// Containers keep libgrpp's semantics (libgrpp/shell.c, potential.c, grpp.c,
+// parameters.c). Every integrator builds a one-task batch and runs the same
+// GPU pipeline as the batched entry points (engine.cu). Differences from the
+// reference's behaviour, by design:
+//  * no caller object is written during a call (libgrpp binds the outercore
+//    shells' origins to the centre, libgrpp/outercore_integrals.c:107-111, which
+//    makes concurrent calls on one GRPP object race); the result is the same;
+//  * misuse is reported through libgrpp_b200_last_error() with the outputs
+//    zeroed, instead of assert().
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/libgrpp.h"
+#include "../../include/libgrpp_b200.h"
+#include "engine.h"
+
+namespace {
+
+int gen_dirac(int L, int *cl)
+{
+    int c = 0;
+    for (int r = L; r >= 0; r--)
+        for (int s = L; s >= 0; s--)
+            for (int t = L; t >= 0; t--)
+                if (r + s + t == L) {
+                    cl[3 * c] = r;
+                    cl[3 * c + 1] = s;
+                    cl[3 * c + 2] = t;
+                    c++;
+                }
+    return (L + 1) * (L + 2) / 2;
+}
+
+int gen_turbomole(int L, int *cl)
+{
+    int c = 0;
+    for (int r = L; r >= 0; r--)
+        for (int s = L - r; s >= 0; s--) {
+            cl[3 * c] = r;
+            cl[3 * c + 1] = s;
+            cl[3 * c + 2] = L - r - s;
+            c++;
+        }
+    return (L + 1) * (L + 2) / 2;
+}
+
+int g_initialized = 0;
+std::mutex g_init_mu;
+
+constexpr int kMaxPots = 100;  // grpp.c:12
+
+double gaussian_norm(int L, double a) { return std::pow(2 * a / M_PI, 0.75) * std::pow(4 * a, 0.5 * L); }
+
+// Flat batch assembled from libgrpp objects.
+struct Builder {
+    std::vector<int> shell_L, shell_nprim, shell_prim_off, shell_cart_off, cart_list;
+    std::vector<double> prim_coef, prim_alpha, shell_origin;
+    std::vector<int> pot_L, pot_J, pot_nprim, pot_prim_off, pot_powers;
+    std::vector<double> pot_coef, pot_alpha;
+    std::vector<int> grpp_UL, grpp_arep_off, grpp_n_arep, grpp_so_off, grpp_n_so, grpp_oc_off, grpp_n_oc, grpp_pot_list,
+        grpp_oc_pot, grpp_oc_shell;
+    std::vector<double> centre_origin;
+    std::vector<int> centre_grpp, task_a, task_b, task_c;
+
+    int add_shell(const libgrpp_shell_t *s)
+    {
+        shell_L.push_back(s->L);
+        shell_nprim.push_back(s->num_primitives);
+        shell_prim_off.push_back((int)prim_coef.size());
+        shell_cart_off.push_back((int)cart_list.size() / 3);
+        for (int i = 0; i < 3 * s->cart_size; i++) cart_list.push_back(s->cart_list[i]);
+        for (int i = 0; i < s->num_primitives; i++) {
+            prim_coef.push_back(s->coeffs[i]);
+            prim_alpha.push_back(s->alpha[i]);
+        }
+        for (int d = 0; d < 3; d++) shell_origin.push_back(s->origin[d]);
+        return (int)shell_L.size() - 1;
+    }
+    int add_pot(const libgrpp_potential_t *p)
+    {
+        pot_L.push_back(p->L);
+        pot_J.push_back(p->J);
+        pot_nprim.push_back(p->num_primitives);
+        pot_prim_off.push_back((int)pot_coef.size());
+        for (int i = 0; i < p->num_primitives; i++) {
+            pot_powers.push_back(p->powers[i]);
+            pot_coef.push_back(p->coeffs[i]);
+            pot_alpha.push_back(p->alpha[i]);
+        }
+        return (int)pot_L.size() - 1;
+    }
+    int add_grpp(const libgrpp_potential_t *UL, int n_arep, libgrpp_potential_t *const *arep, int n_so,
+                 libgrpp_potential_t *const *so, int n_oc, libgrpp_potential_t *const *ocp, libgrpp_shell_t *const *ocs)
+    {
+        grpp_UL.push_back(UL ? add_pot(UL) : -1);
+        grpp_arep_off.push_back((int)grpp_pot_list.size());
+        grpp_n_arep.push_back(n_arep);
+        for (int i = 0; i < n_arep; i++) grpp_pot_list.push_back(add_pot(arep[i]));
+        grpp_so_off.push_back((int)grpp_pot_list.size());
+        grpp_n_so.push_back(n_so);
+        for (int i = 0; i < n_so; i++) grpp_pot_list.push_back(add_pot(so[i]));
+        grpp_oc_off.push_back((int)grpp_oc_pot.size());
+        grpp_n_oc.push_back(n_oc);
+        for (int i = 0; i < n_oc; i++) {
+            const int p = add_pot(ocp[i]);
+            const int s = add_shell(ocs[i]);
+            grpp_oc_pot.push_back(p);
+            grpp_oc_shell.push_back(s);
+        }
+        return (int)grpp_UL.size() - 1;
+    }
+    int add_centre(const double *C, int g)
+    {
+        for (int d = 0; d < 3; d++) centre_origin.push_back(C[d]);
+        centre_grpp.push_back(g);
+        return (int)centre_grpp.size() - 1;
+    }
+    void add_task(int a, int b, int c)
+    {
+        task_a.push_back(a);
+        task_b.push_back(b);
+        task_c.push_back(c);
+    }
+    libgrpp_b200_batch_t view() const
+    {
+        libgrpp_b200_batch_t v;
+        v.n_shells = (int)shell_L.size();
+        v.shell_L = shell_L.data();
+        v.shell_nprim = shell_nprim.data();
+        v.shell_prim_off = shell_prim_off.data();
+        v.prim_coef = prim_coef.data();
+        v.prim_alpha = prim_alpha.data();
+        v.shell_origin = shell_origin.data();
+        v.shell_cart_off = shell_cart_off.data();
+        v.cart_list = cart_list.data();
+        v.n_pots = (int)pot_L.size();
+        v.pot_L = pot_L.data();
+        v.pot_J = pot_J.data();
+        v.pot_nprim = pot_nprim.data();
+        v.pot_prim_off = pot_prim_off.data();
+        v.pot_powers = pot_powers.data();
+        v.pot_coef = pot_coef.data();
+        v.pot_alpha = pot_alpha.data();
+        v.n_grpps = (int)grpp_UL.size();
+        v.grpp_UL = grpp_UL.data();
+        v.grpp_arep_off = grpp_arep_off.data();
+        v.grpp_n_arep = grpp_n_arep.data();
+        v.grpp_so_off = grpp_so_off.data();
+        v.grpp_n_so = grpp_n_so.data();
+        v.grpp_oc_off = grpp_oc_off.data();
+        v.grpp_n_oc = grpp_n_oc.data();
+        v.grpp_pot_list = grpp_pot_list.data();
+        v.grpp_oc_pot = grpp_oc_pot.data();
+        v.grpp_oc_shell = grpp_oc_shell.data();
+        v.n_centres = (int)centre_grpp.size();
+        v.centre_origin = centre_origin.data();
+        v.centre_grpp = centre_grpp.data();
+        v.n_tasks = (int64_t)task_a.size();
+        v.task_a = task_a.data();
+        v.task_b = task_b.data();
+        v.task_c = task_c.data();
+        return v;
+    }
+};
+
+bool check_init()
+{
+    if (!g_initialized) {
+        grpp::set_error(LIBGRPP_B200_ERR_NOT_INIT, "libgrpp_init() was not called");
+        return false;
+    }
+    return true;
+}
+
+// run a one-centre batch; out[k] receive consecutive task blocks
+int run(const Builder &bd, int raw_so, std::vector<double> out[4])
+{
+    libgrpp_b200_batch_t v = bd.view();
+    const int64_t n = grpp::batch_output_size(&v);
+    for (int k = 0; k < 4; k++) out[k].assign(std::max<int64_t>(n, 1), 0.0);
+    grpp::RunOptions opt;
+    opt.raw_so = raw_so;
+    return grpp::run_full_batch(&v, opt, out[0].data(), out[1].data(), out[2].data(), out[3].data());
+}
+
+// differentiate_shell (libgrpp/diff_gaussian.c:35-63): L-1 with N_L/N_{L-1}, L+1 with 2 a N_L/N_{L+1}
+libgrpp_shell_t *shell_down(const libgrpp_shell_t *s)
+{
+    if (s->L == 0) return nullptr;
+    libgrpp_shell_t *d = libgrpp_new_shell((double *)s->origin, s->L - 1, s->num_primitives, s->coeffs, s->alpha);
+    for (int i = 0; i < s->num_primitives; i++)
+        d->coeffs[i] *= gaussian_norm(s->L, s->alpha[i]) / gaussian_norm(s->L - 1, s->alpha[i]);
+    return d;
+}
+
+libgrpp_shell_t *shell_up(const libgrpp_shell_t *s)
+{
+    libgrpp_shell_t *u = libgrpp_new_shell((double *)s->origin, s->L + 1, s->num_primitives, s->coeffs, s->alpha);
+    for (int i = 0; i < s->num_primitives; i++)
+        u->coeffs[i] *= 2.0 * s->alpha[i] * gaussian_norm(s->L, s->alpha[i]) / gaussian_norm(s->L + 1, s->alpha[i]);
+    return u;
+}
+
+// overlap_gradient.c:219-241
+int nlm_to_linear(const int *nlm)
+{
+    const int L = nlm[0] + nlm[1] + nlm[2], n = (L + 1) * (L + 2) / 2;
+    std::vector<int> cl(3 * n);
+    libgrpp_params.cartesian_generator(L, cl.data());
+    int idx;
+    for (idx = 0; idx < n; idx++)
+        if (cl[3 * idx] == nlm[0] && cl[3 * idx + 1] == nlm[1] && cl[3 * idx + 2] == nlm[2]) break;
+    return idx;
+}
+
+int points_equal(const double *a, const double *b)
+{
+    return std::fabs(a[0] - b[0]) < 1e-12 && std::fabs(a[1] - b[1]) < 1e-12 && std::fabs(a[2] - b[2]) < 1e-12;
+}
+
+struct GradContribution {
+    int diff_bra;
+    double factor;
+};
+
+// grpp_integrals_gradient.c:280-393: which (differentiated side, sign) terms contribute
+std::vector<GradContribution> gradient_terms(const double *A, const double *B, const double *C, const double *D)
+{
+    std::vector<GradContribution> out;
+    if (points_equal(A, C) && points_equal(B, C)) return out;
+    if (!points_equal(A, D) && !points_equal(B, D) && !points_equal(C, D)) return out;
+    if (!points_equal(A, C) && !points_equal(C, B) && !points_equal(A, B)) {
+        if (points_equal(A, D)) out.push_back({1, +1.0});
+        if (points_equal(B, D)) out.push_back({0, +1.0});
+        if (points_equal(C, D)) {
+            out.push_back({1, -1.0});
+            out.push_back({0, -1.0});
+        }
+    }
+    if (points_equal(A, B) && !points_equal(A, C)) {
+        const double f = points_equal(A, D) ? +1.0 : -1.0;
+        out.push_back({1, f});
+        out.push_back({0, f});
+    }
+    if (!points_equal(A, C) && points_equal(C, B)) out.push_back({1, points_equal(A, D) ? +1.0 : -1.0});
+    if (points_equal(A, C) && !points_equal(C, B)) out.push_back({0, points_equal(B, D) ? +1.0 : -1.0});
+    return out;
+}
+
+// Full-GRPP gradient of one shell pair w.r.t. point D for one GRPP description added by add_grpp_fn.
+template <typename AddGrpp>
+void gradient_impl(libgrpp_shell_t *A, libgrpp_shell_t *B, const double *C, const double *D, AddGrpp add_grpp, int raw_so,
+                   double **g0, double **g1, double **g2, double **g3)
+{
+    const int nA = A->cart_size, nB = B->cart_size, n = nA * nB;
+    double **gr[4] = {g0, g1, g2, g3};
+    for (int c = 0; c < 4; c++)
+        for (int k = 0; k < 3; k++)
+            if (gr[c] && gr[c][k]) memset(gr[c][k], 0, n * sizeof(double));
+    if (!check_init()) return;
+    const std::vector<GradContribution> terms = gradient_terms(A->origin, B->origin, C, D);
+    if (terms.empty()) return;
+    libgrpp_shell_t *Ad = shell_down(A), *Au = shell_up(A), *Bd = shell_down(B), *Bu = shell_up(B);
+    Builder bd;
+    const int iA = bd.add_shell(A), iB = bd.add_shell(B), iAu = bd.add_shell(Au), iBu = bd.add_shell(Bu);
+    const int iAd = Ad ? bd.add_shell(Ad) : -1, iBd = Bd ? bd.add_shell(Bd) : -1;
+    const int g = add_grpp(bd);
+    const int c = bd.add_centre(C, g);
+    // tasks: (Ad,B) (Au,B) (A,Bd) (A,Bu)
+    int t_ad = -1, t_au, t_bd = -1, t_bu, nt = 0;
+    std::vector<int64_t> off;
+    auto add = [&](int a, int b) {
+        bd.add_task(a, b, c);
+        return nt++;
+    };
+    if (iAd >= 0) t_ad = add(iAd, iB);
+    t_au = add(iAu, iB);
+    if (iBd >= 0) t_bd = add(iA, iBd);
+    t_bu = add(iA, iBu);
+    std::vector<double> out[4];
+    if (run(bd, raw_so, out) == 0) {
+        std::vector<int64_t> boff(nt + 1, 0);
+        for (int t = 0; t < nt; t++)
+            boff[t + 1] = boff[t] + (int64_t)((bd.shell_L[bd.task_a[t]] + 1) * (bd.shell_L[bd.task_a[t]] + 2) / 2) *
+                                        ((bd.shell_L[bd.task_b[t]] + 1) * (bd.shell_L[bd.task_b[t]] + 2) / 2);
+        for (const GradContribution &tc : terms) {
+            const int diff_bra = tc.diff_bra;
+            const int td = diff_bra ? t_ad : t_bd, tu = diff_bra ? t_au : t_bu;
+            const int nd = diff_bra ? (Ad ? Ad->cart_size : 0) : (Bd ? Bd->cart_size : 0);
+            const int nu = diff_bra ? Au->cart_size : Bu->cart_size;
+            for (int k = 0; k < 3; k++)
+                for (int i = 0; i < nA; i++)
+                    for (int j = 0; j < nB; j++) {
+                        int bra[3] = {A->cart_list[3 * i], A->cart_list[3 * i + 1], A->cart_list[3 * i + 2]};
+                        int ket[3] = {B->cart_list[3 * j], B->cart_list[3 * j + 1], B->cart_list[3 * j + 2]};
+                        int *dn = diff_bra ? bra : ket;
+                        const int idx = i * nB + j;
+                        // libgrpp also forms this term when the exponent is 0, reading outside the
+                        // L-1 block and multiplying by 0 (grpp_integrals_gradient.c:452-466);
+                        // skipping it gives the same value without the out-of-bounds read
+                        if (nd > 0 && dn[k] > 0) {
+                            dn[k] -= 1;
+                            const int bi = nlm_to_linear(bra), ki = nlm_to_linear(ket);
+                            dn[k] += 1;
+                            const int nn = dn[k], row = diff_bra ? nB : nd, id = row * bi + ki;
+                            for (int cmp = 0; cmp < 4; cmp++)
+                                if (gr[cmp]) gr[cmp][k][idx] -= tc.factor * nn * out[cmp][boff[td] + id];
+                        }
+                        dn[k] += 1;
+                        const int bi = nlm_to_linear(bra), ki = nlm_to_linear(ket);
+                        dn[k] -= 1;
+                        const int row = diff_bra ? nB : nu, id = row * bi + ki;
+                        for (int cmp = 0; cmp < 4; cmp++)
+                            if (gr[cmp]) gr[cmp][k][idx] += tc.factor * out[cmp][boff[tu] + id];
+                    }
+        }
+    }
+    if (Ad) libgrpp_delete_shell(Ad);
+    if (Bd) libgrpp_delete_shell(Bd);
+    libgrpp_delete_shell(Au);
+    libgrpp_delete_shell(Bu);
+}
+
+}  // namespace
+
+#pragma GCC visibility push(default)
+extern "C" {
+
+// ============================================================ parameters (parameters.c:17-134)
+libgrpp_parameters_t libgrpp_params = {1e-16, 1e-16, 1e-16, gen_dirac};
+
+void libgrpp_set_default_parameters(void)
+{
+    libgrpp_params.radial_tolerance = 1e-16;
+    libgrpp_params.angular_screening_tolerance = 1e-16;
+    libgrpp_params.modified_bessel_tolerance = 1e-16;
+    libgrpp_params.cartesian_generator = gen_dirac;
+}
+void libgrpp_set_radial_tolerance(double t) { libgrpp_params.radial_tolerance = t; }
+void libgrpp_set_angular_screening_tolerance(double t) { libgrpp_params.angular_screening_tolerance = t; }
+void libgrpp_set_modified_bessel_tolerance(double t) { libgrpp_params.modified_bessel_tolerance = t; }
+void libgrpp_set_cartesian_order(int order)
+{
+    if (order == LIBGRPP_CART_ORDER_DIRAC) libgrpp_params.cartesian_generator = gen_dirac;
+    else if (order == LIBGRPP_CART_ORDER_TURBOMOLE) libgrpp_params.cartesian_generator = gen_turbomole;
+    else grpp::set_error(LIBGRPP_B200_ERR_INVALID, "unknown Cartesian order");
+}
+void libgrpp_set_cartesian_generator(int (*g)(int, int *)) { libgrpp_params.cartesian_generator = g; }
+
+// ============================================================ init (init_finalize.c:19-50)
+void libgrpp_init(void)
+{
+    std::lock_guard<std::mutex> lk(g_init_mu);
+    g_initialized = 1;
+}
+void libgrpp_finalize(void)
+{
+    std::lock_guard<std::mutex> lk(g_init_mu);
+    g_initialized = 0;
+}
+int libgrpp_is_initialized(void) { return g_initialized; }
+
+// ============================================================ potentials (potential.c:22-115)
+libgrpp_potential_t *libgrpp_new_potential(int L, int J, int n, int *powers, double *coeffs, double *alpha)
+{
+    libgrpp_potential_t *p = (libgrpp_potential_t *)calloc(1, sizeof(libgrpp_potential_t));
+    p->L = L;
+    p->J = J;
+    p->powers = (int *)calloc(n > 0 ? n : 1, sizeof(int));
+    p->coeffs = (double *)calloc(n > 0 ? n : 1, sizeof(double));
+    p->alpha = (double *)calloc(n > 0 ? n : 1, sizeof(double));
+    for (int i = 0; i < n; i++) {
+        if (std::fabs(coeffs[i]) < LIBGRPP_ZERO_THRESH) continue;
+        p->coeffs[p->num_primitives] = coeffs[i];
+        p->powers[p->num_primitives] = powers[i];
+        p->alpha[p->num_primitives] = alpha[i];
+        p->num_primitives++;
+    }
+    return p;
+}
+
+void libgrpp_delete_potential(libgrpp_potential_t *p)
+{
+    if (!p) return;
+    free(p->powers);
+    free(p->coeffs);
+    free(p->alpha);
+    free(p);
+}
+
+double libgrpp_potential_value(libgrpp_potential_t *p, double r)
+{
+    double v = 0.0;
+    const double r2 = r * r;
+    for (int i = 0; i < p->num_primitives; i++) v += p->coeffs[i] * std::pow(r, p->powers[i] - 2) * std::exp(-p->alpha[i] * r2);
+    return v;
+}
+
+libgrpp_potential_t *libgrpp_shrink_potential(libgrpp_potential_t *src)
+{
+    const int n = src->num_primitives;
+    std::vector<int> pw;
+    std::vector<double> c, a;
+    for (int i = 0; i < n; i++)
+        if (std::fabs(src->coeffs[i]) > LIBGRPP_ZERO_THRESH) {
+            pw.push_back(src->powers[i]);
+            c.push_back(src->coeffs[i]);
+            a.push_back(src->alpha[i]);
+        }
+    return libgrpp_new_potential(src->L, src->J, (int)c.size(), pw.data(), c.data(), a.data());
+}
+
+// ============================================================ shells (shell.c:23-126)
+int *libgrpp_generate_shell_cartesians(int L)
+{
+    const int n = (L + 1) * (L + 2) / 2;
+    int *cl = (int *)calloc(3 * n, sizeof(int));
+    libgrpp_params.cartesian_generator(L, cl);
+    return cl;
+}
+
+libgrpp_shell_t *libgrpp_new_shell(double *origin, int L, int n, double *coeffs, double *alpha)
+{
+    libgrpp_shell_t *s = (libgrpp_shell_t *)malloc(sizeof(libgrpp_shell_t));
+    s->L = L;
+    for (int d = 0; d < 3; d++) s->origin[d] = origin[d];
+    s->cart_size = (L + 1) * (L + 2) / 2;
+    s->cart_list = libgrpp_generate_shell_cartesians(L);
+    s->num_primitives = n;
+    s->coeffs = (double *)calloc(n > 0 ? n : 1, sizeof(double));
+    s->alpha = (double *)calloc(n > 0 ? n : 1, sizeof(double));
+    for (int i = 0; i < n; i++) {
+        s->coeffs[i] = coeffs[i];
+        s->alpha[i] = alpha[i];
+    }
+    return s;
+}
+
+libgrpp_shell_t *libgrpp_shell_deep_copy(libgrpp_shell_t *s)
+{
+    return libgrpp_new_shell(s->origin, s->L, s->num_primitives, s->coeffs, s->alpha);
+}
+
+void libgrpp_shell_shrink(libgrpp_shell_t *s)
+{
+    int n = 0;
+    for (int i = 0; i < s->num_primitives; i++)
+        if (std::fabs(s->coeffs[i]) > LIBGRPP_ZERO_THRESH) {
+            s->coeffs[n] = s->coeffs[i];
+            s->alpha[n] = s->alpha[i];
+            n++;
+        }
+    s->num_primitives = n;
+}
+
+void libgrpp_shell_mult_normcoef(libgrpp_shell_t *s)
+{
+    for (int i = 0; i < s->num_primitives; i++) s->coeffs[i] *= gaussian_norm(s->L, s->alpha[i]);
+}
+
+int libgrpp_get_shell_size(libgrpp_shell_t *s) { return s->cart_size; }
+
+void libgrpp_delete_shell(libgrpp_shell_t *s)
+{
+    if (!s) return;
+    free(s->cart_list);
+    free(s->coeffs);
+    free(s->alpha);
+    free(s);
+}
+
+// ============================================================ GRPP (grpp.c:15-109)
+libgrpp_grpp_t *libgrpp_new_grpp(void) { return (libgrpp_grpp_t *)calloc(1, sizeof(libgrpp_grpp_t)); }
+
+void libgrpp_grpp_set_local_potential(libgrpp_grpp_t *g, libgrpp_potential_t *p)
+{
+    if (g->U_L) libgrpp_delete_potential(g->U_L);
+    g->U_L = p;
+}
+
+void libgrpp_grpp_add_averaged_potential(libgrpp_grpp_t *g, libgrpp_potential_t *p)
+{
+    if (g->n_arep == 0) g->U_arep = (libgrpp_potential_t **)calloc(kMaxPots, sizeof(void *));
+    if (g->n_arep >= kMaxPots) {
+        grpp::set_error(LIBGRPP_B200_ERR_INVALID, "more than 100 averaged potentials");
+        return;
+    }
+    g->U_arep[g->n_arep++] = p;
+}
+
+void libgrpp_grpp_add_spin_orbit_potential(libgrpp_grpp_t *g, libgrpp_potential_t *p)
+{
+    if (g->n_esop == 0) g->U_esop = (libgrpp_potential_t **)calloc(kMaxPots, sizeof(void *));
+    if (g->n_esop >= kMaxPots) {
+        grpp::set_error(LIBGRPP_B200_ERR_INVALID, "more than 100 spin-orbit potentials");
+        return;
+    }
+    g->U_esop[g->n_esop++] = p;
+}
+
+void libgrpp_grpp_add_outercore_potential(libgrpp_grpp_t *g, libgrpp_potential_t *p, libgrpp_shell_t *s)
+{
+    if (g->n_oc_shells == 0) {
+        g->U_oc = (libgrpp_potential_t **)calloc(kMaxPots, sizeof(void *));
+        g->oc_shells = (libgrpp_shell_t **)calloc(kMaxPots, sizeof(void *));
+    }
+    if (g->n_oc_shells >= kMaxPots) {
+        grpp::set_error(LIBGRPP_B200_ERR_INVALID, "more than 100 outercore shells");
+        return;
+    }
+    g->U_oc[g->n_oc_shells] = p;
+    g->oc_shells[g->n_oc_shells] = s;
+    g->n_oc_shells++;
+}
+
+void libgrpp_delete_grpp(libgrpp_grpp_t *g)
+{
+    if (!g) return;
+    if (g->U_L) libgrpp_delete_potential(g->U_L);
+    for (int i = 0; i < g->n_arep; i++) libgrpp_delete_potential(g->U_arep[i]);
+    free(g->U_arep);
+    for (int i = 0; i < g->n_esop; i++) libgrpp_delete_potential(g->U_esop[i]);
+    free(g->U_esop);
+    for (int i = 0; i < g->n_oc_shells; i++) {
+        libgrpp_delete_potential(g->U_oc[i]);
+        libgrpp_delete_shell(g->oc_shells[i]);
+    }
+    free(g->U_oc);
+    free(g->oc_shells);
+    free(g);
+}
+
+// ============================================================ integrators
+static void one_task(libgrpp_shell_t *A, libgrpp_shell_t *B, const double *C, const libgrpp_potential_t *UL, int n_arep,
+                     libgrpp_potential_t *const *arep, int n_so, libgrpp_potential_t *const *so, int n_oc,
+                     libgrpp_potential_t *const *ocp, libgrpp_shell_t *const *ocs, int raw_so, double *o0, double *o1,
+                     double *o2, double *o3)
+{
+    const size_t n = (size_t)A->cart_size * B->cart_size;
+    double *outs[4] = {o0, o1, o2, o3};
+    for (double *o : outs)
+        if (o) memset(o, 0, n * sizeof(double));
+    if (!check_init()) return;
+    Builder bd;
+    const int a = bd.add_shell(A), b = bd.add_shell(B);
+    const int g = bd.add_grpp(UL, n_arep, arep, n_so, so, n_oc, ocp, ocs);
+    const int c = bd.add_centre(C, g);
+    bd.add_task(a, b, c);
+    std::vector<double> out[4];
+    if (run(bd, raw_so, out) != 0) return;
+    for (int k = 0; k < 4; k++)
+        if (outs[k]) memcpy(outs[k], out[k].data(), n * sizeof(double));
+}
+
+void libgrpp_type1_integrals(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, libgrpp_potential_t *pot, double *matrix)
+{
+    one_task(A, B, C, pot, 0, nullptr, 0, nullptr, 0, nullptr, nullptr, 0, matrix, nullptr, nullptr, nullptr);
+}
+
+void libgrpp_type2_integrals(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, libgrpp_potential_t *pot, double *matrix)
+{
+    one_task(A, B, C, nullptr, 1, &pot, 0, nullptr, 0, nullptr, nullptr, 0, matrix, nullptr, nullptr, nullptr);
+}
+
+void libgrpp_spin_orbit_integrals(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, libgrpp_potential_t *pot,
+                                  double *sx, double *sy, double *sz)
+{
+    one_task(A, B, C, nullptr, 0, nullptr, 1, &pot, 0, nullptr, nullptr, 1, nullptr, sx, sy, sz);
+}
+
+void libgrpp_outercore_potential_integrals(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, int noc,
+                                           libgrpp_potential_t **pots, libgrpp_shell_t **ocs, double *arep,
+                                           double *sx, double *sy, double *sz)
+{
+    one_task(A, B, C, nullptr, 0, nullptr, 0, nullptr, noc, pots, ocs, 0, arep, sx, sy, sz);
+}
+
+void libgrpp_full_grpp_integrals(libgrpp_shell_t *A, libgrpp_shell_t *B, libgrpp_grpp_t *g, double *C, double *arep,
+                                 double *sx, double *sy, double *sz)
+{
+    one_task(A, B, C, g->U_L, g->n_arep, g->U_arep, g->n_esop, g->U_esop, g->n_oc_shells, g->U_oc, g->oc_shells, 0, arep,
+             sx, sy, sz);
+}
+
+// ============================================================ gradients (grpp_integrals_gradient.c:123-393)
+void libgrpp_full_grpp_integrals_gradient(libgrpp_shell_t *A, libgrpp_shell_t *B, libgrpp_grpp_t *g, double *C,
+                                          double *D, double **ga, double **gx, double **gy, double **gz)
+{
+    gradient_impl(
+        A, B, C, D,
+        [&](Builder &bd) {
+            return bd.add_grpp(g->U_L, g->n_arep, g->U_arep, g->n_esop, g->U_esop, g->n_oc_shells, g->U_oc, g->oc_shells);
+        },
+        0, ga, gx, gy, gz);
+}
+
+void libgrpp_type1_integrals_gradient(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, libgrpp_potential_t *p,
+                                      double *D, double **ga)
+{
+    gradient_impl(
+        A, B, C, D, [&](Builder &bd) { return bd.add_grpp(p, 0, nullptr, 0, nullptr, 0, nullptr, nullptr); }, 0, ga,
+        nullptr, nullptr, nullptr);
+}
+
+void libgrpp_type2_integrals_gradient(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, libgrpp_potential_t *p,
+                                      double *D, double **ga)
+{
+    gradient_impl(
+        A, B, C, D, [&](Builder &bd) { return bd.add_grpp(nullptr, 1, &p, 0, nullptr, 0, nullptr, nullptr); }, 0, ga,
+        nullptr, nullptr, nullptr);
+}
+
+// the reference scales the full-GRPP result back by (2L+1)/2 (grpp_integrals_gradient.c:229-237);
+// here the spin-orbit blocks are produced without the factor in the first place
+void libgrpp_spin_orbit_integrals_gradient(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, libgrpp_potential_t *p,
+                                           double *D, double **gx, double **gy, double **gz)
+{
+    gradient_impl(
+        A, B, C, D, [&](Builder &bd) { return bd.add_grpp(nullptr, 0, nullptr, 1, &p, 0, nullptr, nullptr); }, 1,
+        nullptr, gx, gy, gz);
+}
+
+void libgrpp_outercore_potential_integrals_gradient(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, int noc,
+                                                    libgrpp_potential_t **pots, libgrpp_shell_t **ocs, double *D,
+                                                    double **ga, double **gx, double **gy, double **gz)
+{
+    gradient_impl(
+        A, B, C, D, [&](Builder &bd) { return bd.add_grpp(nullptr, 0, nullptr, 0, nullptr, noc, pots, ocs); }, 0, ga,
+        gx, gy, gz);
+}
+
+// ============================================================ batched API (libgrpp_b200.h)
+int libgrpp_b200_last_error(void) { return grpp::last_error(); }
+const char *libgrpp_b200_last_error_message(void) { return grpp::last_error_message(); }
+
+int64_t libgrpp_b200_batch_output_size(const libgrpp_b200_batch_t *b) { return grpp::batch_output_size(b); }
+
+int libgrpp_b200_full_grpp_batch(const libgrpp_b200_batch_t *b, int radial_mode, double *arep, double *sx, double *sy,
+                                 double *sz)
+{
+    if (!check_init()) return LIBGRPP_B200_ERR_NOT_INIT;
+    grpp::RunOptions opt;
+    opt.radial_mode = radial_mode;
+    return grpp::run_full_batch(b, opt, arep, sx, sy, sz);
+}
+
+}  // extern "C"
+#pragma GCC visibility pop

@@ -1,0 +1,749 @@
+// GRPP engine: the single CUDA translation unit (device tables, kernels, host
+// orchestration of a batch of (shell A, shell B, centre C) tasks).
+//
+// Pipeline of one batch, all on one stream:
+//   1. atab_kernel    k-independent angular tensors, cached per device and (L, l)
+//   2. mmd_kernel     type 1 blocks <A|U_L|B> written straight into the arep output,
+//                     and <S|U_oc|oc>, <S|oc> Cartesian blocks for every (shell, centre)
+//                     that needs outercore projections
+//   3. oc_proj_kernel Cartesian -> real spherical transform of those blocks
+//   4. radial_kernel  Q tables of every semilocal potential of every task
+//   5. final_kernel   per task: T1 + sum type 2 + sum 2/(2L+1) SO + outercore, in
+//                     libgrpp_full_grpp_integrals' accumulation order
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "grpp_common.cuh"
+#include "specfunc.cuh"
+#include "mmd.cuh"
+#include "radial.cuh"
+#include "angular.cuh"
+#include "tables.h"
+#include "engine.h"
+
+namespace grpp {
+
+// ------------------------------------------------------------------ errors
+namespace {
+thread_local int t_err = 0;
+thread_local std::string t_msg;
+}  // namespace
+
+void set_error(int code, const std::string &msg)
+{
+    t_err = code;
+    t_msg = msg;
+}
+int last_error() { return t_err; }
+const char *last_error_message() { return t_msg.c_str(); }
+
+#define GRPP_CUDA(call)                                                                           \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            set_error(LIBGRPP_B200_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+            return LIBGRPP_B200_ERR_CUDA;                                                         \
+        }                                                                                         \
+    } while (0)
+
+// ------------------------------------------------------------------ device state
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n)
+    {
+        if (n <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(n, 1 << 20);
+        want = want + want / 4;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+};
+
+struct DeviceState {
+    int device = -1;
+    bool ready = false;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[6];
+    std::vector<void *> table_bufs;
+    DevBuf in, scratch, out;
+    DevBuf atab;
+    size_t atab_used = 0;
+    std::vector<int64_t> atab_off;
+    DevBuf atab_off_dev;
+    std::mutex mu;
+};
+
+std::mutex g_state_mu;
+DeviceState g_states[64];
+HostTables g_host;
+bool g_host_ready = false;
+
+template <typename T>
+cudaError_t upload_vec(DeviceState &st, const std::vector<T> &v, const T **out)
+{
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(v.size(), 1) * sizeof(T));
+    if (e != cudaSuccess) return e;
+    st.table_bufs.push_back(p);
+    if (!v.empty()) e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    *out = (const T *)p;
+    return e;
+}
+
+int init_device_state(DeviceState &st, int device)
+{
+    if (!g_host_ready) {
+        build_host_tables(g_host);
+        g_host_ready = true;
+    }
+    const HostTables &h = g_host;
+    DeviceTables d;
+    GRPP_CUDA(upload_vec(st, h.bessel, &d.bessel));
+    GRPP_CUDA(upload_vec(st, h.rfun, &d.rfun));
+    GRPP_CUDA(upload_vec(st, h.boys, &d.boys));
+    GRPP_CUDA(upload_vec(st, h.dawson, &d.dawson));
+    GRPP_CUDA(upload_vec(st, h.rsh_coef, &d.rsh_coef));
+    GRPP_CUDA(upload_vec(st, h.rsh_off, &d.rsh_off));
+    GRPP_CUDA(upload_vec(st, h.rsh_comb, &d.rsh_comb));
+    GRPP_CUDA(upload_vec(st, h.rsh_comb_off, &d.rsh_comb_off));
+    GRPP_CUDA(upload_vec(st, h.lmat, &d.lmat));
+    GRPP_CUDA(upload_vec(st, h.lmat_off, &d.lmat_off));
+    GRPP_CUDA(upload_vec(st, h.dfact, &d.dfact));
+    GRPP_CUDA(upload_vec(st, h.binom, &d.binom));
+    GRPP_CUDA(cudaMemcpyToSymbol(c_tab, &d, sizeof(d)));
+    GRPP_CUDA(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking));
+    for (auto &e : st.ev) GRPP_CUDA(cudaEventCreate(&e));
+    st.atab_off.assign((kMaxL + 2) * (kMaxL + 2), -1);
+    GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(radial_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(radial_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    st.device = device;
+    st.ready = true;
+    return 0;
+}
+
+DeviceState *get_state(int &rc)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        set_error(LIBGRPP_B200_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+        rc = LIBGRPP_B200_ERR_CUDA;
+        return nullptr;
+    }
+    if (dev < 0 || dev >= 64) {
+        set_error(LIBGRPP_B200_ERR_CUDA, "device index out of range");
+        rc = LIBGRPP_B200_ERR_CUDA;
+        return nullptr;
+    }
+    DeviceState &st = g_states[dev];
+    std::lock_guard<std::mutex> lk(g_state_mu);
+    if (!st.ready) {
+        rc = init_device_state(st, dev);
+        if (rc) return nullptr;
+    }
+    rc = 0;
+    return &st;
+}
+
+// ------------------------------------------------------------------ host packing
+struct Packer {
+    std::vector<char> buf;
+    template <typename T>
+    size_t add(const std::vector<T> &v)
+    {
+        size_t off = (buf.size() + 255) & ~size_t(255);
+        buf.resize(off + std::max<size_t>(v.size(), 1) * sizeof(T));
+        if (!v.empty()) memcpy(buf.data() + off, v.data(), v.size() * sizeof(T));
+        return off;
+    }
+};
+
+template <typename T>
+T *at(void *base, size_t off)
+{
+    return (T *)((char *)base + off);
+}
+
+double host_gaussian_norm(int L, double a) { return std::pow(2 * a / kPi, 0.75) * std::pow(4 * a, 0.5 * L); }
+
+double host_dfact(int n)
+{
+    double r = 1.0;
+    for (int k = n; k > 1; k -= 2) r *= k;
+    return r;
+}
+
+double host_factorial(int n)
+{
+    double r = 1.0;
+    for (int k = 2; k <= n; k++) r *= k;
+    return r;
+}
+
+// outercore_integrals.c:481-510: sqrt(2^(L+5/2) / Gamma(L+3/2)) alpha^(3/4+L/2)
+double radial_gto_norm(int L, double alpha)
+{
+    const double g = host_dfact(2 * L + 1) * std::sqrt(kPi) / std::pow(2.0, L + 1);
+    return std::sqrt(std::pow(2.0, L + 2.5) / g) * std::pow(alpha, 0.75 + L / 2.0);
+}
+
+// outercore_integrals.c:457-478
+double one_centre_prim(int L, double a1, double a2, int n, double zeta)
+{
+    const double a = a1 + a2 + zeta;
+    if (n % 2 == 0) {
+        const int k = L + n / 2;
+        return host_dfact(2 * k - 1) / (std::pow(2.0, k + 1) * std::pow(a, k)) * std::sqrt(kPi / a);
+    }
+    const int k = L + (n - 1) / 2;
+    return host_factorial(k) / (2.0 * std::pow(a, k + 1));
+}
+
+struct PotView {
+    int L, J;
+    std::vector<int> pw;
+    std::vector<double> c, a;
+};
+struct ShellView {
+    int L;
+    std::vector<double> c, a;
+};
+
+// outercore_integrals.c:397-450: delta = (U1 + U2)/2, Uk = <oc1| U_k |oc2> one-centre analytic
+double delta_integral(const PotView &p1, const ShellView &s1, const PotView &p2, const ShellView &s2)
+{
+    if (p1.L != p2.L || p1.J != p2.J) return 0.0;
+    auto U = [&](const PotView &p) {
+        double sum = 0.0;
+        const int L = p.L;
+        for (size_t i = 0; i < s1.a.size(); i++) {
+            const double Ni = radial_gto_norm(L, s1.a[i]);
+            for (size_t j = 0; j < s2.a.size(); j++) {
+                const double Nj = radial_gto_norm(L, s2.a[j]);
+                const double f = Ni * Nj * s1.c[i] * s2.c[j];
+                for (size_t k = 0; k < p.a.size(); k++) sum += f * p.c[k] * one_centre_prim(L, s1.a[i], s2.a[j], p.pw[k], p.a[k]);
+            }
+        }
+        return sum;
+    };
+    return 0.5 * (U(p1) + U(p2));
+}
+
+int ensure_atab(DeviceState &st, int L, int l)
+{
+    const int key = L * (kMaxL + 2) + l;
+    if (st.atab_off[key] >= 0) return 0;
+    const int64_t sz = atab_size(L, l);
+    const size_t need = (st.atab_used + sz) * sizeof(double);
+    if (need > st.atab.cap) {
+        void *old = st.atab.p;
+        void *np = nullptr;
+        size_t want = std::max(need * 2, (size_t)8 << 20);
+        GRPP_CUDA(cudaMalloc(&np, want));
+        if (old) {
+            GRPP_CUDA(cudaMemcpyAsync(np, old, st.atab_used * sizeof(double), cudaMemcpyDeviceToDevice, st.stream));
+            GRPP_CUDA(cudaStreamSynchronize(st.stream));
+            cudaFree(old);
+        }
+        st.atab.p = np;
+        st.atab.cap = want;
+    }
+    double *dst = (double *)st.atab.p + st.atab_used;
+    const int threads = 256;
+    const int blocks = (int)std::min<int64_t>((sz + threads - 1) / threads, 4096);
+    atab_kernel<<<std::max(blocks, 1), threads, 0, st.stream>>>(L, l, dst);
+    GRPP_CUDA(cudaGetLastError());
+    st.atab_off[key] = (int64_t)st.atab_used;
+    st.atab_used += sz;
+    return 0;
+}
+
+}  // namespace
+
+int64_t batch_output_size(const libgrpp_b200_batch_t *b)
+{
+    int64_t n = 0;
+    for (int64_t t = 0; t < b->n_tasks; t++) n += (int64_t)ncart(b->shell_L[b->task_a[t]]) * ncart(b->shell_L[b->task_b[t]]);
+    return n;
+}
+
+#define CHECK_INPUT(cond, msg)                               \
+    do {                                                     \
+        if (!(cond)) {                                       \
+            set_error(LIBGRPP_B200_ERR_INVALID, (msg));      \
+            return LIBGRPP_B200_ERR_INVALID;                 \
+        }                                                    \
+    } while (0)
+
+int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double *h_arep, double *h_sx, double *h_sy,
+                   double *h_sz, RunStats *stats)
+{
+    set_error(0, "");
+    int rc = 0;
+    DeviceState *stp = get_state(rc);
+    if (!stp) return rc;
+    DeviceState &st = *stp;
+    std::lock_guard<std::mutex> lk(st.mu);
+    cudaStream_t s = st.stream;
+    const int64_t nt = b->n_tasks;
+    if (nt == 0) return 0;
+
+    // ---------------------------------------------------------------- validation
+    CHECK_INPUT(b->n_shells > 0 && b->n_centres > 0 && b->n_grpps > 0, "empty batch description");
+    for (int i = 0; i < b->n_shells; i++) {
+        CHECK_INPUT(b->shell_L[i] >= 0 && b->shell_L[i] <= kMaxL, "shell angular momentum outside 0..10");
+        CHECK_INPUT(b->shell_nprim[i] >= 0 && b->shell_nprim[i] <= kRadMaxPrims, "more than 64 primitives in a shell");
+    }
+    for (int p = 0; p < b->n_pots; p++) {
+        CHECK_INPUT(b->pot_L[p] >= 0 && b->pot_L[p] <= kMaxL, "potential angular momentum outside 0..10");
+        for (int k = 0; k < b->pot_nprim[p]; k++) {
+            const int n = b->pot_powers[b->pot_prim_off[p] + k];
+            CHECK_INPUT(n >= 0 && n <= 2, "potential power n must be 0, 1 or 2");
+        }
+    }
+    for (int64_t t = 0; t < nt; t++) {
+        CHECK_INPUT(b->task_a[t] >= 0 && b->task_a[t] < b->n_shells && b->task_b[t] >= 0 && b->task_b[t] < b->n_shells &&
+                        b->task_c[t] >= 0 && b->task_c[t] < b->n_centres,
+                    "task index out of range");
+    }
+    for (int c = 0; c < b->n_centres; c++) CHECK_INPUT(b->centre_grpp[c] >= 0 && b->centre_grpp[c] < b->n_grpps, "centre GRPP index out of range");
+
+    // ---------------------------------------------------------------- shells
+    const int ns = b->n_shells;
+    std::vector<int> sh_L(b->shell_L, b->shell_L + ns), sh_np(b->shell_nprim, b->shell_nprim + ns),
+        sh_po(b->shell_prim_off, b->shell_prim_off + ns), sh_co(ns);
+    int total_prims = 0;
+    for (int i = 0; i < ns; i++) total_prims = std::max(total_prims, sh_po[i] + sh_np[i]);
+    std::vector<double> pc(b->prim_coef, b->prim_coef + total_prims), pa(b->prim_alpha, b->prim_alpha + total_prims);
+    std::vector<double> sh_or(b->shell_origin, b->shell_origin + 3 * ns);
+    std::vector<int8_t> cart;
+    for (int i = 0; i < ns; i++) {
+        sh_co[i] = (int)(cart.size() / 3);
+        const int nc = ncart(sh_L[i]);
+        for (int q = 0; q < 3 * nc; q++) {
+            const int v = b->cart_list[3 * b->shell_cart_off[i] + q];
+            CHECK_INPUT(v >= 0 && v <= sh_L[i], "invalid Cartesian component list");
+            cart.push_back((int8_t)v);
+        }
+    }
+    // radial-path primitives: shrunk and normalised (radial_type2_integral.c:164-172)
+    std::vector<int> rp_off(ns), rp_n(ns);
+    std::vector<double> rp_c, rp_a;
+    for (int i = 0; i < ns; i++) {
+        rp_off[i] = (int)rp_c.size();
+        for (int k = 0; k < sh_np[i]; k++) {
+            const double c = pc[sh_po[i] + k], a = pa[sh_po[i] + k];
+            if (std::fabs(c) > kZeroThresh) {
+                rp_c.push_back(c * host_gaussian_norm(sh_L[i], a));
+                rp_a.push_back(a);
+            }
+        }
+        rp_n[i] = (int)rp_c.size() - rp_off[i];
+    }
+
+    // ---------------------------------------------------------------- potentials (|c| < 1e-14 dropped, potential.c:31-42)
+    const int np = b->n_pots;
+    std::vector<int> p_L(np), p_n(np), p_off(np), p_pw;
+    std::vector<double> p_c, p_a;
+    std::vector<PotView> pview(np);
+    for (int p = 0; p < np; p++) {
+        p_L[p] = b->pot_L[p];
+        p_off[p] = (int)p_c.size();
+        pview[p].L = b->pot_L[p];
+        pview[p].J = b->pot_J[p];
+        for (int k = 0; k < b->pot_nprim[p]; k++) {
+            const int o = b->pot_prim_off[p] + k;
+            if (std::fabs(b->pot_coef[o]) < kZeroThresh) continue;
+            p_pw.push_back(b->pot_powers[o]);
+            p_c.push_back(b->pot_coef[o]);
+            p_a.push_back(b->pot_alpha[o]);
+            pview[p].pw.push_back(b->pot_powers[o]);
+            pview[p].c.push_back(b->pot_coef[o]);
+            pview[p].a.push_back(b->pot_alpha[o]);
+        }
+        p_n[p] = (int)p_c.size() - p_off[p];
+    }
+
+    // ---------------------------------------------------------------- GRPP operators
+    const int ng = b->n_grpps;
+    std::vector<int> g_sl_off(ng), g_sl_n(ng), g_n_arep(ng), sl_pot, g_oc_off(ng), g_n_oc(ng), oc_L, oc_J, oc_pot,
+        oc_shell, g_delta_off(ng);
+    std::vector<double> deltas;
+    for (int g = 0; g < ng; g++) {
+        g_sl_off[g] = (int)sl_pot.size();
+        for (int i = 0; i < b->grpp_n_arep[g]; i++) sl_pot.push_back(b->grpp_pot_list[b->grpp_arep_off[g] + i]);
+        for (int i = 0; i < b->grpp_n_so[g]; i++) sl_pot.push_back(b->grpp_pot_list[b->grpp_so_off[g] + i]);
+        g_n_arep[g] = b->grpp_n_arep[g];
+        g_sl_n[g] = (int)sl_pot.size() - g_sl_off[g];
+        CHECK_INPUT(g_sl_n[g] <= kRadMaxPots, "more than 24 semilocal potentials in one GRPP");
+        int nterm = 0;
+        for (int i = g_sl_off[g]; i < g_sl_off[g] + g_sl_n[g]; i++) nterm += p_n[sl_pot[i]];
+        CHECK_INPUT(nterm <= kRadMaxTerms, "more than 256 semilocal potential terms in one GRPP");
+        g_oc_off[g] = (int)oc_L.size();
+        g_n_oc[g] = b->grpp_n_oc[g];
+        CHECK_INPUT(g_n_oc[g] <= kFinMaxOc, "more than 32 outercore shells in one GRPP");
+        for (int i = 0; i < g_n_oc[g]; i++) {
+            const int k = b->grpp_oc_off[g] + i;
+            const int pp = b->grpp_oc_pot[k], so = b->grpp_oc_shell[k];
+            CHECK_INPUT(sh_L[so] == p_L[pp], "outercore shell and potential differ in L");
+            oc_L.push_back(sh_L[so]);
+            oc_J.push_back(b->pot_J[pp]);
+            oc_pot.push_back(pp);
+            oc_shell.push_back(so);
+        }
+        g_delta_off[g] = (int)deltas.size();
+        const int n = g_n_oc[g];
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                const int ki = g_oc_off[g] + i, kj = g_oc_off[g] + j;
+                ShellView si{sh_L[oc_shell[ki]], {}, {}}, sj{sh_L[oc_shell[kj]], {}, {}};
+                for (int q = 0; q < sh_np[oc_shell[ki]]; q++) {
+                    si.c.push_back(pc[sh_po[oc_shell[ki]] + q]);
+                    si.a.push_back(pa[sh_po[oc_shell[ki]] + q]);
+                }
+                for (int q = 0; q < sh_np[oc_shell[kj]]; q++) {
+                    sj.c.push_back(pc[sh_po[oc_shell[kj]] + q]);
+                    sj.a.push_back(pa[sh_po[oc_shell[kj]] + q]);
+                }
+                deltas.push_back(delta_integral(pview[oc_pot[ki]], si, pview[oc_pot[kj]], sj));
+            }
+    }
+
+    // ---------------------------------------------------------------- tasks and work lists
+    std::vector<int> ta(b->task_a, b->task_a + nt), tb(b->task_b, b->task_b + nt), tc(b->task_c, b->task_c + nt);
+    std::vector<int64_t> out_off(nt + 1), q_off(nt, -1);
+    std::vector<uint8_t> has_ul(nt, 0);
+    std::vector<int> proj_a(nt, -1), proj_b(nt, -1);
+    std::vector<MmdItem> items;
+    std::vector<int> rad_task;
+    std::vector<int64_t> rad_qoff;
+    int64_t qtot = 0;
+    out_off[0] = 0;
+    int mmd_lmax = 0, mmd_smax = 0;
+    int rad_l1 = 0, rad_l2 = 0, rad_dn = 1, rad_npot = 0;
+    int fin_lam = 0, fin_nq = 1;
+    std::map<std::pair<int, int>, int> proj_map;
+    std::vector<std::pair<int, int>> projs;
+    std::vector<std::pair<int, int>> atab_need;
+    for (int64_t t = 0; t < nt; t++) {
+        const int A = ta[t], B = tb[t], C = tc[t], g = b->centre_grpp[C];
+        const int la = sh_L[A], lb = sh_L[B];
+        CHECK_INPUT(sh_np[A] >= 1 && sh_np[B] >= 1, "a shell of a task has no primitives");
+        CHECK_INPUT(ncart(la) * ncart(lb) <= kFinThreads * kFinElemPerThread, "shell pair block larger than 1024 Cartesian pairs");
+        out_off[t + 1] = out_off[t] + (int64_t)ncart(la) * ncart(lb);
+        if (b->grpp_UL[g] >= 0 && p_n[b->grpp_UL[g]] > 0) {
+            has_ul[t] = 1;
+            MmdItem it{A, B, 0, C, b->grpp_UL[g], 0, out_off[t]};
+            items.push_back(it);
+            mmd_lmax = std::max(mmd_lmax, std::max(la, lb));
+            mmd_smax = std::max(mmd_smax, la + lb);
+        }
+        if (g_sl_n[g] > 0) {
+            q_off[t] = qtot;
+            rad_task.push_back((int)t);
+            rad_qoff.push_back(qtot);
+            int e = 0;
+            for (int i = 0; i < g_sl_n[g]; i++) {
+                const int L = p_L[sl_pot[g_sl_off[g] + i]];
+                e += (L + la + 1) * (L + lb + 1) * (la + lb + 1);
+                rad_l1 = std::max(rad_l1, L + la);
+                rad_l2 = std::max(rad_l2, L + lb);
+                fin_lam = std::max(fin_lam, L + std::max(la, lb));
+                fin_nq = std::max(fin_nq, (L + la + 1) * (L + lb + 1) * (la + lb + 1));
+                atab_need.push_back({L, la});
+                atab_need.push_back({L, lb});
+            }
+            CHECK_INPUT(e <= kRadMaxEntries, "radial table larger than 16384 entries for one task");
+            CHECK_INPUT(std::max(rad_l1, rad_l2) <= kRadMaxLam && la + lb + 1 <= kRadMaxN, "angular momentum too high for the radial path");
+            qtot += e;
+            rad_dn = std::max(rad_dn, la + lb + 1);
+            rad_npot = std::max(rad_npot, g_sl_n[g]);
+        }
+        if (g_n_oc[g] > 0) {
+            for (int side = 0; side < 2; side++) {
+                const int S = side ? B : A;
+                auto key = std::make_pair(S, C);
+                auto itp = proj_map.find(key);
+                int idx;
+                if (itp == proj_map.end()) {
+                    idx = (int)projs.size();
+                    proj_map[key] = idx;
+                    projs.push_back(key);
+                } else {
+                    idx = itp->second;
+                }
+                (side ? proj_b : proj_a)[t] = idx;
+            }
+        }
+    }
+    // outercore projection blocks
+    std::vector<int> blk_shell, blk_oc;
+    std::vector<int64_t> blk_cart_off, blk_sph_off, proj_off(projs.size() + 1, 0);
+    int64_t cart_tot = 0, sph_tot = 0;
+    for (size_t pi = 0; pi < projs.size(); pi++) {
+        const int S = projs[pi].first, C = projs[pi].second, g = b->centre_grpp[C];
+        proj_off[pi] = sph_tot;
+        for (int k = 0; k < g_n_oc[g]; k++) {
+            const int ko = g_oc_off[g] + k, osh = oc_shell[ko], L = oc_L[ko];
+            blk_shell.push_back(S);
+            blk_oc.push_back(osh);
+            blk_cart_off.push_back(cart_tot);
+            blk_sph_off.push_back(sph_tot);
+            items.push_back(MmdItem{S, osh, 1, C, oc_pot[ko], 1, cart_tot});
+            items.push_back(MmdItem{S, osh, 1, C, -1, 2, cart_tot});
+            mmd_lmax = std::max(mmd_lmax, std::max(sh_L[S], L));
+            mmd_smax = std::max(mmd_smax, sh_L[S] + L);
+            cart_tot += (int64_t)ncart(sh_L[S]) * ncart(L);
+            sph_tot += (int64_t)ncart(sh_L[S]) * (2 * L + 1);
+        }
+    }
+    proj_off[projs.size()] = sph_tot;
+    const int64_t out_tot = out_off[nt];
+
+    // angular tensors
+    std::sort(atab_need.begin(), atab_need.end());
+    atab_need.erase(std::unique(atab_need.begin(), atab_need.end()), atab_need.end());
+    for (auto &lp : atab_need) {
+        rc = ensure_atab(st, lp.first, lp.second);
+        if (rc) return rc;
+    }
+    GRPP_CUDA(st.atab_off_dev.ensure(st.atab_off.size() * sizeof(int64_t)));
+    GRPP_CUDA(cudaMemcpyAsync(st.atab_off_dev.p, st.atab_off.data(), st.atab_off.size() * sizeof(int64_t),
+                              cudaMemcpyHostToDevice, s));
+
+    // ---------------------------------------------------------------- upload
+    std::vector<int> sh_po_v(sh_po), cart_off_v(sh_co);
+    std::vector<double> c_or(b->centre_origin, b->centre_origin + 3 * b->n_centres);
+    std::vector<int> c_g(b->centre_grpp, b->centre_grpp + b->n_centres);
+    Packer pk;
+    const size_t o_shL = pk.add(sh_L), o_shnp = pk.add(sh_np), o_shpo = pk.add(sh_po_v), o_shco = pk.add(cart_off_v);
+    const size_t o_pc = pk.add(pc), o_pa = pk.add(pa), o_sor = pk.add(sh_or), o_cart = pk.add(cart);
+    const size_t o_rpo = pk.add(rp_off), o_rpn = pk.add(rp_n), o_rpc = pk.add(rp_c), o_rpa = pk.add(rp_a);
+    const size_t o_pL = pk.add(p_L), o_pn = pk.add(p_n), o_poff = pk.add(p_off), o_ppw = pk.add(p_pw), o_pcoef = pk.add(p_c),
+                 o_palpha = pk.add(p_a);
+    const size_t o_gslo = pk.add(g_sl_off), o_gsln = pk.add(g_sl_n), o_gnar = pk.add(g_n_arep), o_slp = pk.add(sl_pot);
+    const size_t o_goco = pk.add(g_oc_off), o_gnoc = pk.add(g_n_oc), o_ocL = pk.add(oc_L), o_ocJ = pk.add(oc_J),
+                 o_gdo = pk.add(g_delta_off), o_del = pk.add(deltas);
+    const size_t o_cor = pk.add(c_or), o_cg = pk.add(c_g);
+    const size_t o_ta = pk.add(ta), o_tb = pk.add(tb), o_tc = pk.add(tc), o_too = pk.add(out_off), o_thul = pk.add(has_ul),
+                 o_tqo = pk.add(q_off), o_tpa = pk.add(proj_a), o_tpb = pk.add(proj_b);
+    const size_t o_items = pk.add(items), o_rt = pk.add(rad_task), o_rq = pk.add(rad_qoff);
+    const size_t o_bs = pk.add(blk_shell), o_bo = pk.add(blk_oc), o_bco = pk.add(blk_cart_off), o_bso = pk.add(blk_sph_off),
+                 o_poffp = pk.add(proj_off);
+    std::vector<int8_t> stop_dummy;
+    GRPP_CUDA(st.in.ensure(pk.buf.size()));
+    GRPP_CUDA(cudaMemcpyAsync(st.in.p, pk.buf.data(), pk.buf.size(), cudaMemcpyHostToDevice, s));
+    void *ib = st.in.p;
+
+    // scratch: Q, S_prev, scr | S_cart, U_cart | S_sph, U_sph | status ; outputs: 4 x out_tot
+    const int64_t qn = std::max<int64_t>(qtot, 1), cn = std::max<int64_t>(cart_tot, 1), sn = std::max<int64_t>(sph_tot, 1);
+    const size_t scratch_bytes = (size_t)(3 * qn + 2 * cn + 2 * sn + 16) * sizeof(double);
+    GRPP_CUDA(st.scratch.ensure(scratch_bytes));
+    GRPP_CUDA(st.out.ensure((size_t)4 * std::max<int64_t>(out_tot, 1) * sizeof(double)));
+    double *Qd = (double *)st.scratch.p, *Spd = Qd + qn, *SCd = Spd + qn, *Scd = SCd + qn, *Ucd = Scd + cn, *Ssd = Ucd + cn,
+           *Usd = Ssd + sn;
+    int *statusd = (int *)(Usd + sn);
+    GRPP_CUDA(cudaMemsetAsync(statusd, 0, 16 * sizeof(int), s));
+    double *o_arep = (double *)st.out.p, *o_sx = o_arep + out_tot, *o_sy = o_sx + out_tot, *o_sz = o_sy + out_tot;
+
+    int nsm = 0;
+    GRPP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, st.device));
+    GRPP_CUDA(cudaEventRecord(st.ev[0], s));
+
+    // ---------------------------------------------------------------- 2. MMD
+    if (!items.empty()) {
+        MmdArgs m;
+        m.items = at<MmdItem>(ib, o_items);
+        m.n_items = (int)items.size();
+        m.shell_L = at<int>(ib, o_shL);
+        m.shell_nprim = at<int>(ib, o_shnp);
+        m.shell_prim_off = at<int>(ib, o_shpo);
+        m.shell_cart_off = at<int>(ib, o_shco);
+        m.prim_coef = at<double>(ib, o_pc);
+        m.prim_alpha = at<double>(ib, o_pa);
+        m.shell_origin = at<double>(ib, o_sor);
+        m.cart = at<int8_t>(ib, o_cart);
+        m.pot_nprim = at<int>(ib, o_pn);
+        m.pot_prim_off = at<int>(ib, o_poff);
+        m.pot_powers = at<int>(ib, o_ppw);
+        m.pot_coef = at<double>(ib, o_pcoef);
+        m.pot_alpha = at<double>(ib, o_palpha);
+        m.centre_origin = at<double>(ib, o_cor);
+        m.out[0] = o_arep;
+        m.out[1] = Ucd;
+        m.out[2] = Scd;
+        m.lmax = mmd_lmax;
+        m.smax = mmd_smax;
+        m.status = statusd;
+        const int wpb = 4;
+        const size_t smem = (size_t)wpb * mmd_ws_size(mmd_lmax, mmd_smax) * sizeof(double);
+        const int blocks = (int)std::min<int64_t>(((int64_t)items.size() + wpb - 1) / wpb, (int64_t)nsm * 16);
+        mmd_kernel<<<blocks, 32 * wpb, smem, s>>>(m);
+        GRPP_CUDA(cudaGetLastError());
+    }
+    GRPP_CUDA(cudaEventRecord(st.ev[1], s));
+
+    // ---------------------------------------------------------------- 3. outercore projections
+    if (!blk_shell.empty()) {
+        OcProjArgs o;
+        o.n = (int)blk_shell.size();
+        o.blk_shell = at<int>(ib, o_bs);
+        o.blk_ocshell = at<int>(ib, o_bo);
+        o.blk_cart_off = at<int64_t>(ib, o_bco);
+        o.blk_sph_off = at<int64_t>(ib, o_bso);
+        o.shell_L = at<int>(ib, o_shL);
+        o.shell_cart_off = at<int>(ib, o_shco);
+        o.cart = at<int8_t>(ib, o_cart);
+        o.S_cart = Scd;
+        o.U_cart = Ucd;
+        o.S_sph = Ssd;
+        o.U_sph = Usd;
+        oc_proj_kernel<<<(int)std::min<size_t>(blk_shell.size(), (size_t)nsm * 32), 64, 0, s>>>(o);
+        GRPP_CUDA(cudaGetLastError());
+    }
+
+    // ---------------------------------------------------------------- 4. radial
+    if (!rad_task.empty()) {
+        RadialArgs r;
+        r.n_items = (int)rad_task.size();
+        r.item_task = at<int>(ib, o_rt);
+        r.task_a = at<int>(ib, o_ta);
+        r.task_b = at<int>(ib, o_tb);
+        r.task_c = at<int>(ib, o_tc);
+        r.shell_L = at<int>(ib, o_shL);
+        r.shell_origin = at<double>(ib, o_sor);
+        r.rp_off = at<int>(ib, o_rpo);
+        r.rp_n = at<int>(ib, o_rpn);
+        r.rp_coef = at<double>(ib, o_rpc);
+        r.rp_alpha = at<double>(ib, o_rpa);
+        r.shell_nprim = at<int>(ib, o_shnp);
+        r.shell_prim_off = at<int>(ib, o_shpo);
+        r.prim_coef = at<double>(ib, o_pc);
+        r.prim_alpha = at<double>(ib, o_pa);
+        r.centre_origin = at<double>(ib, o_cor);
+        r.centre_grpp = at<int>(ib, o_cg);
+        r.grpp_sl_off = at<int>(ib, o_gslo);
+        r.grpp_sl_n = at<int>(ib, o_gsln);
+        r.sl_pot = at<int>(ib, o_slp);
+        r.pot_L = at<int>(ib, o_pL);
+        r.pot_nprim = at<int>(ib, o_pn);
+        r.pot_prim_off = at<int>(ib, o_poff);
+        r.pot_powers = at<int>(ib, o_ppw);
+        r.pot_coef = at<double>(ib, o_pcoef);
+        r.pot_alpha = at<double>(ib, o_palpha);
+        r.q_off = at<int64_t>(ib, o_rq);
+        r.Q = Qd;
+        r.S_prev = Spd;
+        r.scr = SCd;
+        r.stop_level = nullptr;
+        r.pred_level = nullptr;
+        r.fallback_count = statusd + 4;
+        r.status = statusd;
+        const size_t smem = (size_t)(1 + rad_npot + (rad_l1 + 1) + (rad_l2 + 1) + rad_dn) * kRadThreads * sizeof(double);
+        const int blocks = (int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 8);
+        radial_kernel<false><<<blocks, kRadThreads, smem, s>>>(r);
+        GRPP_CUDA(cudaGetLastError());
+    }
+    GRPP_CUDA(cudaEventRecord(st.ev[2], s));
+
+    // ---------------------------------------------------------------- 5. final assembly
+    {
+        FinalArgs f;
+        f.n_tasks = (int)nt;
+        f.task_a = at<int>(ib, o_ta);
+        f.task_b = at<int>(ib, o_tb);
+        f.task_c = at<int>(ib, o_tc);
+        f.task_out_off = at<int64_t>(ib, o_too);
+        f.task_has_ul = at<uint8_t>(ib, o_thul);
+        f.task_q_off = at<int64_t>(ib, o_tqo);
+        f.task_proj_a = at<int>(ib, o_tpa);
+        f.task_proj_b = at<int>(ib, o_tpb);
+        f.shell_L = at<int>(ib, o_shL);
+        f.shell_cart_off = at<int>(ib, o_shco);
+        f.shell_prim_off = at<int>(ib, o_shpo);
+        f.prim_alpha = at<double>(ib, o_pa);
+        f.shell_origin = at<double>(ib, o_sor);
+        f.cart = at<int8_t>(ib, o_cart);
+        f.centre_origin = at<double>(ib, o_cor);
+        f.centre_grpp = at<int>(ib, o_cg);
+        f.grpp_sl_off = at<int>(ib, o_gslo);
+        f.grpp_sl_n = at<int>(ib, o_gsln);
+        f.grpp_n_arep = at<int>(ib, o_gnar);
+        f.sl_pot = at<int>(ib, o_slp);
+        f.grpp_oc_off = at<int>(ib, o_goco);
+        f.grpp_n_oc = at<int>(ib, o_gnoc);
+        f.oc_L = at<int>(ib, o_ocL);
+        f.oc_J = at<int>(ib, o_ocJ);
+        f.oc_delta = at<double>(ib, o_del);
+        f.grpp_delta_off = at<int>(ib, o_gdo);
+        f.pot_L = at<int>(ib, o_pL);
+        f.Q = Qd;
+        f.atab_off = (const int64_t *)st.atab_off_dev.p;
+        f.atab = (const double *)st.atab.p;
+        f.proj_off = at<int64_t>(ib, o_poffp);
+        f.S_sph = Ssd;
+        f.U_sph = Usd;
+        f.raw_so = opt.raw_so;
+        f.arep = o_arep;
+        f.so_x = o_sx;
+        f.so_y = o_sy;
+        f.so_z = o_sz;
+        f.status = statusd;
+        FinalSmem fs;
+        fs.rsh_stride = 2 * fin_lam + 1;
+        fs.n_rsh = (fin_lam + 1) * fs.rsh_stride;
+        int n_om = 1, nabmax = 1;
+        for (auto &lp : atab_need) {
+            n_om = std::max(n_om, n_abc(lp.second) * lam_slots(lp.first, lp.second) * (2 * lp.first + 1));
+            nabmax = std::max(nabmax, n_abc(lp.second));
+        }
+        fs.n_omega = n_om;
+        fs.n_q = fin_nq;
+        fs.n_v = std::max(6144, 3 * nabmax);
+        const size_t smem = (size_t)(2 * fs.n_rsh + 2 * fs.n_omega + fs.n_q + fs.n_v) * sizeof(double);
+        const int blocks = (int)std::min<int64_t>(nt, (int64_t)nsm * 8);
+        final_kernel<<<blocks, kFinThreads, smem, s>>>(f, fs);
+        GRPP_CUDA(cudaGetLastError());
+    }
+    GRPP_CUDA(cudaEventRecord(st.ev[3], s));
+
+    // ---------------------------------------------------------------- results
+    GRPP_CUDA(cudaMemcpyAsync(h_arep, o_arep, out_tot * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GRPP_CUDA(cudaMemcpyAsync(h_sx, o_sx, out_tot * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GRPP_CUDA(cudaMemcpyAsync(h_sy, o_sy, out_tot * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GRPP_CUDA(cudaMemcpyAsync(h_sz, o_sz, out_tot * sizeof(double), cudaMemcpyDeviceToHost, s));
+    int hstatus[16];
+    GRPP_CUDA(cudaMemcpyAsync(hstatus, statusd, sizeof(hstatus), cudaMemcpyDeviceToHost, s));
+    GRPP_CUDA(cudaStreamSynchronize(s));
+    if (stats) {
+        stats->n_tasks = nt;
+        stats->n_radial = (int64_t)rad_task.size();
+        stats->n_mmd = (int64_t)items.size();
+        stats->n_entries = qtot;
+        cudaEventElapsedTime(&stats->ms_mmd, st.ev[0], st.ev[1]);
+        cudaEventElapsedTime(&stats->ms_radial, st.ev[1], st.ev[2]);
+        cudaEventElapsedTime(&stats->ms_final, st.ev[2], st.ev[3]);
+        cudaEventElapsedTime(&stats->ms_total, st.ev[0], st.ev[3]);
+    }
+    if (hstatus[0] != 0) {
+        set_error(LIBGRPP_B200_ERR_INVALID, "a kernel reported an index beyond its table limits");
+        return LIBGRPP_B200_ERR_INVALID;
+    }
+    return 0;
+}
+
+}  // namespace grpp

@@ -1,0 +1,33 @@
+// Host interface of the GRPP engine (engine.cu).
+#pragma once
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/libgrpp_b200.h"
+
+namespace grpp {
+
+struct RunOptions {
+    int radial_mode = LIBGRPP_B200_RADIAL_PLAIN;
+    int raw_so = 0;          // spin-orbit output without the 2/(2L+1) factor (libgrpp_spin_orbit_integrals)
+};
+
+struct RunStats {
+    int64_t n_tasks = 0, n_radial = 0, n_mmd = 0, n_entries = 0;
+    int64_t fallbacks = 0;
+    float ms_total = 0.f, ms_mmd = 0.f, ms_radial = 0.f, ms_final = 0.f;
+};
+
+// thread-local last error
+void set_error(int code, const std::string &msg);
+int last_error();
+const char *last_error_message();
+
+// Evaluate all tasks of a batch; outputs are host arrays of libgrpp_b200_batch_output_size doubles.
+int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double *arep, double *so_x, double *so_y,
+                   double *so_z, RunStats *stats = nullptr);
+
+int64_t batch_output_size(const libgrpp_b200_batch_t *b);
+
+}  // namespace grpp

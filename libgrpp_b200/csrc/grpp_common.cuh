@@ -1,0 +1,54 @@
+// Shared device-side declarations of the B200 GRPP engine.
+//
+// All arithmetic is FP64. Tables are generated on the host at libgrpp_init()
+// (tables.cu) and live in global memory; their addresses and small constant
+// tables sit in __constant__ memory.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace grpp {
+
+// ---- limits ------------------------------------------------------------------
+constexpr int kMaxL = 10;          // basis and projector angular momentum (libgrpp.h:16-21), +1 for gradients
+constexpr int kBesL = 40;          // Bessel table orders 0..kBesL-1
+constexpr int kBesNX = 1601;       // x = 0.00 .. 16.00 step 0.01 (specfunc_bessel_table.c:14-17)
+constexpr int kRfunL = 40;         // asymptotic R_l coefficients (specfunc_scaled_mod_sph_bessel.c:163-190)
+constexpr int kBoysNX = 301;       // x = 0.0 .. 30.0 step 0.1 (specfunc_boys.c:24)
+constexpr int kBoysNN = 40;
+constexpr int kRshL = 32;          // real spherical harmonic tables l = 0..kRshL
+constexpr int kDfMax = 96;         // double factorial table n = -1..kDfMax
+constexpr int kDawNY = 256;        // Dawson table y = 3.0 + k/32
+constexpr double kDawY0 = 3.0;
+constexpr double kDawH = 1.0 / 32.0;
+constexpr int kBinN = 48;          // binomial table n = 0..kBinN-1
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kZeroThresh = 1e-14;  // LIBGRPP_ZERO_THRESH
+
+struct DeviceTables {
+    const double *bessel;     // [kBesNX][kBesL][5]: value + 4 derivatives
+    const double *rfun;       // [kRfunL][kRfunL]
+    const double *boys;       // [kBoysNX][kBoysNN]
+    const double *dawson;     // [kDawNY]
+    const double *rsh_coef;   // concatenated per l: [(2l+1)][ncomb(l)]
+    const int *rsh_off;       // [kRshL+1] offsets into rsh_coef
+    const int8_t *rsh_comb;   // concatenated per l: ncomb(l) x 3
+    const int *rsh_comb_off;  // [kRshL+1] offsets (in combos)
+    const double *lmat;       // concatenated per L: 3 x (2L+1)^2 (x, y, z)
+    const int *lmat_off;      // [kMaxL+2]
+    const double *dfact;      // dfact[n+1] = n!!, n = -1..kDfMax
+    const double *binom;      // [kBinN][kBinN]
+};
+
+__host__ __device__ inline int ncart(int L) { return (L + 1) * (L + 2) / 2; }
+
+// ---- error reporting from kernels --------------------------------------------
+// Kernels never trap: they record the first problem in a status word the host reads.
+enum DeviceStatus : int {
+    kDevOk = 0,
+    kDevLimit = 1,      // an index exceeded a table limit; the affected value was skipped
+    kDevTimeout = 2,    // a bounded loop gave up
+};
+
+}  // namespace grpp

@@ -1,0 +1,312 @@
+// Type 1 (radially local) GRPP integrals by McMurchie-Davidson, and
+// two-centre overlaps by Obara-Saika, one warp per work item.
+//
+// Reference algorithm: libgrpp/type1_mcmurchie_davidson.c:107-622 and
+// libgrpp/type1_integrals.c:43-78 (sum over potential terms k of c_k times
+// the primitive-pair contraction), libgrpp/overlap.c:39-139.
+//
+// A work item is <bra| c r^(n-2) exp(-zeta r^2) (centred at C) |ket> summed
+// over the terms of one potential, or the overlap <bra|ket>. Per primitive
+// pair and term the warp builds
+//   E[axis][i][j][t]  Hermite expansion coefficients, by wavefronts w = i+j
+//                     (each E^{ij} depends on E^{i-1,j} or E^{i,j-1} only),
+//   R^n_{tuv}         auxiliary integrals (Boys for n=1, G_n for n=0), by
+//                     levels s = t+u+v (each level depends on s-1, s-2 only),
+// in shared memory, then each lane accumulates its Cartesian pairs
+//   sum_{tuv} E^x_t E^y_u E^z_v R^0_{tuv}.
+// The contraction order (terms outer, primitive pairs inner, c_i c_j then
+// c_k applied as in the reference's daxpy calls) is kept.
+#pragma once
+
+#include "grpp_common.cuh"
+#include "specfunc.cuh"
+
+namespace grpp {
+
+struct MmdItem {
+    int bra, ket;        // shell indices
+    int ket_at_centre;   // 1: ket origin is the centre C (outercore shells)
+    int centre;          // centre index (origin of the potential)
+    int pot;             // potential index, or -1 for an overlap
+    int out_kind;        // 0: arep output, 1: outercore U scratch, 2: outercore S scratch
+    int64_t out_off;     // offset of the nbra x nket row-major block
+};
+
+struct MmdArgs {
+    const MmdItem *items;
+    int n_items;
+    const int *shell_L, *shell_nprim, *shell_prim_off, *shell_cart_off;
+    const double *prim_coef, *prim_alpha, *shell_origin;
+    const int8_t *cart;
+    const int *pot_nprim, *pot_prim_off, *pot_powers;
+    const double *pot_coef, *pot_alpha;
+    const double *centre_origin;
+    double *out[3];
+    int smax;            // max la+lb over the items (sizes the shared workspace)
+    int lmax;            // max l over the items
+    int *status;
+};
+
+// shared workspace per warp, in doubles
+__host__ __device__ inline int mmd_e_size(int lmax) { return 3 * (lmax + 1) * (lmax + 1) * (2 * lmax + 1); }
+__host__ __device__ inline int mmd_r_size(int smax)
+{
+    // sum over levels s of (s+1)(s+2)/2 entries x (smax-s+1) orders
+    int tot = 0;
+    for (int s = 0; s <= smax; s++) tot += (s + 1) * (s + 2) / 2 * (smax - s + 1);
+    return tot;
+}
+__host__ __device__ inline int mmd_ws_size(int lmax, int smax) { return mmd_e_size(lmax) + mmd_r_size(smax) + 2 * (smax + 2) + 16; }
+
+constexpr int kMmdMaxPairsPerLane = 32;  // up to 1024 Cartesian pairs per pass
+
+__device__ __forceinline__ int eidx(int lb1, int S1, int ax, int i, int j, int t, int la1)
+{
+    return ((ax * la1 + i) * lb1 + j) * S1 + t;
+}
+
+// level offsets of the R table: lvl_off[s] = sum_{s'<s} ne(s') (S-s'+1)
+__device__ __forceinline__ int r_level_off(int S, int s)
+{
+    int o = 0;
+    for (int q = 0; q < s; q++) o += (q + 1) * (q + 2) / 2 * (S - q + 1);
+    return o;
+}
+
+// index of (u+v = k, v) within level s: tri(k) + v
+__device__ __forceinline__ int r_in_level(int u, int v) { return (u + v) * (u + v + 1) / 2 + v; }
+
+__global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
+{
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const int ws = mmd_ws_size(a.lmax, a.smax);
+    double *E = smem + warp * ws;
+    double *R = E + mmd_e_size(a.lmax);
+    double *aux = R + mmd_r_size(a.smax);
+    int *lvl = (int *)(aux + (a.smax + 2));
+
+    for (int it = blockIdx.x * wpb + warp; it < a.n_items; it += gridDim.x * wpb) {
+        const MmdItem item = a.items[it];
+        const int la = a.shell_L[item.bra], lb = a.shell_L[item.ket];
+        const int nA = ncart(la), nB = ncart(lb), S = la + lb;
+        const int la1 = la + 1, lb1 = lb + 1, S1 = S + 1;
+        const double *Ao = a.shell_origin + 3 * item.bra;
+        const double *Bo = item.ket_at_centre ? a.centre_origin + 3 * item.centre : a.shell_origin + 3 * item.ket;
+        const double *Co = a.centre_origin + 3 * item.centre;
+        const double A[3] = {Ao[0], Ao[1], Ao[2]}, B[3] = {Bo[0], Bo[1], Bo[2]}, C[3] = {Co[0], Co[1], Co[2]};
+        const int8_t *ca = a.cart + 3 * a.shell_cart_off[item.bra];
+        const int8_t *cb = a.cart + 3 * a.shell_cart_off[item.ket];
+        const int npA = a.shell_nprim[item.bra], npB = a.shell_nprim[item.ket];
+        const double *cA = a.prim_coef + a.shell_prim_off[item.bra], *xA = a.prim_alpha + a.shell_prim_off[item.bra];
+        const double *cB = a.prim_coef + a.shell_prim_off[item.ket], *xB = a.prim_alpha + a.shell_prim_off[item.ket];
+        const bool overlap = item.pot < 0;
+        const int nterms = overlap ? 1 : a.pot_nprim[item.pot];
+        double *out = a.out[item.out_kind] + item.out_off;
+
+        __syncwarp();  // the previous item's readers of lvl are done
+        if (lane == 0) {
+            int o = 0;
+            for (int s = 0; s <= S; s++) {
+                lvl[s] = o;
+                o += (s + 1) * (s + 2) / 2 * (S - s + 1);
+            }
+        }
+        __syncwarp();
+
+        const int npairs = nA * nB;
+        for (int pass = 0; pass < npairs; pass += 32 * kMmdMaxPairsPerLane) {
+            double res[kMmdMaxPairsPerLane];
+#pragma unroll
+            for (int q = 0; q < kMmdMaxPairsPerLane; q++) res[q] = 0.0;
+
+            for (int k = 0; k < nterms; k++) {
+                const double zeta = overlap ? 0.0 : a.pot_alpha[a.pot_prim_off[item.pot] + k];
+                const int npow = overlap ? 3 : a.pot_powers[a.pot_prim_off[item.pot] + k];
+                double accp[kMmdMaxPairsPerLane];
+#pragma unroll
+                for (int q = 0; q < kMmdMaxPairsPerLane; q++) accp[q] = 0.0;
+
+                for (int i = 0; i < npA; i++) {
+                    const double ci = cA[i];
+                    if (fabs(ci) < kZeroThresh && !overlap) continue;
+                    for (int j = 0; j < npB; j++) {
+                        const double cj = cB[j];
+                        if (fabs(cj) < kZeroThresh && !overlap) continue;
+                        const double al = xA[i], be = xB[j];
+                        const double NA = gaussian_norm(la, al), NB = gaussian_norm(lb, be);
+                        double pref;
+                        if (!overlap) {
+                            // ---- Hermite E by wavefronts (type1_mcmurchie_davidson.c:569-622)
+                            const double q = al + be + zeta;
+                            const double muab = al * be / q, muac = al * zeta / q, mubc = be * zeta / q;
+                            double Q[3], K[3];
+#pragma unroll
+                            for (int d = 0; d < 3; d++) {
+                                Q[d] = (al * A[d] + be * B[d] + zeta * C[d]) / q;
+                                const double xab = A[d] - B[d], xac = A[d] - C[d], xbc = B[d] - C[d];
+                                K[d] = exp(-muab * xab * xab) * exp(-muac * xac * xac) * exp(-mubc * xbc * xbc);
+                            }
+                            for (int w = 0; w <= S; w++) {
+                                // entries (axis, i, j=w-i, t<=w)
+                                const int ilo = max(0, w - lb), ihi = min(la, w);
+                                const int ni = ihi - ilo + 1, per_axis = ni * (w + 1), tot = 3 * per_axis;
+                                for (int e = lane; e < tot; e += 32) {
+                                    const int ax = e / per_axis, r = e % per_axis;
+                                    const int ii = ilo + r / (w + 1), t = r % (w + 1), jj = w - ii;
+                                    double v;
+                                    if (t == 0) {
+                                        if (ii == 0 && jj == 0) v = K[ax];
+                                        else if (ii == 1 && jj == 0) v = (Q[ax] - A[ax]) * E[eidx(lb1, S1, ax, 0, 0, 0, la1)];
+                                        else if (ii == 0 && jj == 1) v = (Q[ax] - B[ax]) * E[eidx(lb1, S1, ax, 0, 0, 0, la1)];
+                                        else if (ii == 0)
+                                            v = (Q[ax] - B[ax]) * E[eidx(lb1, S1, ax, ii, jj - 1, 0, la1)] + E[eidx(lb1, S1, ax, ii, jj - 1, 1, la1)];
+                                        else
+                                            v = (Q[ax] - A[ax]) * E[eidx(lb1, S1, ax, ii - 1, jj, 0, la1)] + E[eidx(lb1, S1, ax, ii - 1, jj, 1, la1)];
+                                    } else {
+                                        const double f = 1.0 / (2.0 * q * t);
+                                        v = 0.0;
+                                        if (ii > 0) v += f * ii * E[eidx(lb1, S1, ax, ii - 1, jj, t - 1, la1)];
+                                        if (jj > 0) v += f * jj * E[eidx(lb1, S1, ax, ii, jj - 1, t - 1, la1)];
+                                    }
+                                    E[eidx(lb1, S1, ax, ii, jj, t, la1)] = v;
+                                }
+                                __syncwarp();
+                            }
+                            if (npow == 2) {
+                                pref = 0.0;
+                            } else {
+                                // ---- auxiliary functions and R by levels (type1_mcmurchie_davidson.c:457-564)
+                                const double QC[3] = {Q[0] - C[0], Q[1] - C[1], Q[2] - C[2]};
+                                const double dx = Q[0] - C[0], dy = Q[1] - C[1], dz = Q[2] - C[2];
+                                const double x = q * (dx * dx + dy * dy + dz * dz);
+                                if (npow == 1) {
+                                    if (lane <= S) aux[lane] = boys(lane, x);
+                                } else if (lane == 0) {
+                                    gfun_values(x, S, aux);
+                                }
+                                __syncwarp();
+                                const bool isg = npow == 0;
+                                const double q2 = isg ? 2.0 * q : -2.0 * q;
+                                if (lane <= S) R[lane] = pow(q2, lane) * aux[lane];  // level 0: n = 0..S
+                                __syncwarp();
+                                for (int s = 1; s <= S; s++) {
+                                    const int ne = (s + 1) * (s + 2) / 2, nn = S - s + 1, tot = ne * nn;
+                                    const int o = lvl[s], o1 = lvl[s - 1], o2 = s >= 2 ? lvl[s - 2] : 0;
+                                    const int ne1 = s * (s + 1) / 2, ne2 = (s - 1) * s / 2;
+                                    for (int e = lane; e < tot; e += 32) {
+                                        const int n = e / ne, idx = e % ne;
+                                        // decode idx -> (u+v = kk, v), t = s - kk
+                                        int kk = (int)((sqrt(8.0 * idx + 1.0) - 1.0) * 0.5);
+                                        while ((kk + 1) * (kk + 2) / 2 <= idx) kk++;
+                                        while (kk * (kk + 1) / 2 > idx) kk--;
+                                        const int v = idx - kk * (kk + 1) / 2, u = kk - v, t = s - kk;
+                                        int tt = t, uu = u, vv = v, kq;
+                                        double X;
+                                        if (t + u == 0) { vv = v - 1; kq = v; X = QC[2]; }
+                                        else if (t == 0) { uu = u - 1; kq = u; X = QC[1]; }
+                                        else { tt = t - 1; kq = t; X = QC[0]; }
+                                        // previous-level element (t-1|u-1|v-1) and (t-2|u-2|v-2)
+                                        const int i1 = r_in_level(uu, vv);
+                                        const double r1n1 = R[o1 + (n + 1) * ne1 + i1], r1n = R[o1 + n * ne1 + i1];
+                                        double val = 0.0;
+                                        if (kq > 1) {
+                                            const int t2 = (tt == t) ? t : t - 2, u2 = (uu == u) ? u : u - 2, v2 = (vv == v) ? v : v - 2;
+                                            const int i2 = r_in_level(u2, v2);
+                                            const double r2n1 = R[o2 + (n + 1) * ne2 + i2], r2n = R[o2 + n * ne2 + i2];
+                                            (void)t2;
+                                            if (isg) val += (kq - 1) * (r2n1 - 2.0 * q * r2n);
+                                            else val += (kq - 1) * r2n1;
+                                        }
+                                        if (isg) val += X * (r1n1 - 2.0 * q * r1n);
+                                        else val += X * r1n1;
+                                        R[o + n * ne + idx] = val;
+                                    }
+                                    __syncwarp();
+                                }
+                                pref = npow == 1 ? NA * NB * 2.0 * kPi / q : NA * NB * 2.0 * pow(kPi, 1.5) / sqrt(q);
+                            }
+                            // ---- Cartesian pairs of this lane
+#pragma unroll
+                            for (int qq = 0; qq < kMmdMaxPairsPerLane; qq++) {
+                                const int pr = pass + lane + 32 * qq;
+                                if (pr >= npairs) break;
+                                const int m = pr / nB, n = pr % nB;
+                                const int ax = ca[3 * m], ay = ca[3 * m + 1], az = ca[3 * m + 2];
+                                const int bx = cb[3 * n], by = cb[3 * n + 1], bz = cb[3 * n + 2];
+                                double buf;
+                                if (npow == 2) {
+                                    buf = NA * NB * E[eidx(lb1, S1, 0, ax, bx, 0, la1)] * E[eidx(lb1, S1, 1, ay, by, 0, la1)] *
+                                          E[eidx(lb1, S1, 2, az, bz, 0, la1)] * pow(kPi / q, 1.5);
+                                } else {
+                                    double s = 0.0;
+                                    for (int t = 0; t <= ax + bx; t++) {
+                                        const double ex = E[eidx(lb1, S1, 0, ax, bx, t, la1)];
+                                        for (int u = 0; u <= ay + by; u++) {
+                                            const double ey = E[eidx(lb1, S1, 1, ay, by, u, la1)];
+                                            for (int v = 0; v <= az + bz; v++) {
+                                                const double ez = E[eidx(lb1, S1, 2, az, bz, v, la1)];
+                                                s += ex * ey * ez * R[lvl[t + u + v] + r_in_level(u, v)];
+                                            }
+                                        }
+                                    }
+                                    buf = s * pref;
+                                }
+                                accp[qq] += (ci * cj) * buf;
+                            }
+                        } else {
+                            // ---- overlap: 1D Obara-Saika tables per axis (overlap.c:92-120)
+                            const double p = al + be, mu = al * be / p, pf = 1.0 / (2.0 * p);
+                            if (lane < 3) {
+                                const int ax = lane;
+                                const double P = (al * A[ax] + be * B[ax]) / p, xab = A[ax] - B[ax];
+                                const double xpa = P - A[ax], xpb = P - B[ax];
+                                for (int ii = 0; ii <= la; ii++)
+                                    for (int jj = 0; jj <= lb; jj++) {
+                                        double s = 0.0;
+                                        if (ii + jj == 0) {
+                                            E[eidx(lb1, S1, ax, 0, 0, 0, la1)] = sqrt(kPi / p) * exp(-mu * xab * xab);
+                                            continue;
+                                        }
+                                        if (ii == 0) {
+                                            s += xpb * E[eidx(lb1, S1, ax, ii, jj - 1, 0, la1)];
+                                            if (jj - 1 > 0) s += (jj - 1) * pf * E[eidx(lb1, S1, ax, ii, jj - 2, 0, la1)];
+                                        } else {
+                                            s += xpa * E[eidx(lb1, S1, ax, ii - 1, jj, 0, la1)];
+                                            if (ii - 1 > 0) s += (ii - 1) * pf * E[eidx(lb1, S1, ax, ii - 2, jj, 0, la1)];
+                                            if (jj > 0) s += jj * pf * E[eidx(lb1, S1, ax, ii - 1, jj - 1, 0, la1)];
+                                        }
+                                        E[eidx(lb1, S1, ax, ii, jj, 0, la1)] = s;
+                                    }
+                            }
+                            __syncwarp();
+#pragma unroll
+                            for (int qq = 0; qq < kMmdMaxPairsPerLane; qq++) {
+                                const int pr = pass + lane + 32 * qq;
+                                if (pr >= npairs) break;
+                                const int m = pr / nB, n = pr % nB;
+                                const double buf = NA * NB * E[eidx(lb1, S1, 0, ca[3 * m], cb[3 * n], 0, la1)] *
+                                                   E[eidx(lb1, S1, 1, ca[3 * m + 1], cb[3 * n + 1], 0, la1)] *
+                                                   E[eidx(lb1, S1, 2, ca[3 * m + 2], cb[3 * n + 2], 0, la1)];
+                                accp[qq] += (ci * cj) * buf;
+                            }
+                        }
+                        __syncwarp();
+                    }
+                }
+                const double ck = overlap ? 1.0 : a.pot_coef[a.pot_prim_off[item.pot] + k];
+#pragma unroll
+                for (int qq = 0; qq < kMmdMaxPairsPerLane; qq++) res[qq] += ck * accp[qq];
+            }
+#pragma unroll
+            for (int qq = 0; qq < kMmdMaxPairsPerLane; qq++) {
+                const int pr = pass + lane + 32 * qq;
+                if (pr < npairs) out[pr] = res[qq];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace grpp

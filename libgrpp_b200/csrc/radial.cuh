@@ -1,0 +1,394 @@
+// Radial integrals of the semilocal (type 2) and spin-orbit GRPP terms.
+//
+// Reference algorithm: libgrpp/radial_type2_integral.c:101-489 and
+// libgrpp/screening.c:193-378. For one task (shells A, B, centre C) and each
+// semilocal potential p of the centre, the table
+//   Q_p[l1][l2][N] = int_0^inf U_p(r) F^A_l1(r) F^B_l2(r) r^N dr,
+//   F_l(r) = sum_i c_i N_i exp(-a_i (r-CA)^2) M_l(2 a_i CA r),
+// with l1 <= L_p + la, l2 <= L_p + lb, N <= la + lb, is computed by
+//   * the one-centre analytic formula when CA = CB = 0;
+//   * otherwise, per entry, the Shaw-Hill screening estimate (entries below
+//     1e-16 return the estimate) and the nested Log3 quadrature
+//     r_i = -5 ln(1 - x_i^3), levels of 31, 63, ..., 8191 points, stopping when
+//     |S_L - S_{L-1}| <= 1e-16 unless |S|/|estimate| < 1e-3, capped at 8191 points.
+//
+// GPU mapping: one CTA per task. Phase 1: each warp screens whole entries,
+// its lanes evaluating 32 primitive triples at a time, and stops at the first
+// chunk that contains a failing triple (libgrpp stops at the first failing one;
+// the outcome is the same). Phase 2: the grid is walked level by level in
+// chunks of one point per thread; a point's integrand values
+//   w U_p(r) for every potential, F^A_l, F^B_l for every order, r^N,
+// are evaluated once and shared by all potentials and entries; every thread
+// then advances the running sums of the entries it owns, point by point in the
+// reference's order and association ((((w U) F1) F2) r^N).
+#pragma once
+
+#include "grpp_common.cuh"
+#include "specfunc.cuh"
+
+namespace grpp {
+
+constexpr int kRadThreads = 128;
+constexpr int kRadMaxPrims = 64;     // primitives per shell on the radial path
+constexpr int kRadMaxPots = 24;      // semilocal potentials per centre
+constexpr int kRadMaxTerms = 256;    // potential terms per centre (all semilocal potentials)
+constexpr int kRadMaxLam = 24;       // lambda <= L + l
+constexpr int kRadMaxN = 24;         // N <= la + lb
+constexpr int kRadMaxLevel = 8;      // 8191 points
+constexpr int kRadMaxEntries = 16384;
+
+// entry flag bits
+constexpr uint8_t kEntActive = 1, kEntScrOk = 2;
+
+struct RadialArgs {
+    int n_items;
+    const int *item_task;
+    const int *task_a, *task_b, *task_c;
+    const int *shell_L;
+    const double *shell_origin;
+    // shrunk (|c| > 1e-14) primitives with the normalisation folded in (radial_type2_integral.c:164-172)
+    const int *rp_off, *rp_n;
+    const double *rp_coef, *rp_alpha;
+    // unshrunk primitives (one-centre branch, radial_type2_integral.c:126-155)
+    const int *shell_nprim, *shell_prim_off;
+    const double *prim_coef, *prim_alpha;
+    const double *centre_origin;
+    const int *centre_grpp;
+    const int *grpp_sl_off, *grpp_sl_n, *sl_pot;
+    const int *pot_L, *pot_nprim, *pot_prim_off, *pot_powers;
+    const double *pot_coef, *pot_alpha;
+    const int64_t *q_off;       // per item
+    double *Q;                  // table values (running sums during the walk)
+    double *S_prev, *scr;       // per entry scratch, same indexing as Q
+    int8_t *stop_level;         // per item: deepest level walked (learning labels), may be null
+    const int8_t *pred_level;   // per item: predicted level (learned mode), may be null
+    int *fallback_count;        // learned mode: items that needed more than predicted+1
+    int *status;
+};
+
+struct RadialShared {
+    double CA, CB;
+    int la, lb, np_a, np_b, npot, nterm_tot, d_n;
+    int l1max_all, l2max_all;
+    int one_centre;
+    int n_entries;
+    int any_active;
+    double ca[kRadMaxPrims], xa[kRadMaxPrims], ka[kRadMaxPrims];
+    double cb[kRadMaxPrims], xb[kRadMaxPrims], kb[kRadMaxPrims];
+    int pL[kRadMaxPots], pn[kRadMaxPots], poff[kRadMaxPots], pent[kRadMaxPots + 1];
+    int tpow[kRadMaxTerms];
+    double tcoef[kRadMaxTerms], talpha[kRadMaxTerms];
+};
+
+// ---- screening (screening.c:243-362) ------------------------------------------
+
+__device__ __forceinline__ double scr_ratio(int l, double x)
+{
+    return l == 0 ? bessel_scaled(1, x) / bessel_scaled(0, x) : bessel_scaled(l - 1, x) / bessel_scaled(l, x);
+}
+
+// returns true on failure; *val is the primitive estimate
+__device__ inline bool scr_prim(int l1, int l2, int n, double CA2, double CB2, double aA, double aB, double k1,
+                                double k2, double eta, double *val)
+{
+    *val = 0.0;
+    if (l1 >= 1 && fabs(k1) <= kZeroThresh) return false;
+    if (l2 >= 1 && fabs(k2) <= kZeroThresh) return false;
+    const double p = aA + aB + eta, CA = sqrt(CA2), CB = sqrt(CB2);
+    if (l1 == 0 && l2 == 0 && fabs(k1) <= kZeroThresh && fabs(k2) <= kZeroThresh) {
+        double gi;
+        if (n % 2 == 0) {
+            int k = n / 2;
+            gi = dfact(2 * k - 1) / (pow(2.0, k + 1) * pow(p, k)) * sqrt(kPi / p);
+        } else {
+            int k = (n - 1) / 2;
+            double f = 1.0;
+            for (int q = 2; q <= k; q++) f *= q;
+            gi = f / (2.0 * pow(p, k + 1));
+        }
+        *val = exp(-aA * CA * CA - aB * CB * CB) * gi;
+        return false;
+    }
+    double r0 = (aA * CA + aB * CB) / p, r0p;
+    int steps = 0;
+    do {
+        steps++;
+        if (steps == 5) {
+            *val = 0.0;
+            return true;
+        }
+        r0p = r0;
+        const double x1 = k1 * r0, x2 = k2 * r0;
+        double a = scr_ratio(l1, x1) * x1 + scr_ratio(l2, x2) * x2 + n;
+        if (l1 > 0) a = a - l1 - 1;
+        if (l2 > 0) a = a - l2 - 1;
+        r0 = sqrt(a / (2.0 * p));
+    } while (fabs(r0 - r0p) > 1e-2);
+    *val = sqrt(kPi / p) * pow(r0, n) * bessel_scaled(l1, k1 * r0) * bessel_scaled(l2, k2 * r0) *
+           exp(-eta * r0 * r0 - aA * (r0 - CA) * (r0 - CA) - aB * (r0 - CB) * (r0 - CB)) * 0.5 * (1 + erf(sqrt(p) * r0));
+    return false;
+}
+
+// decode entry index within an item -> (potential, l1, l2, N)
+__device__ __forceinline__ void decode_entry(const RadialShared &sh, int e, int &p, int &l1, int &l2, int &N)
+{
+    p = 0;
+    while (e >= sh.pent[p + 1]) p++;
+    int r = e - sh.pent[p];
+    const int d2 = sh.pL[p] + sh.lb + 1, dn = sh.d_n;
+    l1 = r / (d2 * dn);
+    r -= l1 * d2 * dn;
+    l2 = r / dn;
+    N = r - l2 * dn;
+}
+
+// Log3 point i of a grid of nr points (radial_type2_integral.c:357-365)
+__device__ __forceinline__ void log3_point(int i, int nr, double &r, double &w)
+{
+    const double R = 5.0, R3 = R * R * R;
+    const double xi = i / (nr + 1.0), xi3 = xi * xi * xi, ln = log(1 - xi3);
+    w = 3 * R3 * xi * xi * ln * ln / ((1 - xi3) * (nr + 1.0));
+    r = -R * ln;
+}
+
+template <bool LEARNED>
+__global__ void __launch_bounds__(kRadThreads) radial_kernel(RadialArgs a)
+{
+    __shared__ RadialShared sh;
+    __shared__ uint8_t eflag[kRadMaxEntries];
+    extern __shared__ double chunk[];  // [1 + npot + l1max+1 + l2max+1 + dn][kRadThreads]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = kRadThreads / 32;
+
+    for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
+        const int t = a.item_task[item];
+        const int sa = a.task_a[t], sb = a.task_b[t], c = a.task_c[t];
+        __syncthreads();
+        if (tid == 0) {
+            const double *Ao = a.shell_origin + 3 * sa, *Bo = a.shell_origin + 3 * sb, *Co = a.centre_origin + 3 * c;
+            double CAv[3], CBv[3];
+            for (int d = 0; d < 3; d++) {
+                CAv[d] = Co[d] - Ao[d];
+                CBv[d] = Co[d] - Bo[d];
+            }
+            const double CA2 = CAv[0] * CAv[0] + CAv[1] * CAv[1] + CAv[2] * CAv[2];
+            const double CB2 = CBv[0] * CBv[0] + CBv[1] * CBv[1] + CBv[2] * CBv[2];
+            sh.one_centre = CA2 < 1e-14 && CB2 < 1e-14;
+            sh.CA = sqrt(CA2);
+            sh.CB = sqrt(CB2);
+            sh.la = a.shell_L[sa];
+            sh.lb = a.shell_L[sb];
+            sh.d_n = sh.la + sh.lb + 1;
+            const int g = a.centre_grpp[c];
+            sh.npot = a.grpp_sl_n[g];
+            int e = 0, nt = 0, l1m = 0, l2m = 0;
+            for (int p = 0; p < sh.npot; p++) {
+                const int pot = a.sl_pot[a.grpp_sl_off[g] + p];
+                sh.pL[p] = a.pot_L[pot];
+                sh.pn[p] = a.pot_nprim[pot];
+                sh.poff[p] = nt;
+                for (int k = 0; k < sh.pn[p]; k++) {
+                    const int o = a.pot_prim_off[pot] + k;
+                    sh.tpow[nt] = a.pot_powers[o];
+                    sh.tcoef[nt] = a.pot_coef[o];
+                    sh.talpha[nt] = a.pot_alpha[o];
+                    nt++;
+                }
+                sh.pent[p] = e;
+                e += (sh.pL[p] + sh.la + 1) * (sh.pL[p] + sh.lb + 1) * sh.d_n;
+                l1m = max(l1m, sh.pL[p] + sh.la);
+                l2m = max(l2m, sh.pL[p] + sh.lb);
+            }
+            sh.pent[sh.npot] = e;
+            sh.n_entries = e;
+            sh.nterm_tot = nt;
+            sh.l1max_all = l1m;
+            sh.l2max_all = l2m;
+            sh.np_a = a.rp_n[sa];
+            sh.np_b = a.rp_n[sb];
+        }
+        __syncthreads();
+        const int np_a = sh.np_a, np_b = sh.np_b;
+        for (int i = tid; i < np_a; i += kRadThreads) {
+            sh.ca[i] = a.rp_coef[a.rp_off[sa] + i];
+            sh.xa[i] = a.rp_alpha[a.rp_off[sa] + i];
+            sh.ka[i] = 2.0 * sh.xa[i] * sh.CA;
+        }
+        for (int i = tid; i < np_b; i += kRadThreads) {
+            sh.cb[i] = a.rp_coef[a.rp_off[sb] + i];
+            sh.xb[i] = a.rp_alpha[a.rp_off[sb] + i];
+            sh.kb[i] = 2.0 * sh.xb[i] * sh.CB;
+        }
+        const int64_t qo = a.q_off[item];
+        double *Q = a.Q + qo, *Sp = a.S_prev + qo, *SC = a.scr + qo;
+        const int nE = sh.n_entries;
+        __syncthreads();
+
+        if (sh.one_centre) {
+            // ---- analytic one-centre table: only l1 = l2 = 0 is non-zero
+            for (int e = tid; e < nE; e += kRadThreads) {
+                int p, l1, l2, N;
+                decode_entry(sh, e, p, l1, l2, N);
+                double v = 0.0;
+                if (l1 == 0 && l2 == 0) {
+                    const int na = a.shell_nprim[sa], nb = a.shell_nprim[sb];
+                    const double *pca = a.prim_coef + a.shell_prim_off[sa], *pxa = a.prim_alpha + a.shell_prim_off[sa];
+                    const double *pcb = a.prim_coef + a.shell_prim_off[sb], *pxb = a.prim_alpha + a.shell_prim_off[sb];
+                    for (int i = 0; i < na; i++) {
+                        const double ci = pca[i] * gaussian_norm(sh.la, pxa[i]);
+                        for (int j = 0; j < nb; j++) {
+                            const double cj = pcb[j] * gaussian_norm(sh.lb, pxb[j]);
+                            for (int k = 0; k < sh.pn[p]; k++) {
+                                const int tk = sh.poff[p] + k;
+                                const double pp = pxa[i] + pxb[j] + sh.talpha[tk];
+                                const double f = ci * cj * sh.tcoef[tk];
+                                const int n = sh.tpow[tk] + N;
+                                double gi;
+                                if (n % 2 == 0) {
+                                    int kk = n / 2;
+                                    gi = dfact(2 * kk - 1) / (pow(2.0, kk + 1) * pow(pp, kk)) * sqrt(kPi / pp);
+                                } else {
+                                    int kk = (n - 1) / 2;
+                                    double fct = 1.0;
+                                    for (int q = 2; q <= kk; q++) fct *= q;
+                                    gi = fct / (2.0 * pow(pp, kk + 1));
+                                }
+                                v += f * gi;
+                            }
+                        }
+                    }
+                }
+                Q[e] = v;
+            }
+            if (tid == 0 && a.stop_level) a.stop_level[item] = 0;
+            continue;
+        }
+
+        // ---- phase 1: screening, one warp per entry
+        const double CA2 = sh.CA * sh.CA, CB2 = sh.CB * sh.CB;
+        for (int e = warp; e < nE; e += nwarps) {
+            int p, l1, l2, N;
+            decode_entry(sh, e, p, l1, l2, N);
+            const int nk = sh.pn[p], ncomb = np_a * np_b * nk;
+            double sum = 0.0;
+            bool fail = false;
+            for (int c0 = 0; c0 < ncomb && !fail; c0 += 32) {
+                const int cc = c0 + lane;
+                double contrib = 0.0;
+                bool f = false;
+                if (cc < ncomb) {
+                    const int k = cc % nk, ij = cc / nk, j = ij % np_b, i = ij / np_b;
+                    const int tk = sh.poff[p] + k;
+                    double v;
+                    f = scr_prim(l1, l2, N + sh.tpow[tk], CA2, CB2, sh.xa[i], sh.xb[j], sh.ka[i], sh.kb[j],
+                                 sh.talpha[tk], &v);
+                    contrib = sh.ca[i] * sh.cb[j] * sh.tcoef[tk] * v;
+                }
+                fail = __any_sync(0xffffffffu, f);
+                for (int o = 16; o > 0; o >>= 1) contrib += __shfl_down_sync(0xffffffffu, contrib, o);
+                sum += contrib;
+            }
+            if (lane == 0) {
+                const bool ok = !fail;
+                SC[e] = sum;
+                if (ok && fabs(sum) < 1e-16) {
+                    Q[e] = sum;
+                    eflag[e] = kEntScrOk;  // screened: not active
+                } else {
+                    Q[e] = 0.0;
+                    eflag[e] = kEntActive | (ok ? kEntScrOk : 0);
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- phase 2: nested Log3 quadrature
+        const int npot = sh.npot, l1m = sh.l1max_all, l2m = sh.l2max_all, dn = sh.d_n;
+        double *cr = chunk;                                   // unused slot kept for layout clarity
+        double *cwu = chunk + kRadThreads;                    // [npot][T]
+        double *cf1 = cwu + npot * kRadThreads;               // [l1m+1][T]
+        double *cf2 = cf1 + (l1m + 1) * kRadThreads;          // [l2m+1][T]
+        double *crn = cf2 + (l2m + 1) * kRadThreads;          // [dn][T]
+        int level_reached = 0;
+        int nr = 31;
+        for (int level = 0; level <= kRadMaxLevel; level++) {
+            if (level > 0) nr = 2 * nr + 1;
+            const int npts = level == 0 ? nr : (nr + 1) / 2;  // new points of this level
+            level_reached = level;
+            if (level > 0) {
+                for (int e = tid; e < nE; e += kRadThreads)
+                    if (eflag[e] & kEntActive) {
+                        const double s = Q[e];
+                        Sp[e] = s;
+                        Q[e] = 0.5 * s;
+                    }
+            }
+            for (int p0 = 0; p0 < npts; p0 += kRadThreads) {
+                const int np = min(kRadThreads, npts - p0);
+                __syncthreads();
+                if (tid < np) {
+                    const int i = level == 0 ? (p0 + tid + 1) : 2 * (p0 + tid) + 1;
+                    double r, w;
+                    log3_point(i, nr, r, w);
+                    cr[tid] = r;
+                    const double r2 = r * r;
+                    for (int pp = 0; pp < npot; pp++) {
+                        double u = 0.0;
+                        for (int k = 0; k < sh.pn[pp]; k++) {
+                            const int tk = sh.poff[pp] + k;
+                            u += sh.tcoef[tk] * pow(r, sh.tpow[tk] - 2) * exp(-sh.talpha[tk] * r2);
+                        }
+                        cwu[pp * kRadThreads + tid] = w * u;
+                    }
+                    for (int l = 0; l <= l1m; l++) cf1[l * kRadThreads + tid] = 0.0;
+                    for (int l = 0; l <= l2m; l++) cf2[l * kRadThreads + tid] = 0.0;
+                    double mv[kRadMaxLam + 1];
+                    const double dA2 = (r - sh.CA) * (r - sh.CA), dB2 = (r - sh.CB) * (r - sh.CB);
+                    for (int q = 0; q < np_a; q++) {
+                        const double ex = sh.ca[q] * exp(-sh.xa[q] * dA2);
+                        bessel_scaled_row<kRadMaxLam>(l1m, sh.ka[q] * r, mv);
+                        for (int l = 0; l <= l1m; l++) cf1[l * kRadThreads + tid] += ex * mv[l];
+                    }
+                    for (int q = 0; q < np_b; q++) {
+                        const double ex = sh.cb[q] * exp(-sh.xb[q] * dB2);
+                        bessel_scaled_row<kRadMaxLam>(l2m, sh.kb[q] * r, mv);
+                        for (int l = 0; l <= l2m; l++) cf2[l * kRadThreads + tid] += ex * mv[l];
+                    }
+                    for (int n = 0; n < dn; n++) crn[n * kRadThreads + tid] = pow(r, n);
+                }
+                __syncthreads();
+                for (int e = tid; e < nE; e += kRadThreads) {
+                    if (!(eflag[e] & kEntActive)) continue;
+                    int p, l1, l2, N;
+                    decode_entry(sh, e, p, l1, l2, N);
+                    const double *pwu = cwu + p * kRadThreads, *p1 = cf1 + l1 * kRadThreads, *p2 = cf2 + l2 * kRadThreads,
+                                 *pn = crn + N * kRadThreads;
+                    double s = Q[e];
+                    for (int q = 0; q < np; q++)
+                        s = __dadd_rn(s, __dmul_rn(__dmul_rn(__dmul_rn(pwu[q], p1[q]), p2[q]), pn[q]));
+                    Q[e] = s;
+                }
+            }
+            // convergence bookkeeping (radial_type2_integral.c:285-315)
+            int active = 0;
+            if (level > 0) {
+                for (int e = tid; e < nE; e += kRadThreads) {
+                    uint8_t f = eflag[e];
+                    if (!(f & kEntActive)) continue;
+                    const double s = Q[e];
+                    if ((f & kEntScrOk) && (fabs(s) / fabs(SC[e]) < 0.001)) {
+                        active = 1;
+                        continue;
+                    }
+                    if (fabs(s - Sp[e]) <= 1e-16) eflag[e] = f & ~kEntActive;
+                    else active = 1;
+                }
+            } else {
+                active = 1;
+            }
+            if (!__syncthreads_or(active)) break;
+        }
+        if (tid == 0 && a.stop_level) a.stop_level[item] = (int8_t)level_reached;
+    }
+}
+
+}  // namespace grpp

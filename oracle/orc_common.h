@@ -66,6 +66,9 @@ typedef struct {
     uint64_t screened_out;      /* entries returned by the screening gate */
     uint64_t level_hist[10];    /* stop level histogram (index 9 = capped) */
     uint64_t mmd_prim_pairs;    /* primitive shell pairs through MMD */
+    uint64_t scr_prim_calls;    /* primitive screening estimates */
+    uint64_t scr_fail;          /* contracted screenings that failed */
+    uint64_t bessel_calls;      /* scaled Bessel evaluations */
 } orc_stats_t;
 extern orc_stats_t orc_stats;
 

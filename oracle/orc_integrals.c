@@ -569,6 +569,7 @@ static int scr_prim(int l1, int l2, int n, double CA2, double CB2, double aA, do
                     double eta, double *val)
 {
     *val = 0.0;
+    orc_stats.scr_prim_calls++;
     if (l1 >= 1 && fabs(k1) <= LIBGRPP_ZERO_THRESH) return 0;
     if (l2 >= 1 && fabs(k2) <= LIBGRPP_ZERO_THRESH) return 0;
     double p = aA + aB + eta, CA = sqrt(CA2), CB = sqrt(CB2);
@@ -622,6 +623,7 @@ static double r2_integral(r2grid_t *g, int n, int l1, int l2, double tol)
     double sum = 0.0, prev, scr = 0.0;
     int scr_fail = scr_contracted(l1, l2, n, g->CA * g->CA, g->CB * g->CB, g->bra, g->ket, g->pot, &scr);
     orc_stats.radial_entries++;
+    if (scr_fail) orc_stats.scr_fail++;
     if (!scr_fail && fabs(scr) < tol) {
         orc_stats.screened_out++;
         return scr;
@@ -1155,7 +1157,10 @@ static void grad_contribution(libgrpp_shell_t *A, libgrpp_shell_t *B, libgrpp_gr
                 int bra[3] = {A->cart_list[3 * i], A->cart_list[3 * i + 1], A->cart_list[3 * i + 2]};
                 int ket[3] = {B->cart_list[3 * j], B->cart_list[3 * j + 1], B->cart_list[3 * j + 2]};
                 int *dn = diff_bra ? bra : ket, idx = i * nB + j;
-                if (nd > 0) {
+                /* libgrpp forms this term also when the exponent is 0; it then reads outside
+                 * the L-1 block (nlm_to_linear finds no match) and multiplies by 0. The term
+                 * is skipped here, which is the same value without the out-of-bounds read. */
+                if (nd > 0 && dn[k] > 0) {
                     dn[k] -= 1;
                     int bi = nlm_to_linear(bra), ki = nlm_to_linear(ket);
                     dn[k] += 1;

@@ -134,6 +134,7 @@ static void bessel_tables_init(void)
 /* specfunc_scaled_mod_sph_bessel.c:72-122 */
 double orc_bessel_scaled(int n, double x)
 {
+    orc_stats.bessel_calls++;
     if (x <= 1e-7) {
         switch (n) {
         case 0: return 1.0 - x;

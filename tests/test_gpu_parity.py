@@ -1,0 +1,108 @@
+"""Parity of the CUDA engine with libgrpp (golden fixtures) and with the oracle.
+
+Criterion of record, element by element:
+    |gpu - ref| <= max(1e-10, 1e-9 |ref| if |ref| > 1e-6, 4 * env)
+1e-10 absolute is libgrpp's own comparator (test/compare_matrices.c:25); env
+is the reference's own change when its inputs move by a few units of roundoff
+(tests.util.perturbed): libgrpp's radial quadrature stops on an absolute
+|S_L - S_{L-1}| <= 1e-16 test and some blocks are exact zeros computed as
+cancelling sums of large terms, so a few elements carry a noise floor that no
+implementation short of bit-identical arithmetic can go below. Each test
+reports how many elements needed the envelope.
+"""
+import numpy as np
+import pytest
+
+from libgrpp_b200 import synthetic
+from libgrpp_b200.system import ncart
+from tests.util import COMPS, envelope, load_fixture, parity, system_from_fixture
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", ["h2o", "cs", "kcs", "tho", "uo2"])
+def test_fixture_blocks(gpu_lib, name):
+    batch, z = load_fixture(name)
+    outs = gpu_lib.full_grpp_batch(batch)
+    for m, comp in enumerate(COMPS):
+        ok, ab, rel, n_env = parity(outs[m], z["ref_" + comp], z["env_" + comp])
+        print(f"{name} {comp}: max abs {ab:.2e} max rel {rel:.2e} envelope-only elements {n_env}")
+        assert ok, f"{name} {comp}: max abs {ab:.3e}, max rel {rel:.3e}"
+
+
+def test_config0_full_matrix(gpu_lib, oracle_lib):
+    S = synthetic.config0()
+    b = S.batch()
+    got = gpu_lib.full_grpp_batch(b)
+    want, env = envelope(oracle_lib, b)
+    for m in range(4):
+        ok, ab, rel, n_env = parity(got[m], want[m], env[m])
+        print(f"config0 {COMPS[m]}: max abs {ab:.2e} max rel {rel:.2e} envelope-only {n_env}")
+        assert ok, (COMPS[m], ab, rel)
+    assert S.assemble(b, got[0]).shape == (40, 40)
+
+
+def _term_reference(oracle_lib, si, sj, C, kind, pot):
+    """Oracle result and envelope of one GRPP term on one shell pair, as a one-task batch."""
+    from libgrpp_b200.system import GRPP, System
+    g = GRPP()
+    if kind == 1:
+        g.UL = pot
+    elif kind == 2:
+        g.arep = [pot]
+    else:
+        g.so = [pot]
+    S = System([si, sj], [g], [(np.asarray(C, dtype=float), 0)], synthetic.CART_ORDER_TURBOMOLE)
+    b = S.batch(np.array([0]), np.array([1]), np.array([0]))
+    want, env = envelope(oracle_lib, b, nthreads=1)
+    if kind == 3:  # the batch scales spin-orbit by 2/(2L+1); the single-call API does not
+        f = (2 * pot.L + 1) / 2.0
+        want = [w * f for w in want]
+        env = [e * f + 4e-16 * np.abs(w) for e, w in zip(env, want)]
+    return want, env
+
+
+def test_single_task_terms(gpu_lib, oracle_lib):
+    """libgrpp_type1/type2/spin_orbit_integrals through the single-call C API."""
+    S = synthetic.config2(seed=7, n_heavy=2, n_h=1, lmax=3, box=6.0)
+    gpu_lib.set_cartesian_order(S.cart_order)
+    g = S.grpps[0]
+    C = S.centres[0][0]
+    rng = np.random.default_rng(0)
+    for _ in range(6):
+        i, j = rng.integers(0, len(S.shells), 2)
+        si, sj = S.shells[i], S.shells[j]
+        nA, nB = ncart(si.L), ncart(sj.L)
+        hA, hB = gpu_lib.new_shell(si), gpu_lib.new_shell(sj)
+        got = {1: [gpu_lib.type1(hA, hB, C, gpu_lib.new_potential(g.UL), nA, nB)],
+               2: [gpu_lib.type2(hA, hB, C, gpu_lib.new_potential(g.arep[1]), nA, nB)],
+               3: gpu_lib.spin_orbit(hA, hB, C, gpu_lib.new_potential(g.so[1]), nA, nB)}
+        for kind, pot in ((1, g.UL), (2, g.arep[1]), (3, g.so[1])):
+            want, env = _term_reference(oracle_lib, si, sj, C, kind, pot)
+            comps = [0] if kind < 3 else [1, 2, 3]
+            for x, m in zip(got[kind], comps):
+                ok, ab, rel, n_env = parity(x.ravel(), want[m], env[m])
+                assert ok, (int(i), int(j), kind, m, ab, rel)
+
+
+def test_h2o_gradients(gpu_lib):
+    """d V / d R_atom for all atoms against libgrpp's gradient matrices (test/H2O/*_grad_*)."""
+    batch, z = load_fixture("h2o")
+    S = system_from_fixture(z)
+    gpu_lib.set_cartesian_order(S.cart_order)
+    hs = [gpu_lib.new_shell(s) for s in S.shells]
+    hg = [gpu_lib.new_grpp(g) for g in S.grpps]
+    off = S.basis_offsets()
+    n = int(off[-1])
+    nat = len(S.atoms)
+    G = np.zeros((4, nat, 3, n, n))
+    for i, si in enumerate(S.shells):
+        for j, sj in enumerate(S.shells):
+            for at in range(nat):
+                for C, gi in S.centres:
+                    G[:, at, :, off[i]:off[i + 1], off[j]:off[j + 1]] += gpu_lib.full_gradient(
+                        hs[i], hs[j], hg[gi], C, S.atoms[at], ncart(si.L), ncart(sj.L))
+    tri = np.tril_indices(n)
+    got = G[:, :, :, tri[0], tri[1]]
+    ok, ab, rel, _ = parity(got.ravel(), z["ref_grad_lower"].ravel())
+    assert ok, (ab, rel)

@@ -1,0 +1,97 @@
+"""The oracle (CPU restatement of libgrpp's GRPP path, oracle/orc_*.c) pinned
+against libgrpp's own outputs: the golden fixtures generated from the compiled
+reference and checked against libgrpp's shipped matrices
+(tests/golden/make_golden.py), and, where the compiled reference is present,
+against it directly on synthetic inputs."""
+import numpy as np
+import pytest
+
+from libgrpp_b200 import synthetic
+from tests.util import COMPS, envelope, load_fixture, parity
+
+
+@pytest.mark.parametrize("name", ["h2o", "cs", "kcs", "tho", "uo2"])
+def test_oracle_matches_golden(oracle_lib, name):
+    batch, z = load_fixture(name)
+    outs = oracle_lib.driver_full_batch(batch, nthreads=4)
+    for m, comp in enumerate(COMPS):
+        # the restatement regenerates libgrpp's Bessel/Boys tables, so it sits within
+        # the reference's own last-bit sensitivity, with margin for the deep-level elements
+        ok, ab, rel, n_env = parity(outs[m], z["ref_" + comp], z["env_" + comp], env_factor=16.0)
+        assert ok, (name, comp, ab, rel)
+
+
+def test_oracle_h2o_gradient_entry(oracle_lib):
+    """One H2O gradient block through libgrpp_full_grpp_integrals_gradient."""
+    from libgrpp_b200.system import ncart
+    from tests.util import system_from_fixture
+    _, z = load_fixture("h2o")
+    S = system_from_fixture(z)
+    oracle_lib.set_cartesian_order(S.cart_order)
+    hs = [oracle_lib.new_shell(s) for s in S.shells]
+    hg = [oracle_lib.new_grpp(g) for g in S.grpps]
+    off = S.basis_offsets()
+    n = int(off[-1])
+    tri = np.tril_indices(n)
+    # d/dR of atom 0 (O), all shell pairs, all centres
+    G = np.zeros((4, 3, n, n))
+    for i, si in enumerate(S.shells):
+        for j, sj in enumerate(S.shells):
+            for C, gi in S.centres:
+                G[:, :, off[i]:off[i + 1], off[j]:off[j + 1]] += oracle_lib.full_gradient(
+                    hs[i], hs[j], hg[gi], C, S.atoms[0], ncart(si.L), ncart(sj.L))
+    want = z["ref_grad_lower"][:, 0]
+    got = G[:, :, tri[0], tri[1]]
+    ok, ab, rel, _ = parity(got.ravel(), want.ravel())
+    assert ok, (ab, rel)
+
+
+@pytest.mark.slow
+def test_oracle_matches_reference_config0(oracle_lib, ref_lib):
+    S = synthetic.config0()
+    b = S.batch()
+    want, env = envelope(ref_lib, b)
+    got = oracle_lib.driver_full_batch(b, nthreads=8)
+    for m in range(4):
+        ok, ab, rel, _ = parity(got[m], want[m], env[m])
+        assert ok, (COMPS[m], ab, rel)
+
+
+def test_oracle_matches_reference_full_grpp(oracle_lib, ref_lib):
+    """Heavy atoms with SO and outercore terms (config 2 generator, small)."""
+    S = synthetic.config2(seed=11, n_heavy=2, n_h=2, lmax=3, box=7.0)
+    a, b, c = S.all_tasks()
+    sel = np.random.default_rng(0).choice(len(a), 40, replace=False)
+    batch = S.batch(a[sel], b[sel], c[sel])
+    want, env = envelope(ref_lib, batch)
+    got = oracle_lib.driver_full_batch(batch, nthreads=8)
+    for m in range(4):
+        ok, ab, rel, _ = parity(got[m], want[m], env[m], env_factor=16.0)
+        assert ok, (COMPS[m], ab, rel)
+
+
+def test_special_functions_against_scipy(oracle_lib):
+    """Bessel M_l(x) = exp(-x) i_l(x), Boys F_n, Dawson, against scipy (independent implementations)."""
+    import ctypes as ct
+    from scipy import special
+    L = oracle_lib.lib
+    L.orc_bessel_scaled_export.restype = ct.c_double
+    L.orc_bessel_scaled_export.argtypes = [ct.c_int, ct.c_double]
+    L.orc_boys_export.restype = ct.c_double
+    L.orc_boys_export.argtypes = [ct.c_int, ct.c_double]
+    L.orc_dawson_export.restype = ct.c_double
+    L.orc_dawson_export.argtypes = [ct.c_double]
+    for x in [1e-3, 0.37, 2.0, 7.5, 15.99, 16.5, 40.0]:
+        for l in range(0, 9):
+            want = special.spherical_in(l, x) * np.exp(-x)
+            got = L.orc_bessel_scaled_export(l, x)
+            # libgrpp's scheme (Taylor on a 0.01 grid, asymptotic above 16) is accurate
+            # to ~1e-13 relative of M_0
+            assert abs(got - want) <= 1e-12 * max(1.0, abs(want)) + 1e-13, (l, x, got, want)
+    for x in [0.0, 0.05, 1.3, 9.99, 29.0, 35.0]:
+        for n in range(0, 12):
+            want = special.hyp1f1(n + 0.5, n + 1.5, -x) / (2 * n + 1)
+            got = L.orc_boys_export(n, x)
+            assert abs(got - want) <= 1e-12 * abs(want) + 1e-15, (n, x, got, want)
+    for y in [0.1, 1.0, 3.3, 5.0, 7.2, 11.0, 40.0]:
+        assert abs(L.orc_dawson_export(y) - special.dawsn(y)) <= 1e-14 * special.dawsn(y)

@@ -1,0 +1,146 @@
+"""Shared helpers of the test suite (fixtures, libraries, comparisons)."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+from libgrpp_b200.system import BatchArrays
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "libgrpp_oracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libgrpp_ref.so")
+COMPS = ("arep", "so_x", "so_y", "so_z")
+
+
+def ensure_oracle():
+    if not os.path.exists(ORACLE_SO):
+        import subprocess
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True, capture_output=True)
+    return ORACLE_SO
+
+
+def load_oracle():
+    from libgrpp_b200.capi import LibGRPP
+    return LibGRPP(ensure_oracle())
+
+
+def load_ref():
+    from libgrpp_b200.capi import LibGRPP
+    if not os.path.exists(REF_SO):
+        return None
+    return LibGRPP(REF_SO)
+
+
+def load_product():
+    from libgrpp_b200 import engine
+    return engine.load()
+
+
+def load_fixture(name: str):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    arrays = {k[2:]: np.ascontiguousarray(z[k]) for k in z.files if k.startswith("b_")}
+    arrays["task_a"] = np.ascontiguousarray(z["task_a"], dtype=np.int32)
+    arrays["task_b"] = np.ascontiguousarray(z["task_b"], dtype=np.int32)
+    arrays["task_c"] = np.ascontiguousarray(z["task_c"], dtype=np.int32)
+    return BatchArrays(**arrays), z
+
+
+def max_abs(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b)))) if len(a) else 0.0
+
+
+def parity_report(got, want):
+    """max abs error, and max relative error over elements with |want| > 1e-6"""
+    got, want = np.asarray(got), np.asarray(want)
+    ab = float(np.max(np.abs(got - want))) if got.size else 0.0
+    big = np.abs(want) > 1e-6
+    rel = float(np.max(np.abs(got[big] - want[big]) / np.abs(want[big]))) if big.any() else 0.0
+    return ab, rel
+
+
+def system_from_fixture(z):
+    """Rebuild the System (basis shells, GRPPs, centres) stored flat in a fixture."""
+    from libgrpp_b200.system import GRPP, Potential, Shell, System
+
+    g = lambda k: z["b_" + k]  # noqa: E731
+    nbasis = int(max(z["task_a"].max(), z["task_b"].max())) + 1
+
+    def shell(i):
+        o, n = int(g("shell_prim_off")[i]), int(g("shell_nprim")[i])
+        return Shell(g("shell_origin")[3 * i:3 * i + 3], int(g("shell_L")[i]), g("prim_coef")[o:o + n], g("prim_alpha")[o:o + n])
+
+    def pot(p):
+        o, n = int(g("pot_prim_off")[p]), int(g("pot_nprim")[p])
+        return Potential(int(g("pot_L")[p]), int(g("pot_J")[p]), g("pot_powers")[o:o + n], g("pot_coef")[o:o + n],
+                         g("pot_alpha")[o:o + n])
+
+    grpps = []
+    for k in range(len(g("grpp_UL"))):
+        G = GRPP()
+        G.UL = pot(int(g("grpp_UL")[k])) if g("grpp_UL")[k] >= 0 else None
+        lst = g("grpp_pot_list")
+        G.arep = [pot(int(lst[g("grpp_arep_off")[k] + i])) for i in range(int(g("grpp_n_arep")[k]))]
+        G.so = [pot(int(lst[g("grpp_so_off")[k] + i])) for i in range(int(g("grpp_n_so")[k]))]
+        G.oc = [(pot(int(g("grpp_oc_pot")[g("grpp_oc_off")[k] + i])), shell(int(g("grpp_oc_shell")[g("grpp_oc_off")[k] + i])))
+                for i in range(int(g("grpp_n_oc")[k]))]
+        grpps.append(G)
+    co = g("centre_origin").reshape(-1, 3)
+    centres = [(co[i].copy(), int(g("centre_grpp")[i])) for i in range(len(g("centre_grpp")))]
+    shells = [shell(i) for i in range(nbasis)]
+    atoms = z["atoms"] if "atoms" in z.files else None
+    sa = z["shell_atom"] if "shell_atom" in z.files else None
+    ca = z["centre_atom"] if "centre_atom" in z.files else None
+    return System(shells, grpps, centres, int(z["cart_order"]), sa, ca, atoms)
+
+
+U = 2.0 ** -53  # unit roundoff
+
+
+def perturbed(batch: BatchArrays, mode: int) -> BatchArrays:
+    """The same workload with inputs moved by a few units in the last place:
+    mode 1 scales every exponent by (1 + 4u); mode 2 scales contraction and
+    potential coefficients by (1 - 4u), (1 + 4u) and every coordinate by (1 + 4u)
+    (coincident centres stay coincident)."""
+    d = {k: v for k, v in batch.__dict__.items() if not k.startswith("_")}
+    d = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
+    if mode == 1:
+        d["prim_alpha"] = d["prim_alpha"] * (1 + 4 * U)
+        d["pot_alpha"] = d["pot_alpha"] * (1 + 4 * U)
+    else:
+        d["prim_coef"] = d["prim_coef"] * (1 - 4 * U)
+        d["pot_coef"] = d["pot_coef"] * (1 + 4 * U)
+        d["shell_origin"] = d["shell_origin"] * (1 + 4 * U)
+        d["centre_origin"] = d["centre_origin"] * (1 + 4 * U)
+    return BatchArrays(**d)
+
+
+def envelope(lib, batch: BatchArrays, base=None, nthreads=8):
+    """Per-element sensitivity of a CPU library's result to last-bit input changes:
+    max over the two perturbations of |result(perturbed) - result|."""
+    if base is None:
+        base = lib.driver_full_batch(batch, nthreads=nthreads)
+    env = [np.zeros_like(x) for x in base]
+    for mode in (1, 2):
+        p = lib.driver_full_batch(perturbed(batch, mode), nthreads=nthreads)
+        for m in range(4):
+            env[m] = np.maximum(env[m], np.abs(p[m] - base[m]))
+    return base, env
+
+
+def parity(got, want, env=None, abs_tol=1e-10, rel_tol=1e-9, env_factor=4.0):
+    """Element-wise check of record: |got - want| <= max(abs_tol, rel_tol*|want| for |want| > 1e-6,
+    env_factor * envelope). Returns (ok, max_abs, max_rel, n_elements_within_envelope_only)."""
+    got, want = np.asarray(got), np.asarray(want)
+    err = np.abs(got - want)
+    tol = np.full(err.shape, abs_tol)
+    big = np.abs(want) > 1e-6
+    tol[big] = np.maximum(tol[big], rel_tol * np.abs(want[big]))
+    strict_ok = err <= tol
+    if env is not None:
+        tol = np.maximum(tol, env_factor * np.asarray(env))
+    ok = bool(np.all(err <= tol)) and bool(np.all(np.isfinite(got)))
+    max_rel = float(np.max(err[big] / np.abs(want[big]))) if big.any() else 0.0
+    n_env = int(np.sum(~strict_ok & (err <= tol)))
+    return ok, float(err.max()) if err.size else 0.0, max_rel, n_env
