@@ -1,0 +1,294 @@
+#!/usr/bin/env python
+"""Throughput benchmark: shell-pair x RPP-centre tasks per second.
+
+Workload (config 1): 64 atoms uniform in a 40-bohr cube (min separation 3 bohr,
+seed 1), each with U_L (4 terms) + semilocal projectors l = 0..4 (3 terms) and
+s..g shells of 8 primitives (exponents log-uniform [0.02, 5e3]). The full task
+list is 320^2 ordered shell pairs x 64 centres = 6.55M tasks. A step is one
+block of it: 32 bra shells x 32 ket shells x all 64 centres = 65536 tasks,
+ordered by (la, lb); step s of rank r takes block pair (r + s*N) mod 100, so
+ranks never repeat each other's work (weak scaling, no collective on the data
+path; NCCL/gloo only for the start barrier and the max-over-ranks time).
+
+Reported: value = tasks / device time of the engine's kernels with inputs
+resident in HBM (CUDA events on the engine's stream, L2 flushed between
+steps); e2e = the same tasks through the public batched C-ABI call with host
+inputs and outputs (packing, host->device and device->host copies included).
+--impl reference times libgrpp itself (oracle/_ref, compiled from its
+sources) on this host's cores over a bounded sample of each step's tasks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BLOCK = 32
+WORKLOAD = ("config1: 64 atoms in a 40-bohr cube, s..g shells x 8 primitives, U_L + projectors l=0..4; "
+            "step = 32 x 32 shell block x 64 centres = 65536 tasks")
+METRIC = "shell-pair x RPP-centre tasks/s (full GRPP blocks, FP64)"
+
+
+def get_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+_SYSTEM = None
+
+
+def system():
+    global _SYSTEM
+    if _SYSTEM is None:
+        from libgrpp_b200 import synthetic
+        _SYSTEM = synthetic.config1()
+    return _SYSTEM
+
+
+def step_tasks(idx: int):
+    """Tasks of block pair idx (of 100): 32 x 32 shells x 64 centres, ordered by (la, lb)."""
+    S = system()
+    nb = len(S.shells) // BLOCK
+    ia, ib = (idx // nb) % nb, idx % nb
+    sa = np.arange(ia * BLOCK, (ia + 1) * BLOCK)
+    sb = np.arange(ib * BLOCK, (ib + 1) * BLOCK)
+    a, b, c = np.meshgrid(sa, sb, np.arange(len(S.centres)), indexing="ij")
+    a, b, c = a.ravel().astype(np.int32), b.ravel().astype(np.int32), c.ravel().astype(np.int32)
+    La = np.array([s.L for s in S.shells])
+    o = np.lexsort((c, b, a, La[b], La[a]))
+    return a[o], b[o], c[o]
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_rate(batch_fn, n_sample: int, threads: int, seed: int = 0):
+    """libgrpp (oracle/_ref) on a seeded sample of a step's tasks: (tasks/s, sample description)."""
+    from libgrpp_b200.capi import LibGRPP
+    ref = LibGRPP(os.path.join(ROOT, "oracle", "_ref", "libgrpp_ref.so"))
+    a, b, c = batch_fn()
+    sel = np.sort(np.random.default_rng(seed).choice(len(a), n_sample, replace=False))
+    batch = system().batch(a[sel], b[sel], c[sel])
+    t0 = time.perf_counter()
+    ref.driver_full_batch(batch, nthreads=threads)
+    dt = time.perf_counter() - t0
+    return n_sample / dt, dt
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = host_threads()
+    n_sample = args.ref_sample
+    for w in range(args.warmup):
+        cpu_reference_rate(lambda: step_tasks(w), max(8, threads), threads, seed=100 + w)
+    rates, secs = [], []
+    for s in range(args.steps):
+        r, dt = cpu_reference_rate(lambda: step_tasks(s), n_sample, threads, seed=s)
+        rates.append(r)
+        secs.append(dt)
+    rate = len(rates) * n_sample / sum(secs)
+    sample = f"{n_sample} seeded random tasks of each step's 65536-task block, {threads} threads"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "tasks/s", "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": rate, "unit": "tasks/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": rate, "unit": "tasks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    from libgrpp_b200 import engine
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    lib = engine.load()
+    lib.set_device(local)
+    mode = 1 if args.mode == "learned" else 0
+
+    idxs = [(rank + world * s) % 100 for s in range(args.steps)]
+    S = system()
+    batches = [S.batch(*step_tasks(i)) for i in idxs]
+    plans = [lib.plan(b, mode) for b in batches]
+    n_tasks = [len(b.task_a) for b in batches]
+
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for w in range(args.warmup):
+        plans[w % len(plans)].execute()
+
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms, kms = [], {"ms_type1": 0.0, "ms_radial": 0.0, "ms_assembly": 0.0}
+    with ClockSampler(local) as clk:
+        for p in plans:
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            p.execute()
+            st = p.stats()
+            ms.append(st["ms_total"])
+            for k in kms:
+                kms[k] += st[k]
+    torch.cuda.synchronize()
+    total_ms = float(sum(ms))
+    tasks = float(sum(n_tasks))
+    if dist is not None:
+        t = torch.tensor([total_ms, tasks], dtype=torch.float64, device="cuda")
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        total_ms, tasks = float(tmax[0]), float(t[1])
+    value = tasks / (total_ms / 1e3)
+
+    # end to end through the public batched call (host in, host out)
+    e2e_batches = batches[: max(1, min(len(batches), args.e2e_steps))]
+    lib.full_grpp_batch(e2e_batches[0], mode)
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for b in e2e_batches:
+        lib.full_grpp_batch(b, mode)
+    e2e_s = time.perf_counter() - t0
+    e2e_tasks = float(sum(len(b.task_a) for b in e2e_batches))
+    if dist is not None:
+        t = torch.tensor([e2e_s, e2e_tasks], dtype=torch.float64, device="cuda")
+        tm = t.clone()
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        e2e_s, e2e_tasks = float(tm[0]), float(t[1])
+    st0 = plans[0].stats()
+    h2d = st0["h2d_bytes"]
+    d2h = 4 * 8 * int(batches[0].block_offsets()[-1])
+
+    kernel_ms = {k: v / len(plans) for k, v in kms.items()}
+    dominant = max(kernel_ms, key=kernel_ms.get)
+    line = {
+        "metric": METRIC, "value": value, "unit": "tasks/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / len(plans), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config 1)",
+        "config": {"workload": WORKLOAD, "tasks_per_step": n_tasks[0], "radial_mode": args.mode,
+                   "l2": "flushed between steps (512 MiB write)", "parallelism": f"task blocks over {world} GPU(s)"},
+        "kernel_ms_per_step": kernel_ms,
+        "gpu_launches": args.steps * (3 if st0["n_radial"] else 2),
+        "e2e": {"value": e2e_tasks / e2e_s, "unit": "tasks/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = host_threads()
+        rate, dt = cpu_reference_rate(lambda: step_tasks(idxs[0]), args.ref_sample, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": "tasks/s", "cores": threads, "kind": "reference",
+                                "sample": f"{args.ref_sample} seeded random tasks of the first step's block "
+                                          f"({dt:.1f} s on {threads} threads)"}
+    line["roofline"] = roofline(args, dominant, kernel_ms)
+    for p in plans:
+        p.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def roofline(args, dominant, kernel_ms):
+    return {"bound": "fp64", "kernel": dominant, "achieved": None, "peak": None, "unit": "TFLOP/s", "frac": None,
+            "traffic": None, "note": "algorithmic FLOP model pending"}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["plain", "learned"], default="plain")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--ref-sample", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = get_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

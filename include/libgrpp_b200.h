@@ -100,6 +100,23 @@ int64_t libgrpp_b200_batch_output_size(const libgrpp_b200_batch_t *batch);
 int libgrpp_b200_full_grpp_batch(const libgrpp_b200_batch_t *batch, int radial_mode, double *arep,
                                  double *so_x, double *so_y, double *so_z);
 
+/* Select the CUDA device used by the calling thread (this library keeps its own
+ * CUDA runtime state; default device 0). Returns a status code. */
+int libgrpp_b200_set_device(int device);
+
+/* A batch prepared once on the device: inputs uploaded and work lists built, device
+ * buffers owned by the plan. execute() runs the kernels only (outputs stay on the
+ * device until outputs() copies them to host arrays). Not thread-safe per plan. */
+typedef struct libgrpp_b200_plan libgrpp_b200_plan_t;
+
+libgrpp_b200_plan_t *libgrpp_b200_plan_create(const libgrpp_b200_batch_t *batch, int radial_mode);
+int libgrpp_b200_plan_execute(libgrpp_b200_plan_t *plan);
+int libgrpp_b200_plan_outputs(libgrpp_b200_plan_t *plan, double *arep, double *so_x, double *so_y, double *so_z);
+/* ms[4] = kernel time of the last execute(): total, type 1, radial, assembly (CUDA events on the
+ * engine stream); counts[5] = tasks, radial tasks, type 1 work items, radial entries, bytes uploaded */
+int libgrpp_b200_plan_stats(const libgrpp_b200_plan_t *plan, double *ms, int64_t *counts);
+void libgrpp_b200_plan_destroy(libgrpp_b200_plan_t *plan);
+
 #ifdef __cplusplus
 }
 #endif

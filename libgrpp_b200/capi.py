@@ -77,6 +77,12 @@ class LibGRPP:
         self._opt("libgrpp_b200_last_error", ct.c_int, [])
         self._opt("libgrpp_b200_last_error_message", ct.c_char_p, [])
         self._opt("libgrpp_b200_full_grpp_batch", ct.c_int, [_V, ct.c_int, _D, _D, _D, _D])
+        self._opt("libgrpp_b200_set_device", ct.c_int, [ct.c_int])
+        self._opt("libgrpp_b200_plan_create", _V, [_V, ct.c_int])
+        self._opt("libgrpp_b200_plan_execute", ct.c_int, [_V])
+        self._opt("libgrpp_b200_plan_outputs", ct.c_int, [_V, _D, _D, _D, _D])
+        self._opt("libgrpp_b200_plan_stats", ct.c_int, [_V, _D, ct.POINTER(ct.c_int64)])
+        self._opt("libgrpp_b200_plan_destroy", None, [_V])
         self.lib.libgrpp_init()
 
     def _opt(self, name, res, args):
@@ -183,6 +189,14 @@ class LibGRPP:
             raise RuntimeError(f"libgrpp_b200_full_grpp_batch failed ({rc}): {self.last_error_message()}")
         return [x[:n] for x in outs]
 
+    def set_device(self, device: int):
+        rc = self.lib.libgrpp_b200_set_device(int(device))
+        if rc != 0:
+            raise RuntimeError(f"libgrpp_b200_set_device({device}) failed: {self.last_error_message()}")
+
+    def plan(self, batch, radial_mode=0) -> "Plan":
+        return Plan(self, batch, radial_mode)
+
     def last_error(self) -> int:
         return int(self.lib.libgrpp_b200_last_error())
 
@@ -211,3 +225,46 @@ def dense_full(lib: LibGRPP, system, threads=None):
                 for m in range(4):
                     M[m, off[i]:off[i + 1], off[j]:off[j + 1]] += blocks[m]
     return M
+
+
+class Plan:
+    """A batch prepared on the device (libgrpp_b200_plan_*): execute() runs the kernels only."""
+
+    def __init__(self, lib: LibGRPP, batch, radial_mode=0):
+        self.lib = lib
+        self.batch = batch
+        self.n_out = int(batch.block_offsets()[-1])
+        self.h = lib.lib.libgrpp_b200_plan_create(ct.byref(batch.struct), radial_mode)
+        if not self.h:
+            raise RuntimeError(f"libgrpp_b200_plan_create failed: {lib.last_error_message()}")
+
+    def execute(self):
+        rc = self.lib.lib.libgrpp_b200_plan_execute(self.h)
+        if rc != 0:
+            raise RuntimeError(f"libgrpp_b200_plan_execute failed ({rc}): {self.lib.last_error_message()}")
+
+    def outputs(self):
+        outs = [np.zeros(max(self.n_out, 1)) for _ in range(4)]
+        rc = self.lib.lib.libgrpp_b200_plan_outputs(self.h, *[_dp(x) for x in outs])
+        if rc != 0:
+            raise RuntimeError(self.lib.last_error_message())
+        return [x[: self.n_out] for x in outs]
+
+    def stats(self):
+        ms = np.zeros(4)
+        cnt = np.zeros(5, dtype=np.int64)
+        self.lib.lib.libgrpp_b200_plan_stats(self.h, _dp(ms), cnt.ctypes.data_as(ct.POINTER(ct.c_int64)))
+        return {"ms_total": ms[0], "ms_type1": ms[1], "ms_radial": ms[2], "ms_assembly": ms[3],
+                "n_tasks": int(cnt[0]), "n_radial": int(cnt[1]), "n_type1_items": int(cnt[2]),
+                "n_entries": int(cnt[3]), "h2d_bytes": int(cnt[4])}
+
+    def close(self):
+        if self.h:
+            self.lib.lib.libgrpp_b200_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

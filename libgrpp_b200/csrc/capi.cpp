@@ -649,5 +649,52 @@ int libgrpp_b200_full_grpp_batch(const libgrpp_b200_batch_t *b, int radial_mode,
     return grpp::run_full_batch(b, opt, arep, sx, sy, sz);
 }
 
+int libgrpp_b200_set_device(int device) { return grpp::set_device(device); }
+
+libgrpp_b200_plan_t *libgrpp_b200_plan_create(const libgrpp_b200_batch_t *b, int radial_mode)
+{
+    if (!check_init()) return nullptr;
+    grpp::RunOptions opt;
+    opt.radial_mode = radial_mode;
+    return (libgrpp_b200_plan_t *)grpp::plan_create(b, opt);
+}
+
+int libgrpp_b200_plan_execute(libgrpp_b200_plan_t *plan)
+{
+    if (!plan) {
+        grpp::set_error(LIBGRPP_B200_ERR_INVALID, "null plan");
+        return LIBGRPP_B200_ERR_INVALID;
+    }
+    return grpp::plan_run((grpp::Plan *)plan);
+}
+
+int libgrpp_b200_plan_outputs(libgrpp_b200_plan_t *plan, double *arep, double *sx, double *sy, double *sz)
+{
+    if (!plan) return LIBGRPP_B200_ERR_INVALID;
+    return grpp::plan_outputs((grpp::Plan *)plan, arep, sx, sy, sz);
+}
+
+int libgrpp_b200_plan_stats(const libgrpp_b200_plan_t *plan, double *ms, int64_t *counts)
+{
+    if (!plan) return LIBGRPP_B200_ERR_INVALID;
+    const grpp::RunStats *st = grpp::plan_stats((const grpp::Plan *)plan);
+    if (ms) {
+        ms[0] = st->ms_total;
+        ms[1] = st->ms_mmd;
+        ms[2] = st->ms_radial;
+        ms[3] = st->ms_final;
+    }
+    if (counts) {
+        counts[0] = st->n_tasks;
+        counts[1] = st->n_radial;
+        counts[2] = st->n_mmd;
+        counts[3] = st->n_entries;
+        counts[4] = grpp::plan_h2d_bytes((const grpp::Plan *)plan);
+    }
+    return 0;
+}
+
+void libgrpp_b200_plan_destroy(libgrpp_b200_plan_t *plan) { grpp::plan_destroy((grpp::Plan *)plan); }
+
 }  // extern "C"
 #pragma GCC visibility pop

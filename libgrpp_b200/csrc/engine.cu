@@ -274,6 +274,28 @@ int ensure_atab(DeviceState &st, int L, int l)
 
 }  // namespace
 
+struct Plan {
+    DeviceState *st = nullptr;
+    RunOptions opt;
+    int64_t n_tasks = 0, out_tot = 0, n_radial = 0, n_mmd = 0, n_entries = 0, h2d_bytes = 0, scratch_bytes = 0;
+    DevBuf in, scratch, out;
+    double *outs[4] = {nullptr, nullptr, nullptr, nullptr};
+    int *status = nullptr;
+    MmdArgs mmd;
+    int mmd_blocks = 0, mmd_threads = 128;
+    size_t mmd_smem = 0;
+    OcProjArgs ocp;
+    int ocp_blocks = 0;
+    RadialArgs rad;
+    int rad_blocks = 0;
+    size_t rad_smem = 0;
+    FinalArgs fin;
+    FinalSmem fin_smem_layout;
+    int fin_blocks = 0;
+    size_t fin_smem = 0;
+    RunStats stats;
+};
+
 int64_t batch_output_size(const libgrpp_b200_batch_t *b)
 {
     int64_t n = 0;
@@ -289,17 +311,17 @@ int64_t batch_output_size(const libgrpp_b200_batch_t *b)
         }                                                    \
     } while (0)
 
-int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double *h_arep, double *h_sx, double *h_sy,
-                   double *h_sz, RunStats *stats)
+// Host preprocessing, upload and kernel arguments of one batch. With own_buffers the
+// plan allocates its device memory (kept until plan_destroy); otherwise it borrows the
+// device state's buffers and is valid until the next batch on that device.
+int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions &opt, bool own_buffers, Plan &P)
 {
-    set_error(0, "");
     int rc = 0;
-    DeviceState *stp = get_state(rc);
-    if (!stp) return rc;
-    DeviceState &st = *stp;
-    std::lock_guard<std::mutex> lk(st.mu);
     cudaStream_t s = st.stream;
     const int64_t nt = b->n_tasks;
+    P.st = &st;
+    P.n_tasks = nt;
+    P.opt = opt;
     if (nt == 0) return 0;
 
     // ---------------------------------------------------------------- validation
@@ -545,24 +567,35 @@ int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double 
     const size_t o_bs = pk.add(blk_shell), o_bo = pk.add(blk_oc), o_bco = pk.add(blk_cart_off), o_bso = pk.add(blk_sph_off),
                  o_poffp = pk.add(proj_off);
     std::vector<int8_t> stop_dummy;
-    GRPP_CUDA(st.in.ensure(pk.buf.size()));
-    GRPP_CUDA(cudaMemcpyAsync(st.in.p, pk.buf.data(), pk.buf.size(), cudaMemcpyHostToDevice, s));
-    void *ib = st.in.p;
+    DevBuf *bin = own_buffers ? &P.in : &st.in, *bscr = own_buffers ? &P.scratch : &st.scratch,
+           *bout = own_buffers ? &P.out : &st.out;
+    GRPP_CUDA(bin->ensure(pk.buf.size()));
+    GRPP_CUDA(cudaMemcpyAsync(bin->p, pk.buf.data(), pk.buf.size(), cudaMemcpyHostToDevice, s));
+    P.h2d_bytes = (int64_t)pk.buf.size();
+    void *ib = bin->p;
 
     // scratch: Q, S_prev, scr | S_cart, U_cart | S_sph, U_sph | status ; outputs: 4 x out_tot
     const int64_t qn = std::max<int64_t>(qtot, 1), cn = std::max<int64_t>(cart_tot, 1), sn = std::max<int64_t>(sph_tot, 1);
     const size_t scratch_bytes = (size_t)(3 * qn + 2 * cn + 2 * sn + 16) * sizeof(double);
-    GRPP_CUDA(st.scratch.ensure(scratch_bytes));
-    GRPP_CUDA(st.out.ensure((size_t)4 * std::max<int64_t>(out_tot, 1) * sizeof(double)));
-    double *Qd = (double *)st.scratch.p, *Spd = Qd + qn, *SCd = Spd + qn, *Scd = SCd + qn, *Ucd = Scd + cn, *Ssd = Ucd + cn,
+    GRPP_CUDA(bscr->ensure(scratch_bytes));
+    GRPP_CUDA(bout->ensure((size_t)4 * std::max<int64_t>(out_tot, 1) * sizeof(double)));
+    P.scratch_bytes = (int64_t)scratch_bytes;
+    double *Qd = (double *)bscr->p, *Spd = Qd + qn, *SCd = Spd + qn, *Scd = SCd + qn, *Ucd = Scd + cn, *Ssd = Ucd + cn,
            *Usd = Ssd + sn;
     int *statusd = (int *)(Usd + sn);
-    GRPP_CUDA(cudaMemsetAsync(statusd, 0, 16 * sizeof(int), s));
-    double *o_arep = (double *)st.out.p, *o_sx = o_arep + out_tot, *o_sy = o_sx + out_tot, *o_sz = o_sy + out_tot;
+    double *o_arep = (double *)bout->p, *o_sx = o_arep + out_tot, *o_sy = o_sx + out_tot, *o_sz = o_sy + out_tot;
 
     int nsm = 0;
     GRPP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, st.device));
-    GRPP_CUDA(cudaEventRecord(st.ev[0], s));
+    P.status = statusd;
+    P.out_tot = out_tot;
+    P.outs[0] = o_arep;
+    P.outs[1] = o_sx;
+    P.outs[2] = o_sy;
+    P.outs[3] = o_sz;
+    P.n_radial = (int64_t)rad_task.size();
+    P.n_mmd = (int64_t)items.size();
+    P.n_entries = qtot;
 
     // ---------------------------------------------------------------- 2. MMD
     if (!items.empty()) {
@@ -591,11 +624,11 @@ int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double 
         m.status = statusd;
         const int wpb = 4;
         const size_t smem = (size_t)wpb * mmd_ws_size(mmd_lmax, mmd_smax) * sizeof(double);
-        const int blocks = (int)std::min<int64_t>(((int64_t)items.size() + wpb - 1) / wpb, (int64_t)nsm * 16);
-        mmd_kernel<<<blocks, 32 * wpb, smem, s>>>(m);
-        GRPP_CUDA(cudaGetLastError());
+        P.mmd = m;
+        P.mmd_blocks = (int)std::min<int64_t>(((int64_t)items.size() + wpb - 1) / wpb, (int64_t)nsm * 16);
+        P.mmd_threads = 32 * wpb;
+        P.mmd_smem = smem;
     }
-    GRPP_CUDA(cudaEventRecord(st.ev[1], s));
 
     // ---------------------------------------------------------------- 3. outercore projections
     if (!blk_shell.empty()) {
@@ -612,8 +645,8 @@ int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double 
         o.U_cart = Ucd;
         o.S_sph = Ssd;
         o.U_sph = Usd;
-        oc_proj_kernel<<<(int)std::min<size_t>(blk_shell.size(), (size_t)nsm * 32), 64, 0, s>>>(o);
-        GRPP_CUDA(cudaGetLastError());
+        P.ocp = o;
+        P.ocp_blocks = (int)std::min<size_t>(blk_shell.size(), (size_t)nsm * 32);
     }
 
     // ---------------------------------------------------------------- 4. radial
@@ -654,11 +687,10 @@ int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double 
         r.fallback_count = statusd + 4;
         r.status = statusd;
         const size_t smem = (size_t)(1 + rad_npot + (rad_l1 + 1) + (rad_l2 + 1) + rad_dn) * kRadThreads * sizeof(double);
-        const int blocks = (int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 8);
-        radial_kernel<false><<<blocks, kRadThreads, smem, s>>>(r);
-        GRPP_CUDA(cudaGetLastError());
+        P.rad = r;
+        P.rad_blocks = (int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 8);
+        P.rad_smem = smem;
     }
-    GRPP_CUDA(cudaEventRecord(st.ev[2], s));
 
     // ---------------------------------------------------------------- 5. final assembly
     {
@@ -715,35 +747,132 @@ int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double 
         fs.n_q = fin_nq;
         fs.n_v = std::max(6144, 3 * nabmax);
         const size_t smem = (size_t)(2 * fs.n_rsh + 2 * fs.n_omega + fs.n_q + fs.n_v) * sizeof(double);
-        const int blocks = (int)std::min<int64_t>(nt, (int64_t)nsm * 8);
-        final_kernel<<<blocks, kFinThreads, smem, s>>>(f, fs);
+        P.fin = f;
+        P.fin_smem_layout = fs;
+        P.fin_blocks = (int)std::min<int64_t>(nt, (int64_t)nsm * 8);
+        P.fin_smem = smem;
+    }
+    return 0;
+}
+
+int plan_execute(Plan &P)
+{
+    DeviceState &st = *P.st;
+    cudaStream_t s = st.stream;
+    if (P.n_tasks == 0) return 0;
+    GRPP_CUDA(cudaMemsetAsync(P.status, 0, 16 * sizeof(int), s));
+    GRPP_CUDA(cudaEventRecord(st.ev[0], s));
+    if (P.mmd_blocks > 0) {
+        mmd_kernel<<<P.mmd_blocks, P.mmd_threads, P.mmd_smem, s>>>(P.mmd);
         GRPP_CUDA(cudaGetLastError());
     }
-    GRPP_CUDA(cudaEventRecord(st.ev[3], s));
-
-    // ---------------------------------------------------------------- results
-    GRPP_CUDA(cudaMemcpyAsync(h_arep, o_arep, out_tot * sizeof(double), cudaMemcpyDeviceToHost, s));
-    GRPP_CUDA(cudaMemcpyAsync(h_sx, o_sx, out_tot * sizeof(double), cudaMemcpyDeviceToHost, s));
-    GRPP_CUDA(cudaMemcpyAsync(h_sy, o_sy, out_tot * sizeof(double), cudaMemcpyDeviceToHost, s));
-    GRPP_CUDA(cudaMemcpyAsync(h_sz, o_sz, out_tot * sizeof(double), cudaMemcpyDeviceToHost, s));
-    int hstatus[16];
-    GRPP_CUDA(cudaMemcpyAsync(hstatus, statusd, sizeof(hstatus), cudaMemcpyDeviceToHost, s));
-    GRPP_CUDA(cudaStreamSynchronize(s));
-    if (stats) {
-        stats->n_tasks = nt;
-        stats->n_radial = (int64_t)rad_task.size();
-        stats->n_mmd = (int64_t)items.size();
-        stats->n_entries = qtot;
-        cudaEventElapsedTime(&stats->ms_mmd, st.ev[0], st.ev[1]);
-        cudaEventElapsedTime(&stats->ms_radial, st.ev[1], st.ev[2]);
-        cudaEventElapsedTime(&stats->ms_final, st.ev[2], st.ev[3]);
-        cudaEventElapsedTime(&stats->ms_total, st.ev[0], st.ev[3]);
+    GRPP_CUDA(cudaEventRecord(st.ev[1], s));
+    if (P.ocp_blocks > 0) {
+        oc_proj_kernel<<<P.ocp_blocks, 64, 0, s>>>(P.ocp);
+        GRPP_CUDA(cudaGetLastError());
     }
+    if (P.rad_blocks > 0) {
+        if (P.opt.radial_mode == LIBGRPP_B200_RADIAL_LEARNED) radial_kernel<true><<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(P.rad);
+        else radial_kernel<false><<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(P.rad);
+        GRPP_CUDA(cudaGetLastError());
+    }
+    GRPP_CUDA(cudaEventRecord(st.ev[2], s));
+    final_kernel<<<P.fin_blocks, kFinThreads, P.fin_smem, s>>>(P.fin, P.fin_smem_layout);
+    GRPP_CUDA(cudaGetLastError());
+    GRPP_CUDA(cudaEventRecord(st.ev[3], s));
+    int hstatus[16];
+    GRPP_CUDA(cudaMemcpyAsync(hstatus, P.status, sizeof(hstatus), cudaMemcpyDeviceToHost, s));
+    GRPP_CUDA(cudaStreamSynchronize(s));
+    cudaEventElapsedTime(&P.stats.ms_mmd, st.ev[0], st.ev[1]);
+    cudaEventElapsedTime(&P.stats.ms_radial, st.ev[1], st.ev[2]);
+    cudaEventElapsedTime(&P.stats.ms_final, st.ev[2], st.ev[3]);
+    cudaEventElapsedTime(&P.stats.ms_total, st.ev[0], st.ev[3]);
+    P.stats.n_tasks = P.n_tasks;
+    P.stats.n_radial = P.n_radial;
+    P.stats.n_mmd = P.n_mmd;
+    P.stats.n_entries = P.n_entries;
     if (hstatus[0] != 0) {
         set_error(LIBGRPP_B200_ERR_INVALID, "a kernel reported an index beyond its table limits");
         return LIBGRPP_B200_ERR_INVALID;
     }
     return 0;
 }
+
+int plan_download(Plan &P, double *h_arep, double *h_sx, double *h_sy, double *h_sz)
+{
+    if (P.n_tasks == 0) return 0;
+    cudaStream_t s = P.st->stream;
+    double *h[4] = {h_arep, h_sx, h_sy, h_sz};
+    for (int k = 0; k < 4; k++)
+        if (h[k]) GRPP_CUDA(cudaMemcpyAsync(h[k], P.outs[k], P.out_tot * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GRPP_CUDA(cudaStreamSynchronize(s));
+    return 0;
+}
+
+int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double *h_arep, double *h_sx, double *h_sy,
+                   double *h_sz, RunStats *stats)
+{
+    set_error(0, "");
+    int rc = 0;
+    DeviceState *stp = get_state(rc);
+    if (!stp) return rc;
+    std::lock_guard<std::mutex> lk(stp->mu);
+    Plan P;
+    rc = plan_build(*stp, b, opt, false, P);
+    if (rc) return rc;
+    rc = plan_execute(P);
+    if (rc) return rc;
+    rc = plan_download(P, h_arep, h_sx, h_sy, h_sz);
+    if (stats) *stats = P.stats;
+    return rc;
+}
+
+Plan *plan_create(const libgrpp_b200_batch_t *b, const RunOptions &opt)
+{
+    set_error(0, "");
+    int rc = 0;
+    DeviceState *stp = get_state(rc);
+    if (!stp) return nullptr;
+    std::lock_guard<std::mutex> lk(stp->mu);
+    Plan *P = new Plan();
+    rc = plan_build(*stp, b, opt, true, *P);
+    if (rc == 0) rc = cudaStreamSynchronize(stp->stream) == cudaSuccess ? 0 : LIBGRPP_B200_ERR_CUDA;
+    if (rc) {
+        plan_destroy(P);
+        return nullptr;
+    }
+    return P;
+}
+
+int plan_run(Plan *P)
+{
+    set_error(0, "");
+    std::lock_guard<std::mutex> lk(P->st->mu);
+    return plan_execute(*P);
+}
+
+int plan_outputs(Plan *P, double *h_arep, double *h_sx, double *h_sy, double *h_sz)
+{
+    std::lock_guard<std::mutex> lk(P->st->mu);
+    return plan_download(*P, h_arep, h_sx, h_sy, h_sz);
+}
+
+const RunStats *plan_stats(const Plan *P) { return &P->stats; }
+int64_t plan_h2d_bytes(const Plan *P) { return P->h2d_bytes; }
+
+int set_device(int device)
+{
+    GRPP_CUDA(cudaSetDevice(device));
+    return 0;
+}
+
+void plan_destroy(Plan *P)
+{
+    if (!P) return;
+    for (DevBuf *d : {&P->in, &P->scratch, &P->out})
+        if (d->p) cudaFree(d->p);
+    delete P;
+}
+
 
 }  // namespace grpp

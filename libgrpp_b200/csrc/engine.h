@@ -30,4 +30,15 @@ int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double 
 
 int64_t batch_output_size(const libgrpp_b200_batch_t *b);
 
+// A batch prepared on the device (inputs uploaded, work lists built, buffers owned):
+// execute any number of times, read the outputs, destroy.
+struct Plan;
+Plan *plan_create(const libgrpp_b200_batch_t *b, const RunOptions &opt);
+int plan_run(Plan *P);
+int plan_outputs(Plan *P, double *arep, double *so_x, double *so_y, double *so_z);
+void plan_destroy(Plan *P);
+const RunStats *plan_stats(const Plan *P);
+int64_t plan_h2d_bytes(const Plan *P);
+int set_device(int device);
+
 }  // namespace grpp
