@@ -185,7 +185,13 @@ def run_ours(args, rank, world, local):
 
     idxs = [(rank + world * s) % 100 for s in range(args.steps)]
     S = system()
-    batches = [S.batch(*step_tasks(i)) for i in idxs]
+    batches = []
+    for i in idxs:
+        a, b, c = step_tasks(i)
+        if args.tasks_per_step and args.tasks_per_step < len(a):
+            sel = np.linspace(0, len(a) - 1, args.tasks_per_step).astype(np.int64)
+            a, b, c = a[sel], b[sel], c[sel]
+        batches.append(S.batch(a, b, c))
     plans = [lib.plan(b, mode) for b in batches]
     n_tasks = [len(b.task_a) for b in batches]
 
@@ -197,6 +203,7 @@ def run_ours(args, rank, world, local):
         dist.barrier()
     torch.cuda.synchronize()
     ms, kms = [], {"ms_type1": 0.0, "ms_radial": 0.0, "ms_assembly": 0.0}
+    cnt = None
     with ClockSampler(local) as clk:
         for p in plans:
             flush.fill_(1.0)
@@ -206,6 +213,8 @@ def run_ours(args, rank, world, local):
             ms.append(st["ms_total"])
             for k in kms:
                 kms[k] += st[k]
+            c = p.counters()
+            cnt = c if cnt is None else {k: cnt[k] + c[k] for k in c}
     torch.cuda.synchronize()
     total_ms = float(sum(ms))
     tasks = float(sum(n_tasks))
@@ -257,7 +266,9 @@ def run_ours(args, rank, world, local):
         line["cpu_baseline"] = {"value": rate, "unit": "tasks/s", "cores": threads, "kind": "reference",
                                 "sample": f"{args.ref_sample} seeded random tasks of the first step's block "
                                           f"({dt:.1f} s on {threads} threads)"}
-    line["roofline"] = roofline(args, dominant, kernel_ms)
+    peak = lib.fp64_peak()
+    per_step = {k: v / len(plans) for k, v in cnt.items()} if cnt else None
+    line["roofline"] = roofline(args, dominant, kernel_ms, per_step, peak)
     for p in plans:
         p.close()
     if rank == 0:
@@ -267,9 +278,38 @@ def run_ours(args, rank, world, local):
         dist.destroy_process_group()
 
 
-def roofline(args, dominant, kernel_ms):
-    return {"bound": "fp64", "kernel": dominant, "achieved": None, "peak": None, "unit": "TFLOP/s", "frac": None,
-            "traffic": None, "note": "algorithmic FLOP model pending"}
+# FLOP model of the radial path (count of FP64 add/mul, FMA = 2, each exp/pow/sqrt/log/erf = 1,
+# per operation of libgrpp's algorithm, libgrpp/radial_type2_integral.c and screening.c):
+RADIAL_FLOPS = {
+    "points": 15,      # Log3 abscissa and weight of one grid point
+    "term_pts": 6,     # c r^(n-2) exp(-zeta r^2) for one potential term at one point
+    "prim_pts": 6,     # c exp(-a (r-CA)^2) and k r for one primitive at one point
+    "bessel": 18,      # 4th-order Taylor M_l(x) (16) and F += e M (2)
+    "pow_pts": 1,      # r^N
+    "accum": 5,        # S += w U F1 F2 r^N
+    "scr_combos": 12,  # setup and contribution of one primitive screening estimate
+    "scr_iters": 80,   # one fixed-point step: 4 M_l evaluations, 2 ratios, sqrt
+    "scr_final": 57,   # the envelope: 2 M_l, exp, erf, pow, sqrt
+}
+
+
+def radial_flops(counters):
+    return float(sum(RADIAL_FLOPS[k] * counters[k] for k in RADIAL_FLOPS))
+
+
+def roofline(args, dominant, kernel_ms, counters, peak_tflops):
+    """FP64 roofline of the dominant kernel. bound is "fp64": the radial quadrature is
+    compute bound on the FP64 pipe (no dense contraction, a few kB of input per task)."""
+    out = {"bound": "fp64", "kernel": dominant, "unit": "TFLOP/s", "peak": peak_tflops,
+           "peak_source": "measured in this run (FP64 FMA microkernel, all SMs)", "traffic": None}
+    if dominant == "ms_radial" and counters is not None:
+        fl = radial_flops(counters)
+        ach = fl / (kernel_ms["ms_radial"] * 1e-3) / 1e12
+        out.update({"achieved": ach, "frac": ach / peak_tflops if peak_tflops else None,
+                    "flops_per_launch": fl, "counters": counters})
+    else:
+        out.update({"achieved": None, "frac": None})
+    return out
 
 
 def main():
@@ -282,6 +322,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-sample", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tasks-per-step", type=int, default=0,
+                    help="evenly spaced subset of each step's tasks (profiling runs); 0 = the full block")
     args = ap.parse_args()
     rank, world, local = get_env()
     if args.impl == "reference":

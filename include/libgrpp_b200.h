@@ -104,6 +104,10 @@ int libgrpp_b200_full_grpp_batch(const libgrpp_b200_batch_t *batch, int radial_m
  * CUDA runtime state; default device 0). Returns a status code. */
 int libgrpp_b200_set_device(int device);
 
+/* Measured FP64 FMA throughput of the current device in TFLOP/s (8 independent FMA chains
+ * per thread, all SMs busy): the denominator of this engine's roofline. */
+int libgrpp_b200_fp64_peak(double *tflops);
+
 /* A batch prepared once on the device: inputs uploaded and work lists built, device
  * buffers owned by the plan. execute() runs the kernels only (outputs stay on the
  * device until outputs() copies them to host arrays). Not thread-safe per plan. */
@@ -115,6 +119,10 @@ int libgrpp_b200_plan_outputs(libgrpp_b200_plan_t *plan, double *arep, double *s
 /* ms[4] = kernel time of the last execute(): total, type 1, radial, assembly (CUDA events on the
  * engine stream); counts[5] = tasks, radial tasks, type 1 work items, radial entries, bytes uploaded */
 int libgrpp_b200_plan_stats(const libgrpp_b200_plan_t *plan, double *ms, int64_t *counts);
+/* operation counters of the radial kernel in the last execute() (n <= 16 slots): screening and
+ * grid-walk SM cycles, tasks, integrand points, Bessel evaluations, primitive Gaussians, potential
+ * terms, r^N powers, entry x point accumulations, screening estimates / iterations / envelopes, levels */
+int libgrpp_b200_plan_counters(const libgrpp_b200_plan_t *plan, uint64_t *counters, int n);
 void libgrpp_b200_plan_destroy(libgrpp_b200_plan_t *plan);
 
 #ifdef __cplusplus

@@ -78,11 +78,13 @@ class LibGRPP:
         self._opt("libgrpp_b200_last_error_message", ct.c_char_p, [])
         self._opt("libgrpp_b200_full_grpp_batch", ct.c_int, [_V, ct.c_int, _D, _D, _D, _D])
         self._opt("libgrpp_b200_set_device", ct.c_int, [ct.c_int])
+        self._opt("libgrpp_b200_fp64_peak", ct.c_int, [_D])
         self._opt("libgrpp_b200_plan_create", _V, [_V, ct.c_int])
         self._opt("libgrpp_b200_plan_execute", ct.c_int, [_V])
         self._opt("libgrpp_b200_plan_outputs", ct.c_int, [_V, _D, _D, _D, _D])
         self._opt("libgrpp_b200_plan_stats", ct.c_int, [_V, _D, ct.POINTER(ct.c_int64)])
         self._opt("libgrpp_b200_plan_destroy", None, [_V])
+        self._opt("libgrpp_b200_plan_counters", ct.c_int, [_V, ct.POINTER(ct.c_uint64), ct.c_int])
         self.lib.libgrpp_init()
 
     def _opt(self, name, res, args):
@@ -194,6 +196,13 @@ class LibGRPP:
         if rc != 0:
             raise RuntimeError(f"libgrpp_b200_set_device({device}) failed: {self.last_error_message()}")
 
+    def fp64_peak(self) -> float:
+        v = ct.c_double(0.0)
+        rc = self.lib.libgrpp_b200_fp64_peak(ct.byref(v))
+        if rc != 0:
+            raise RuntimeError(self.last_error_message())
+        return v.value
+
     def plan(self, batch, radial_mode=0) -> "Plan":
         return Plan(self, batch, radial_mode)
 
@@ -257,6 +266,14 @@ class Plan:
         return {"ms_total": ms[0], "ms_type1": ms[1], "ms_radial": ms[2], "ms_assembly": ms[3],
                 "n_tasks": int(cnt[0]), "n_radial": int(cnt[1]), "n_type1_items": int(cnt[2]),
                 "n_entries": int(cnt[3]), "h2d_bytes": int(cnt[4])}
+
+    COUNTERS = ("screen_cycles", "quad_cycles", "items", "points", "bessel", "prim_pts", "term_pts", "pow_pts",
+                "accum", "scr_combos", "scr_iters", "scr_final", "levels")
+
+    def counters(self):
+        c = np.zeros(len(self.COUNTERS), dtype=np.uint64)
+        self.lib.lib.libgrpp_b200_plan_counters(self.h, c.ctypes.data_as(ct.POINTER(ct.c_uint64)), len(c))
+        return {k: int(v) for k, v in zip(self.COUNTERS, c)}
 
     def close(self):
         if self.h:

@@ -651,6 +651,8 @@ int libgrpp_b200_full_grpp_batch(const libgrpp_b200_batch_t *b, int radial_mode,
 
 int libgrpp_b200_set_device(int device) { return grpp::set_device(device); }
 
+int libgrpp_b200_fp64_peak(double *tflops) { return grpp::measure_fp64_peak(tflops); }
+
 libgrpp_b200_plan_t *libgrpp_b200_plan_create(const libgrpp_b200_batch_t *b, int radial_mode)
 {
     if (!check_init()) return nullptr;
@@ -691,6 +693,14 @@ int libgrpp_b200_plan_stats(const libgrpp_b200_plan_t *plan, double *ms, int64_t
         counts[3] = st->n_entries;
         counts[4] = grpp::plan_h2d_bytes((const grpp::Plan *)plan);
     }
+    return 0;
+}
+
+int libgrpp_b200_plan_counters(const libgrpp_b200_plan_t *plan, uint64_t *counters, int n)
+{
+    if (!plan || n < 0 || n > 16) return LIBGRPP_B200_ERR_INVALID;
+    const grpp::RunStats *st = grpp::plan_stats((const grpp::Plan *)plan);
+    for (int i = 0; i < n; i++) counters[i] = st->radial_counters[i];
     return 0;
 }
 

@@ -127,8 +127,8 @@ int init_device_state(DeviceState &st, int device)
     for (auto &e : st.ev) GRPP_CUDA(cudaEventCreate(&e));
     st.atab_off.assign((kMaxL + 2) * (kMaxL + 2), -1);
     GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    GRPP_CUDA(cudaFuncSetAttribute(radial_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-    GRPP_CUDA(cudaFuncSetAttribute(radial_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(radial_walk_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(radial_walk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     st.device = device;
     st.ready = true;
@@ -281,13 +281,14 @@ struct Plan {
     DevBuf in, scratch, out;
     double *outs[4] = {nullptr, nullptr, nullptr, nullptr};
     int *status = nullptr;
+    unsigned long long *counters = nullptr;  // kRadCntNum slots inside the status area
     MmdArgs mmd;
     int mmd_blocks = 0, mmd_threads = 128;
     size_t mmd_smem = 0;
     OcProjArgs ocp;
     int ocp_blocks = 0;
     RadialArgs rad;
-    int rad_blocks = 0;
+    int rad_blocks = 0, scr_blocks = 0;
     size_t rad_smem = 0;
     FinalArgs fin;
     FinalSmem fin_smem_layout;
@@ -576,18 +577,23 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
 
     // scratch: Q, S_prev, scr | S_cart, U_cart | S_sph, U_sph | status ; outputs: 4 x out_tot
     const int64_t qn = std::max<int64_t>(qtot, 1), cn = std::max<int64_t>(cart_tot, 1), sn = std::max<int64_t>(sph_tot, 1);
-    const size_t scratch_bytes = (size_t)(3 * qn + 2 * cn + 2 * sn + 16) * sizeof(double);
+    const int64_t nrad = std::max<int64_t>((int64_t)rad_task.size(), 1);
+    const int64_t flag_words = (qn + nrad + 2 * 8) / 8 + 1;  // entry flags + per-task walk flags, in doubles
+    const size_t scratch_bytes = (size_t)(3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words) * sizeof(double);
     GRPP_CUDA(bscr->ensure(scratch_bytes));
     GRPP_CUDA(bout->ensure((size_t)4 * std::max<int64_t>(out_tot, 1) * sizeof(double)));
     P.scratch_bytes = (int64_t)scratch_bytes;
     double *Qd = (double *)bscr->p, *Spd = Qd + qn, *SCd = Spd + qn, *Scd = SCd + qn, *Ucd = Scd + cn, *Ssd = Ucd + cn,
            *Usd = Ssd + sn;
     int *statusd = (int *)(Usd + sn);
+    uint8_t *eflagd = (uint8_t *)(Usd + sn + 32);
+    uint8_t *walkd = eflagd + qn;
     double *o_arep = (double *)bout->p, *o_sx = o_arep + out_tot, *o_sy = o_sx + out_tot, *o_sz = o_sy + out_tot;
 
     int nsm = 0;
     GRPP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, st.device));
     P.status = statusd;
+    P.counters = (unsigned long long *)(statusd + 16);
     P.out_tot = out_tot;
     P.outs[0] = o_arep;
     P.outs[1] = o_sx;
@@ -686,9 +692,13 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         r.pred_level = nullptr;
         r.fallback_count = statusd + 4;
         r.status = statusd;
-        const size_t smem = (size_t)(1 + rad_npot + (rad_l1 + 1) + (rad_l2 + 1) + rad_dn) * kRadThreads * sizeof(double);
+        r.counters = (unsigned long long *)(statusd + 16);
+        r.eflag = eflagd;
+        r.walk = walkd;
+        const size_t smem = (size_t)(rad_npot + (rad_l1 + 1) + (rad_l2 + 1) + rad_dn) * kRadRow * sizeof(double);
         P.rad = r;
-        P.rad_blocks = (int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 8);
+        P.rad_blocks = (int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 16);
+        P.scr_blocks = (int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 32);
         P.rad_smem = smem;
     }
 
@@ -760,7 +770,7 @@ int plan_execute(Plan &P)
     DeviceState &st = *P.st;
     cudaStream_t s = st.stream;
     if (P.n_tasks == 0) return 0;
-    GRPP_CUDA(cudaMemsetAsync(P.status, 0, 16 * sizeof(int), s));
+    GRPP_CUDA(cudaMemsetAsync(P.status, 0, 16 * sizeof(int) + kRadCntNum * sizeof(unsigned long long), s));
     GRPP_CUDA(cudaEventRecord(st.ev[0], s));
     if (P.mmd_blocks > 0) {
         mmd_kernel<<<P.mmd_blocks, P.mmd_threads, P.mmd_smem, s>>>(P.mmd);
@@ -772,8 +782,12 @@ int plan_execute(Plan &P)
         GRPP_CUDA(cudaGetLastError());
     }
     if (P.rad_blocks > 0) {
-        if (P.opt.radial_mode == LIBGRPP_B200_RADIAL_LEARNED) radial_kernel<true><<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(P.rad);
-        else radial_kernel<false><<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(P.rad);
+        radial_screen_kernel<<<P.scr_blocks, kRadThreads, 0, s>>>(P.rad);
+        GRPP_CUDA(cudaGetLastError());
+        if (P.opt.radial_mode == LIBGRPP_B200_RADIAL_LEARNED)
+            radial_walk_kernel<true><<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(P.rad);
+        else
+            radial_walk_kernel<false><<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(P.rad);
         GRPP_CUDA(cudaGetLastError());
     }
     GRPP_CUDA(cudaEventRecord(st.ev[2], s));
@@ -782,6 +796,8 @@ int plan_execute(Plan &P)
     GRPP_CUDA(cudaEventRecord(st.ev[3], s));
     int hstatus[16];
     GRPP_CUDA(cudaMemcpyAsync(hstatus, P.status, sizeof(hstatus), cudaMemcpyDeviceToHost, s));
+    GRPP_CUDA(cudaMemcpyAsync(P.stats.radial_counters, P.counters, kRadCntNum * sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, s));
     GRPP_CUDA(cudaStreamSynchronize(s));
     cudaEventElapsedTime(&P.stats.ms_mmd, st.ev[0], st.ev[1]);
     cudaEventElapsedTime(&P.stats.ms_radial, st.ev[1], st.ev[2]);
@@ -855,6 +871,47 @@ int plan_outputs(Plan *P, double *h_arep, double *h_sx, double *h_sy, double *h_
 {
     std::lock_guard<std::mutex> lk(P->st->mu);
     return plan_download(*P, h_arep, h_sx, h_sy, h_sz);
+}
+
+// FP64 FMA throughput: 8 independent chains per thread keep the pipes busy; the
+// measured rate is the denominator of the engine's FP64 roofline.
+__global__ void fp64_peak_kernel(double *out, int iters, double a, double b)
+{
+    double x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = threadIdx.x * 1e-9 + k;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) x[k] = fma(x[k], a, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += x[k];
+    if (s == 12345.678) out[0] = s;  // keeps the chains live; never true for these inputs
+}
+
+int measure_fp64_peak(double *tflops)
+{
+    int rc = 0;
+    DeviceState *stp = get_state(rc);
+    if (!stp) return rc;
+    std::lock_guard<std::mutex> lk(stp->mu);
+    cudaStream_t s = stp->stream;
+    int nsm = 0;
+    GRPP_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, stp->device));
+    double *d = nullptr;
+    GRPP_CUDA(cudaMalloc(&d, sizeof(double)));
+    const int threads = 256, blocks = nsm * 8, iters = 4096;
+    fp64_peak_kernel<<<blocks, threads, 0, s>>>(d, 64, 0.999999, 1e-7);
+    GRPP_CUDA(cudaEventRecord(stp->ev[4], s));
+    fp64_peak_kernel<<<blocks, threads, 0, s>>>(d, iters, 0.999999, 1e-7);
+    GRPP_CUDA(cudaEventRecord(stp->ev[5], s));
+    GRPP_CUDA(cudaEventSynchronize(stp->ev[5]));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, stp->ev[4], stp->ev[5]);
+    cudaFree(d);
+    *tflops = 2.0 * 8.0 * iters * (double)threads * blocks / (ms * 1e-3) / 1e12;
+    return 0;
 }
 
 const RunStats *plan_stats(const Plan *P) { return &P->stats; }

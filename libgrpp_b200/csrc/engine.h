@@ -17,6 +17,7 @@ struct RunStats {
     int64_t n_tasks = 0, n_radial = 0, n_mmd = 0, n_entries = 0;
     int64_t fallbacks = 0;
     float ms_total = 0.f, ms_mmd = 0.f, ms_radial = 0.f, ms_final = 0.f;
+    unsigned long long radial_counters[16] = {0};  // RadialCounter slots (radial.cuh)
 };
 
 // thread-local last error
@@ -40,5 +41,6 @@ void plan_destroy(Plan *P);
 const RunStats *plan_stats(const Plan *P);
 int64_t plan_h2d_bytes(const Plan *P);
 int set_device(int device);
+int measure_fp64_peak(double *tflops);
 
 }  // namespace grpp

@@ -12,15 +12,20 @@
 //     r_i = -5 ln(1 - x_i^3), levels of 31, 63, ..., 8191 points, stopping when
 //     |S_L - S_{L-1}| <= 1e-16 unless |S|/|estimate| < 1e-3, capped at 8191 points.
 //
-// GPU mapping: one CTA per task. Phase 1: each warp screens whole entries,
-// its lanes evaluating 32 primitive triples at a time, and stops at the first
-// chunk that contains a failing triple (libgrpp stops at the first failing one;
-// the outcome is the same). Phase 2: the grid is walked level by level in
-// chunks of one point per thread; a point's integrand values
-//   w U_p(r) for every potential, F^A_l, F^B_l for every order, r^N,
-// are evaluated once and shared by all potentials and entries; every thread
-// then advances the running sums of the entries it owns, point by point in the
-// reference's order and association ((((w U) F1) F2) r^N).
+// GPU mapping, two kernels:
+//  * radial_screen_kernel: one CTA per task, one thread per entry. A thread
+//    walks the primitive triples (i, j, k) of its entry in libgrpp's order and
+//    stops at the first failing one, exactly as libgrpp does, so the estimate
+//    and the gate decision are those of the reference, and no work is spent on
+//    triples libgrpp never evaluates. One-centre tasks get their analytic
+//    table here and need no grid walk.
+//  * radial_walk_kernel: one CTA per task that has entries left. The grid is
+//    walked level by level in chunks of one point per thread; a point's
+//    integrand values
+//      w U_p(r) for every potential, F^A_l, F^B_l for every order, r^N,
+//    are evaluated once and shared by all potentials and entries; every thread
+//    then advances the running sums of the entries it owns, point by point in
+//    the reference's order and association ((((w U) F1) F2) r^N).
 #pragma once
 
 #include "grpp_common.cuh"
@@ -60,10 +65,32 @@ struct RadialArgs {
     const int64_t *q_off;       // per item
     double *Q;                  // table values (running sums during the walk)
     double *S_prev, *scr;       // per entry scratch, same indexing as Q
+    uint8_t *eflag;             // per entry: kEntActive | kEntScrOk
+    uint8_t *walk;              // per item: 1 if the grid walk has work
     int8_t *stop_level;         // per item: deepest level walked (learning labels), may be null
     const int8_t *pred_level;   // per item: predicted level (learned mode), may be null
     int *fallback_count;        // learned mode: items that needed more than predicted+1
     int *status;
+    // operation counters (accumulated per CTA, one atomic add per item), see kRadCnt*
+    unsigned long long *counters;
+};
+
+// counter slots: the FLOP model of the radial path is built from these counts
+enum RadialCounter {
+    kRadCntScreenCycles = 0,   // SM clock cycles spent in screening (sum over CTAs)
+    kRadCntQuadCycles,         // SM clock cycles spent in the grid walk
+    kRadCntItems,              // tasks through the grid walk
+    kRadCntPoints,             // integrand points evaluated
+    kRadCntBessel,             // M_l(x) evaluations of the integrand (points x prims x orders)
+    kRadCntPrimPts,            // primitive Gaussians evaluated (points x prims)
+    kRadCntTermPts,            // potential terms evaluated (points x terms)
+    kRadCntPowPts,             // r^N evaluations (points x (la+lb+1))
+    kRadCntAccum,              // entry x point accumulations
+    kRadCntScrCombos,          // primitive screening estimates started
+    kRadCntScrIters,           // fixed-point iterations of the screening
+    kRadCntScrFinal,           // screening envelopes evaluated
+    kRadCntLevels,             // grid levels walked (sum over tasks)
+    kRadCntNum
 };
 
 struct RadialShared {
@@ -82,16 +109,29 @@ struct RadialShared {
 
 // ---- screening (screening.c:243-362) ------------------------------------------
 
-__device__ __forceinline__ double scr_ratio(int l, double x)
+// M_a(x) / M_b(x) for the adjacent orders (a, b) = (1, 0) if l = 0, else (l-1, l), both
+// from one table row (screening.c:332-346 evaluates them as two separate calls)
+__device__ __noinline__ double scr_ratio(int l, double x)
 {
-    return l == 0 ? bessel_scaled(1, x) / bessel_scaled(0, x) : bessel_scaled(l - 1, x) / bessel_scaled(l, x);
+    const int na = l == 0 ? 1 : l - 1, nb = l == 0 ? 0 : l;
+    if (x <= 1e-7) return bessel_small(na, x) / bessel_small(nb, x);
+    if (x <= 16.0) {
+        const int i0 = (int)(round(x * 100) + 1e-5);
+        const double dx = x - i0 * 0.01;
+        const double *row = c_tab.bessel + (size_t)i0 * kBesL * 5;
+        return taylor4(row + 5 * na, dx) / taylor4(row + 5 * nb, dx);
+    }
+    return bessel_asym(na, x) / bessel_asym(nb, x);
 }
+
+__device__ __noinline__ double bessel_scaled_nl(int n, double x) { return bessel_scaled(n, x); }
 
 // returns true on failure; *val is the primitive estimate
 __device__ inline bool scr_prim(int l1, int l2, int n, double CA2, double CB2, double aA, double aB, double k1,
-                                double k2, double eta, double *val)
+                                double k2, double eta, double *val, int *iters)
 {
     *val = 0.0;
+    *iters = 0;
     if (l1 >= 1 && fabs(k1) <= kZeroThresh) return false;
     if (l2 >= 1 && fabs(k2) <= kZeroThresh) return false;
     const double p = aA + aB + eta, CA = sqrt(CA2), CB = sqrt(CB2);
@@ -123,9 +163,11 @@ __device__ inline bool scr_prim(int l1, int l2, int n, double CA2, double CB2, d
         if (l1 > 0) a = a - l1 - 1;
         if (l2 > 0) a = a - l2 - 1;
         r0 = sqrt(a / (2.0 * p));
+        *iters = steps;
     } while (fabs(r0 - r0p) > 1e-2);
-    *val = sqrt(kPi / p) * pow(r0, n) * bessel_scaled(l1, k1 * r0) * bessel_scaled(l2, k2 * r0) *
+    *val = sqrt(kPi / p) * pow(r0, n) * bessel_scaled_nl(l1, k1 * r0) * bessel_scaled_nl(l2, k2 * r0) *
            exp(-eta * r0 * r0 - aA * (r0 - CA) * (r0 - CA) - aB * (r0 - CB) * (r0 - CB)) * 0.5 * (1 + erf(sqrt(p) * r0));
+    *iters = -*iters - 1;  // negative: the envelope was evaluated
     return false;
 }
 
@@ -151,172 +193,240 @@ __device__ __forceinline__ void log3_point(int i, int nr, double &r, double &w)
     r = -R * ln;
 }
 
-template <bool LEARNED>
-__global__ void __launch_bounds__(kRadThreads) radial_kernel(RadialArgs a)
+
+// task geometry, primitives and potential terms into shared memory
+__device__ void load_task(const RadialArgs &a, int item, RadialShared &sh, int tid, int nthr)
+{
+    const int t = a.item_task[item];
+    const int sa = a.task_a[t], sb = a.task_b[t], c = a.task_c[t];
+    if (tid == 0) {
+        const double *Ao = a.shell_origin + 3 * sa, *Bo = a.shell_origin + 3 * sb, *Co = a.centre_origin + 3 * c;
+        double CAv[3], CBv[3];
+        for (int d = 0; d < 3; d++) {
+            CAv[d] = Co[d] - Ao[d];
+            CBv[d] = Co[d] - Bo[d];
+        }
+        const double CA2 = CAv[0] * CAv[0] + CAv[1] * CAv[1] + CAv[2] * CAv[2];
+        const double CB2 = CBv[0] * CBv[0] + CBv[1] * CBv[1] + CBv[2] * CBv[2];
+        sh.one_centre = CA2 < 1e-14 && CB2 < 1e-14;
+        sh.CA = sqrt(CA2);
+        sh.CB = sqrt(CB2);
+        sh.la = a.shell_L[sa];
+        sh.lb = a.shell_L[sb];
+        sh.d_n = sh.la + sh.lb + 1;
+        const int g = a.centre_grpp[c];
+        sh.npot = a.grpp_sl_n[g];
+        int e = 0, nt = 0, l1m = 0, l2m = 0;
+        for (int p = 0; p < sh.npot; p++) {
+            const int pot = a.sl_pot[a.grpp_sl_off[g] + p];
+            sh.pL[p] = a.pot_L[pot];
+            sh.pn[p] = a.pot_nprim[pot];
+            sh.poff[p] = nt;
+            for (int k = 0; k < sh.pn[p]; k++) {
+                const int o = a.pot_prim_off[pot] + k;
+                sh.tpow[nt] = a.pot_powers[o];
+                sh.tcoef[nt] = a.pot_coef[o];
+                sh.talpha[nt] = a.pot_alpha[o];
+                nt++;
+            }
+            sh.pent[p] = e;
+            e += (sh.pL[p] + sh.la + 1) * (sh.pL[p] + sh.lb + 1) * sh.d_n;
+            l1m = max(l1m, sh.pL[p] + sh.la);
+            l2m = max(l2m, sh.pL[p] + sh.lb);
+        }
+        sh.pent[sh.npot] = e;
+        sh.n_entries = e;
+        sh.nterm_tot = nt;
+        sh.l1max_all = l1m;
+        sh.l2max_all = l2m;
+        sh.np_a = a.rp_n[sa];
+        sh.np_b = a.rp_n[sb];
+    }
+    __syncthreads();
+    for (int i = tid; i < sh.np_a; i += nthr) {
+        sh.ca[i] = a.rp_coef[a.rp_off[sa] + i];
+        sh.xa[i] = a.rp_alpha[a.rp_off[sa] + i];
+        sh.ka[i] = 2.0 * sh.xa[i] * sh.CA;
+    }
+    for (int i = tid; i < sh.np_b; i += nthr) {
+        sh.cb[i] = a.rp_coef[a.rp_off[sb] + i];
+        sh.xb[i] = a.rp_alpha[a.rp_off[sb] + i];
+        sh.kb[i] = 2.0 * sh.xb[i] * sh.CB;
+    }
+    __syncthreads();
+}
+
+// analytic one-centre entry (radial_type2_integral.c:126-155): only l1 = l2 = 0 is non-zero
+__device__ double one_centre_entry(const RadialArgs &a, const RadialShared &sh, int sa, int sb, int p, int l1, int l2, int N)
+{
+    double v = 0.0;
+    if (l1 != 0 || l2 != 0) return 0.0;
+    const int na = a.shell_nprim[sa], nb = a.shell_nprim[sb];
+    const double *pca = a.prim_coef + a.shell_prim_off[sa], *pxa = a.prim_alpha + a.shell_prim_off[sa];
+    const double *pcb = a.prim_coef + a.shell_prim_off[sb], *pxb = a.prim_alpha + a.shell_prim_off[sb];
+    for (int i = 0; i < na; i++) {
+        const double ci = pca[i] * gaussian_norm(sh.la, pxa[i]);
+        for (int j = 0; j < nb; j++) {
+            const double cj = pcb[j] * gaussian_norm(sh.lb, pxb[j]);
+            for (int k = 0; k < sh.pn[p]; k++) {
+                const int tk = sh.poff[p] + k;
+                const double pp = pxa[i] + pxb[j] + sh.talpha[tk];
+                const double f = ci * cj * sh.tcoef[tk];
+                const int n = sh.tpow[tk] + N;
+                double gi;
+                if (n % 2 == 0) {
+                    const int kk = n / 2;
+                    gi = dfact(2 * kk - 1) / (pow(2.0, kk + 1) * pow(pp, kk)) * sqrt(kPi / pp);
+                } else {
+                    const int kk = (n - 1) / 2;
+                    double fct = 1.0;
+                    for (int q = 2; q <= kk; q++) fct *= q;
+                    gi = fct / (2.0 * pow(pp, kk + 1));
+                }
+                v += f * gi;
+            }
+        }
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(kRadThreads) radial_screen_kernel(RadialArgs a)
 {
     __shared__ RadialShared sh;
-    __shared__ uint8_t eflag[kRadMaxEntries];
-    extern __shared__ double chunk[];  // [1 + npot + l1max+1 + l2max+1 + dn][kRadThreads]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = kRadThreads / 32;
-
+    const int tid = threadIdx.x, lane = tid & 31;
     for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
+        __syncthreads();
+        load_task(a, item, sh, tid, kRadThreads);
         const int t = a.item_task[item];
-        const int sa = a.task_a[t], sb = a.task_b[t], c = a.task_c[t];
-        __syncthreads();
-        if (tid == 0) {
-            const double *Ao = a.shell_origin + 3 * sa, *Bo = a.shell_origin + 3 * sb, *Co = a.centre_origin + 3 * c;
-            double CAv[3], CBv[3];
-            for (int d = 0; d < 3; d++) {
-                CAv[d] = Co[d] - Ao[d];
-                CBv[d] = Co[d] - Bo[d];
-            }
-            const double CA2 = CAv[0] * CAv[0] + CAv[1] * CAv[1] + CAv[2] * CAv[2];
-            const double CB2 = CBv[0] * CBv[0] + CBv[1] * CBv[1] + CBv[2] * CBv[2];
-            sh.one_centre = CA2 < 1e-14 && CB2 < 1e-14;
-            sh.CA = sqrt(CA2);
-            sh.CB = sqrt(CB2);
-            sh.la = a.shell_L[sa];
-            sh.lb = a.shell_L[sb];
-            sh.d_n = sh.la + sh.lb + 1;
-            const int g = a.centre_grpp[c];
-            sh.npot = a.grpp_sl_n[g];
-            int e = 0, nt = 0, l1m = 0, l2m = 0;
-            for (int p = 0; p < sh.npot; p++) {
-                const int pot = a.sl_pot[a.grpp_sl_off[g] + p];
-                sh.pL[p] = a.pot_L[pot];
-                sh.pn[p] = a.pot_nprim[pot];
-                sh.poff[p] = nt;
-                for (int k = 0; k < sh.pn[p]; k++) {
-                    const int o = a.pot_prim_off[pot] + k;
-                    sh.tpow[nt] = a.pot_powers[o];
-                    sh.tcoef[nt] = a.pot_coef[o];
-                    sh.talpha[nt] = a.pot_alpha[o];
-                    nt++;
-                }
-                sh.pent[p] = e;
-                e += (sh.pL[p] + sh.la + 1) * (sh.pL[p] + sh.lb + 1) * sh.d_n;
-                l1m = max(l1m, sh.pL[p] + sh.la);
-                l2m = max(l2m, sh.pL[p] + sh.lb);
-            }
-            sh.pent[sh.npot] = e;
-            sh.n_entries = e;
-            sh.nterm_tot = nt;
-            sh.l1max_all = l1m;
-            sh.l2max_all = l2m;
-            sh.np_a = a.rp_n[sa];
-            sh.np_b = a.rp_n[sb];
-        }
-        __syncthreads();
-        const int np_a = sh.np_a, np_b = sh.np_b;
-        for (int i = tid; i < np_a; i += kRadThreads) {
-            sh.ca[i] = a.rp_coef[a.rp_off[sa] + i];
-            sh.xa[i] = a.rp_alpha[a.rp_off[sa] + i];
-            sh.ka[i] = 2.0 * sh.xa[i] * sh.CA;
-        }
-        for (int i = tid; i < np_b; i += kRadThreads) {
-            sh.cb[i] = a.rp_coef[a.rp_off[sb] + i];
-            sh.xb[i] = a.rp_alpha[a.rp_off[sb] + i];
-            sh.kb[i] = 2.0 * sh.xb[i] * sh.CB;
-        }
+        const int sa = a.task_a[t], sb = a.task_b[t];
         const int64_t qo = a.q_off[item];
-        double *Q = a.Q + qo, *Sp = a.S_prev + qo, *SC = a.scr + qo;
-        const int nE = sh.n_entries;
-        __syncthreads();
-
+        double *Q = a.Q + qo, *SC = a.scr + qo;
+        uint8_t *EF = a.eflag + qo;
+        const int nE = sh.n_entries, np_a = sh.np_a, np_b = sh.np_b;
+        const long long t0 = clock64();
+        unsigned long long c_combo = 0, c_iter = 0, c_final = 0;
+        int active = 0;
         if (sh.one_centre) {
-            // ---- analytic one-centre table: only l1 = l2 = 0 is non-zero
             for (int e = tid; e < nE; e += kRadThreads) {
                 int p, l1, l2, N;
                 decode_entry(sh, e, p, l1, l2, N);
-                double v = 0.0;
-                if (l1 == 0 && l2 == 0) {
-                    const int na = a.shell_nprim[sa], nb = a.shell_nprim[sb];
-                    const double *pca = a.prim_coef + a.shell_prim_off[sa], *pxa = a.prim_alpha + a.shell_prim_off[sa];
-                    const double *pcb = a.prim_coef + a.shell_prim_off[sb], *pxb = a.prim_alpha + a.shell_prim_off[sb];
-                    for (int i = 0; i < na; i++) {
-                        const double ci = pca[i] * gaussian_norm(sh.la, pxa[i]);
-                        for (int j = 0; j < nb; j++) {
-                            const double cj = pcb[j] * gaussian_norm(sh.lb, pxb[j]);
-                            for (int k = 0; k < sh.pn[p]; k++) {
-                                const int tk = sh.poff[p] + k;
-                                const double pp = pxa[i] + pxb[j] + sh.talpha[tk];
-                                const double f = ci * cj * sh.tcoef[tk];
-                                const int n = sh.tpow[tk] + N;
-                                double gi;
-                                if (n % 2 == 0) {
-                                    int kk = n / 2;
-                                    gi = dfact(2 * kk - 1) / (pow(2.0, kk + 1) * pow(pp, kk)) * sqrt(kPi / pp);
-                                } else {
-                                    int kk = (n - 1) / 2;
-                                    double fct = 1.0;
-                                    for (int q = 2; q <= kk; q++) fct *= q;
-                                    gi = fct / (2.0 * pow(pp, kk + 1));
-                                }
-                                v += f * gi;
+                Q[e] = one_centre_entry(a, sh, sa, sb, p, l1, l2, N);
+                EF[e] = 0;
+            }
+        } else {
+            const double CA2 = sh.CA * sh.CA, CB2 = sh.CB * sh.CB;
+            for (int e = tid; e < nE; e += kRadThreads) {
+                int p, l1, l2, N;
+                decode_entry(sh, e, p, l1, l2, N);
+                // screening.c:193-220: triples in (bra, ket, potential term) order, stop at the first failure
+                double sum = 0.0;
+                bool fail = false;
+                const int nk = sh.pn[p];
+                for (int i = 0; i < np_a && !fail; i++)
+                    for (int j = 0; j < np_b && !fail; j++)
+                        for (int k = 0; k < nk; k++) {
+                            const int tk = sh.poff[p] + k;
+                            double v;
+                            int it;
+                            const bool f = scr_prim(l1, l2, N + sh.tpow[tk], CA2, CB2, sh.xa[i], sh.xb[j], sh.ka[i],
+                                                    sh.kb[j], sh.talpha[tk], &v, &it);
+                            c_combo++;
+                            if (it < 0) {
+                                c_final++;
+                                it = -it - 1;
                             }
+                            c_iter += it;
+                            if (f) {
+                                fail = true;
+                                break;
+                            }
+                            sum += sh.ca[i] * sh.cb[j] * sh.tcoef[tk] * v;
                         }
-                    }
-                }
-                Q[e] = v;
-            }
-            if (tid == 0 && a.stop_level) a.stop_level[item] = 0;
-            continue;
-        }
-
-        // ---- phase 1: screening, one warp per entry
-        const double CA2 = sh.CA * sh.CA, CB2 = sh.CB * sh.CB;
-        for (int e = warp; e < nE; e += nwarps) {
-            int p, l1, l2, N;
-            decode_entry(sh, e, p, l1, l2, N);
-            const int nk = sh.pn[p], ncomb = np_a * np_b * nk;
-            double sum = 0.0;
-            bool fail = false;
-            for (int c0 = 0; c0 < ncomb && !fail; c0 += 32) {
-                const int cc = c0 + lane;
-                double contrib = 0.0;
-                bool f = false;
-                if (cc < ncomb) {
-                    const int k = cc % nk, ij = cc / nk, j = ij % np_b, i = ij / np_b;
-                    const int tk = sh.poff[p] + k;
-                    double v;
-                    f = scr_prim(l1, l2, N + sh.tpow[tk], CA2, CB2, sh.xa[i], sh.xb[j], sh.ka[i], sh.kb[j],
-                                 sh.talpha[tk], &v);
-                    contrib = sh.ca[i] * sh.cb[j] * sh.tcoef[tk] * v;
-                }
-                fail = __any_sync(0xffffffffu, f);
-                for (int o = 16; o > 0; o >>= 1) contrib += __shfl_down_sync(0xffffffffu, contrib, o);
-                sum += contrib;
-            }
-            if (lane == 0) {
-                const bool ok = !fail;
                 SC[e] = sum;
-                if (ok && fabs(sum) < 1e-16) {
+                if (!fail && fabs(sum) < 1e-16) {
                     Q[e] = sum;
-                    eflag[e] = kEntScrOk;  // screened: not active
+                    EF[e] = kEntScrOk;
                 } else {
                     Q[e] = 0.0;
-                    eflag[e] = kEntActive | (ok ? kEntScrOk : 0);
+                    EF[e] = kEntActive | (fail ? 0 : kEntScrOk);
+                    active = 1;
                 }
             }
         }
-        __syncthreads();
+        const int any = __syncthreads_or(active);
+        if (tid == 0) {
+            a.walk[item] = (uint8_t)any;
+            if (a.stop_level) a.stop_level[item] = 0;
+        }
+        if (a.counters) {
+            unsigned long long v[3] = {c_combo, c_iter, c_final};
+            for (int k = 0; k < 3; k++)
+                for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+            if (lane == 0) {
+                atomicAdd(a.counters + kRadCntScrCombos, v[0]);
+                atomicAdd(a.counters + kRadCntScrIters, v[1]);
+                atomicAdd(a.counters + kRadCntScrFinal, v[2]);
+            }
+            if (tid == 0) atomicAdd(a.counters + kRadCntScreenCycles, (unsigned long long)(clock64() - t0));
+        }
+    }
+}
 
-        // ---- phase 2: nested Log3 quadrature
+// dst[l * stride] += e * M_l(x) for l = 0..lmax, one table row (specfunc_scaled_mod_sph_bessel.c:72-122)
+__device__ __forceinline__ void bessel_row_acc(int lmax, double x, double e, double *dst, int stride)
+{
+    if (x <= 1e-7) {
+#pragma unroll 1
+        for (int l = 0; l <= lmax; l++) dst[l * stride] += e * bessel_small(l, x);
+    } else if (x <= 16.0) {
+        const int i0 = (int)(round(x * 100) + 1e-5);
+        const double dx = x - i0 * 0.01;
+        const double dx2 = dx * dx, dx3 = dx2 * dx, dx4 = dx3 * dx;
+        const double *d = c_tab.bessel + (size_t)i0 * kBesL * 5;
+#pragma unroll 1
+        for (int l = 0; l <= lmax; l++) {
+            const double *q = d + 5 * l;
+            const double m = __ldg(q) + __ldg(q + 1) * dx + __ldg(q + 2) * dx2 * 0.5 + __ldg(q + 3) * dx3 * (1.0 / 6.0) +
+                             __ldg(q + 4) * dx4 * (1.0 / 24.0);
+            dst[l * stride] += e * m;
+        }
+    } else {
+#pragma unroll 1
+        for (int l = 0; l <= lmax; l++) dst[l * stride] += e * bessel_asym(l, x);
+    }
+}
+
+constexpr int kRadRow = kRadThreads + 1;  // padded row stride of the chunk arrays (no bank conflicts)
+
+template <bool LEARNED>
+__global__ void __launch_bounds__(kRadThreads, 4) radial_walk_kernel(RadialArgs a)
+{
+    __shared__ RadialShared sh;
+    extern __shared__ double chunk[];  // [npot + l1max+1 + l2max+1 + dn][kRadRow]
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
+        if (!a.walk[item]) continue;
+        __syncthreads();
+        load_task(a, item, sh, tid, kRadThreads);
+        const int64_t qo = a.q_off[item];
+        double *Q = a.Q + qo, *Sp = a.S_prev + qo, *SC = a.scr + qo;
+        uint8_t *EF = a.eflag + qo;
+        const int nE = sh.n_entries, np_a = sh.np_a, np_b = sh.np_b;
         const int npot = sh.npot, l1m = sh.l1max_all, l2m = sh.l2max_all, dn = sh.d_n;
-        double *cr = chunk;                                   // unused slot kept for layout clarity
-        double *cwu = chunk + kRadThreads;                    // [npot][T]
-        double *cf1 = cwu + npot * kRadThreads;               // [l1m+1][T]
-        double *cf2 = cf1 + (l1m + 1) * kRadThreads;          // [l2m+1][T]
-        double *crn = cf2 + (l2m + 1) * kRadThreads;          // [dn][T]
-        int level_reached = 0;
-        int nr = 31;
+        double *cwu = chunk;                       // [npot][kRadRow]
+        double *cf1 = cwu + npot * kRadRow;        // [l1m+1][kRadRow]
+        double *cf2 = cf1 + (l1m + 1) * kRadRow;   // [l2m+1][kRadRow]
+        double *crn = cf2 + (l2m + 1) * kRadRow;   // [dn][kRadRow]
+        const long long t0 = clock64();
+        unsigned long long c_pts = 0, c_acc = 0;
+        int level_reached = 0, nr = 31;
         for (int level = 0; level <= kRadMaxLevel; level++) {
             if (level > 0) nr = 2 * nr + 1;
             const int npts = level == 0 ? nr : (nr + 1) / 2;  // new points of this level
             level_reached = level;
             if (level > 0) {
                 for (int e = tid; e < nE; e += kRadThreads)
-                    if (eflag[e] & kEntActive) {
+                    if (EF[e] & kEntActive) {
                         const double s = Q[e];
                         Sp[e] = s;
                         Q[e] = 0.5 * s;
@@ -329,7 +439,6 @@ __global__ void __launch_bounds__(kRadThreads) radial_kernel(RadialArgs a)
                     const int i = level == 0 ? (p0 + tid + 1) : 2 * (p0 + tid) + 1;
                     double r, w;
                     log3_point(i, nr, r, w);
-                    cr[tid] = r;
                     const double r2 = r * r;
                     for (int pp = 0; pp < npot; pp++) {
                         double u = 0.0;
@@ -337,57 +446,72 @@ __global__ void __launch_bounds__(kRadThreads) radial_kernel(RadialArgs a)
                             const int tk = sh.poff[pp] + k;
                             u += sh.tcoef[tk] * pow(r, sh.tpow[tk] - 2) * exp(-sh.talpha[tk] * r2);
                         }
-                        cwu[pp * kRadThreads + tid] = w * u;
+                        cwu[pp * kRadRow + tid] = w * u;
                     }
-                    for (int l = 0; l <= l1m; l++) cf1[l * kRadThreads + tid] = 0.0;
-                    for (int l = 0; l <= l2m; l++) cf2[l * kRadThreads + tid] = 0.0;
-                    double mv[kRadMaxLam + 1];
+                    for (int l = 0; l <= l1m; l++) cf1[l * kRadRow + tid] = 0.0;
+                    for (int l = 0; l <= l2m; l++) cf2[l * kRadRow + tid] = 0.0;
                     const double dA2 = (r - sh.CA) * (r - sh.CA), dB2 = (r - sh.CB) * (r - sh.CB);
-                    for (int q = 0; q < np_a; q++) {
-                        const double ex = sh.ca[q] * exp(-sh.xa[q] * dA2);
-                        bessel_scaled_row<kRadMaxLam>(l1m, sh.ka[q] * r, mv);
-                        for (int l = 0; l <= l1m; l++) cf1[l * kRadThreads + tid] += ex * mv[l];
-                    }
-                    for (int q = 0; q < np_b; q++) {
-                        const double ex = sh.cb[q] * exp(-sh.xb[q] * dB2);
-                        bessel_scaled_row<kRadMaxLam>(l2m, sh.kb[q] * r, mv);
-                        for (int l = 0; l <= l2m; l++) cf2[l * kRadThreads + tid] += ex * mv[l];
-                    }
-                    for (int n = 0; n < dn; n++) crn[n * kRadThreads + tid] = pow(r, n);
+#pragma unroll 1
+                    for (int q = 0; q < np_a; q++)
+                        bessel_row_acc(l1m, sh.ka[q] * r, sh.ca[q] * exp(-sh.xa[q] * dA2), cf1 + tid, kRadRow);
+#pragma unroll 1
+                    for (int q = 0; q < np_b; q++)
+                        bessel_row_acc(l2m, sh.kb[q] * r, sh.cb[q] * exp(-sh.xb[q] * dB2), cf2 + tid, kRadRow);
+                    for (int n = 0; n < dn; n++) crn[n * kRadRow + tid] = pow(r, n);
+                    c_pts++;
                 }
                 __syncthreads();
                 for (int e = tid; e < nE; e += kRadThreads) {
-                    if (!(eflag[e] & kEntActive)) continue;
+                    if (!(EF[e] & kEntActive)) continue;
                     int p, l1, l2, N;
                     decode_entry(sh, e, p, l1, l2, N);
-                    const double *pwu = cwu + p * kRadThreads, *p1 = cf1 + l1 * kRadThreads, *p2 = cf2 + l2 * kRadThreads,
-                                 *pn = crn + N * kRadThreads;
+                    const double *pwu = cwu + p * kRadRow, *p1 = cf1 + l1 * kRadRow, *p2 = cf2 + l2 * kRadRow,
+                                 *pn = crn + N * kRadRow;
                     double s = Q[e];
                     for (int q = 0; q < np; q++)
                         s = __dadd_rn(s, __dmul_rn(__dmul_rn(__dmul_rn(pwu[q], p1[q]), p2[q]), pn[q]));
                     Q[e] = s;
+                    c_acc += np;
                 }
             }
             // convergence bookkeeping (radial_type2_integral.c:285-315)
             int active = 0;
-            if (level > 0) {
-                for (int e = tid; e < nE; e += kRadThreads) {
-                    uint8_t f = eflag[e];
-                    if (!(f & kEntActive)) continue;
-                    const double s = Q[e];
-                    if ((f & kEntScrOk) && (fabs(s) / fabs(SC[e]) < 0.001)) {
-                        active = 1;
-                        continue;
-                    }
-                    if (fabs(s - Sp[e]) <= 1e-16) eflag[e] = f & ~kEntActive;
-                    else active = 1;
+            for (int e = tid; e < nE; e += kRadThreads) {
+                const uint8_t f = EF[e];
+                if (!(f & kEntActive)) continue;
+                if (level == 0) {
+                    active = 1;
+                    continue;
                 }
-            } else {
-                active = 1;
+                const double s = Q[e];
+                if ((f & kEntScrOk) && (fabs(s) / fabs(SC[e]) < 0.001)) {
+                    active = 1;
+                    continue;
+                }
+                if (fabs(s - Sp[e]) <= 1e-16) EF[e] = f & ~kEntActive;
+                else active = 1;
             }
             if (!__syncthreads_or(active)) break;
         }
         if (tid == 0 && a.stop_level) a.stop_level[item] = (int8_t)level_reached;
+        if (a.counters) {
+            unsigned long long v[2] = {c_pts, c_acc};
+            for (int k = 0; k < 2; k++)
+                for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+            if (lane == 0) {
+                atomicAdd(a.counters + kRadCntPoints, v[0]);
+                atomicAdd(a.counters + kRadCntBessel, v[0] * (unsigned long long)(np_a * (l1m + 1) + np_b * (l2m + 1)));
+                atomicAdd(a.counters + kRadCntPrimPts, v[0] * (unsigned long long)(np_a + np_b));
+                atomicAdd(a.counters + kRadCntTermPts, v[0] * (unsigned long long)sh.nterm_tot);
+                atomicAdd(a.counters + kRadCntPowPts, v[0] * (unsigned long long)dn);
+                atomicAdd(a.counters + kRadCntAccum, v[1]);
+            }
+            if (tid == 0) {
+                atomicAdd(a.counters + kRadCntQuadCycles, (unsigned long long)(clock64() - t0));
+                atomicAdd(a.counters + kRadCntItems, 1ull);
+                atomicAdd(a.counters + kRadCntLevels, (unsigned long long)(level_reached + 1));
+            }
+        }
     }
 }
 
