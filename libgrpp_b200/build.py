@@ -18,7 +18,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 
-SOURCES = ["engine.cu", "tables.cpp", "capi.cpp"]
+SOURCES = ["engine.cu", "tables.cpp", "capi.cpp", "noalloc.cu"]
 HEADERS = ["grpp_common.cuh", "specfunc.cuh", "mmd.cuh", "radial.cuh", "angular.cuh", "tables.h", "engine.h"]
 
 

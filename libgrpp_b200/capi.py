@@ -79,6 +79,7 @@ class LibGRPP:
         self._opt("libgrpp_b200_full_grpp_batch", ct.c_int, [_V, ct.c_int, _D, _D, _D, _D])
         self._opt("libgrpp_b200_set_device", ct.c_int, [ct.c_int])
         self._opt("libgrpp_b200_fp64_peak", ct.c_int, [_D])
+        self._opt("libgrpp_b200_type2_batch_noalloc", ct.c_int, [_V, _D])
         self._opt("libgrpp_b200_plan_create", _V, [_V, ct.c_int])
         self._opt("libgrpp_b200_plan_execute", ct.c_int, [_V])
         self._opt("libgrpp_b200_plan_outputs", ct.c_int, [_V, _D, _D, _D, _D])
@@ -190,6 +191,15 @@ class LibGRPP:
         if rc != 0:
             raise RuntimeError(f"libgrpp_b200_full_grpp_batch failed ({rc}): {self.last_error_message()}")
         return [x[:n] for x in outs]
+
+    def type2_batch_noalloc(self, batch):
+        """AREP type 2 blocks of every task through the allocation-free entry point."""
+        n = int(batch.block_offsets()[-1])
+        out = np.zeros(max(n, 1))
+        rc = self.lib.libgrpp_b200_type2_batch_noalloc(ct.byref(batch.struct), _dp(out))
+        if rc != 0:
+            raise RuntimeError(f"libgrpp_b200_type2_batch_noalloc failed ({rc}): {self.last_error_message()}")
+        return out[:n]
 
     def set_device(self, device: int):
         rc = self.lib.libgrpp_b200_set_device(int(device))
