@@ -116,8 +116,8 @@ typedef struct libgrpp_b200_plan libgrpp_b200_plan_t;
 libgrpp_b200_plan_t *libgrpp_b200_plan_create(const libgrpp_b200_batch_t *batch, int radial_mode);
 int libgrpp_b200_plan_execute(libgrpp_b200_plan_t *plan);
 int libgrpp_b200_plan_outputs(libgrpp_b200_plan_t *plan, double *arep, double *so_x, double *so_y, double *so_z);
-/* ms[4] = kernel time of the last execute(): total, type 1, radial, assembly (CUDA events on the
- * engine stream); counts[5] = tasks, radial tasks, type 1 work items, radial entries, bytes uploaded */
+/* ms[5] = kernel time of the last execute(): total, type 1, radial (screening + grid walk),
+ * assembly, screening alone (CUDA events on the engine stream); counts[5] = tasks, radial tasks, type 1 work items, radial entries, bytes uploaded */
 int libgrpp_b200_plan_stats(const libgrpp_b200_plan_t *plan, double *ms, int64_t *counts);
 /* operation counters of the radial kernel in the last execute() (n <= 16 slots): screening and
  * grid-walk SM cycles, tasks, integrand points, Bessel evaluations, primitive Gaussians, potential

@@ -270,10 +270,10 @@ class Plan:
         return [x[: self.n_out] for x in outs]
 
     def stats(self):
-        ms = np.zeros(4)
+        ms = np.zeros(5)
         cnt = np.zeros(5, dtype=np.int64)
         self.lib.lib.libgrpp_b200_plan_stats(self.h, _dp(ms), cnt.ctypes.data_as(ct.POINTER(ct.c_int64)))
-        return {"ms_total": ms[0], "ms_type1": ms[1], "ms_radial": ms[2], "ms_assembly": ms[3],
+        return {"ms_total": ms[0], "ms_type1": ms[1], "ms_radial": ms[2], "ms_assembly": ms[3], "ms_screen": ms[4],
                 "n_tasks": int(cnt[0]), "n_radial": int(cnt[1]), "n_type1_items": int(cnt[2]),
                 "n_entries": int(cnt[3]), "h2d_bytes": int(cnt[4])}
 

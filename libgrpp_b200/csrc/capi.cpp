@@ -685,6 +685,7 @@ int libgrpp_b200_plan_stats(const libgrpp_b200_plan_t *plan, double *ms, int64_t
         ms[1] = st->ms_mmd;
         ms[2] = st->ms_radial;
         ms[3] = st->ms_final;
+        ms[4] = st->ms_screen;
     }
     if (counts) {
         counts[0] = st->n_tasks;

@@ -126,7 +126,8 @@ int init_device_state(DeviceState &st, int device)
     GRPP_CUDA(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking));
     for (auto &e : st.ev) GRPP_CUDA(cudaEventCreate(&e));
     st.atab_off.assign((kMaxL + 2) * (kMaxL + 2), -1);
-    GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(radial_walk_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(radial_walk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -283,7 +284,7 @@ struct Plan {
     int *status = nullptr;
     unsigned long long *counters = nullptr;  // kRadCntNum slots inside the status area
     MmdArgs mmd;
-    int mmd_blocks = 0, mmd_threads = 128;
+    int mmd_blocks = 0, mmd_threads = 128, mmd_kpl = 32;
     size_t mmd_smem = 0;
     OcProjArgs ocp;
     int ocp_blocks = 0;
@@ -631,6 +632,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         const int wpb = 4;
         const size_t smem = (size_t)wpb * mmd_ws_size(mmd_lmax, mmd_smax) * sizeof(double);
         P.mmd = m;
+        P.mmd_kpl = ncart(mmd_lmax) * ncart(mmd_lmax) <= 256 ? 8 : 32;
         P.mmd_blocks = (int)std::min<int64_t>(((int64_t)items.size() + wpb - 1) / wpb, (int64_t)nsm * 16);
         P.mmd_threads = 32 * wpb;
         P.mmd_smem = smem;
@@ -773,7 +775,8 @@ int plan_execute(Plan &P)
     GRPP_CUDA(cudaMemsetAsync(P.status, 0, 16 * sizeof(int) + kRadCntNum * sizeof(unsigned long long), s));
     GRPP_CUDA(cudaEventRecord(st.ev[0], s));
     if (P.mmd_blocks > 0) {
-        mmd_kernel<<<P.mmd_blocks, P.mmd_threads, P.mmd_smem, s>>>(P.mmd);
+        if (P.mmd_kpl == 8) mmd_kernel<8><<<P.mmd_blocks, P.mmd_threads, P.mmd_smem, s>>>(P.mmd);
+        else mmd_kernel<32><<<P.mmd_blocks, P.mmd_threads, P.mmd_smem, s>>>(P.mmd);
         GRPP_CUDA(cudaGetLastError());
     }
     GRPP_CUDA(cudaEventRecord(st.ev[1], s));
@@ -784,6 +787,7 @@ int plan_execute(Plan &P)
     if (P.rad_blocks > 0) {
         radial_screen_kernel<<<P.scr_blocks, kRadThreads, 0, s>>>(P.rad);
         GRPP_CUDA(cudaGetLastError());
+        GRPP_CUDA(cudaEventRecord(st.ev[4], s));
         if (P.opt.radial_mode == LIBGRPP_B200_RADIAL_LEARNED)
             radial_walk_kernel<true><<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(P.rad);
         else
@@ -801,6 +805,7 @@ int plan_execute(Plan &P)
     GRPP_CUDA(cudaStreamSynchronize(s));
     cudaEventElapsedTime(&P.stats.ms_mmd, st.ev[0], st.ev[1]);
     cudaEventElapsedTime(&P.stats.ms_radial, st.ev[1], st.ev[2]);
+    if (P.rad_blocks > 0) cudaEventElapsedTime(&P.stats.ms_screen, st.ev[1], st.ev[4]);
     cudaEventElapsedTime(&P.stats.ms_final, st.ev[2], st.ev[3]);
     cudaEventElapsedTime(&P.stats.ms_total, st.ev[0], st.ev[3]);
     P.stats.n_tasks = P.n_tasks;

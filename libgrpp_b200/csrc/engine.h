@@ -16,7 +16,7 @@ struct RunOptions {
 struct RunStats {
     int64_t n_tasks = 0, n_radial = 0, n_mmd = 0, n_entries = 0;
     int64_t fallbacks = 0;
-    float ms_total = 0.f, ms_mmd = 0.f, ms_radial = 0.f, ms_final = 0.f;
+    float ms_total = 0.f, ms_mmd = 0.f, ms_radial = 0.f, ms_final = 0.f, ms_screen = 0.f;
     unsigned long long radial_counters[16] = {0};  // RadialCounter slots (radial.cuh)
 };
 

@@ -58,7 +58,7 @@ __host__ __device__ inline int mmd_r_size(int smax)
 }
 __host__ __device__ inline int mmd_ws_size(int lmax, int smax) { return mmd_e_size(lmax) + mmd_r_size(smax) + 2 * (smax + 2) + 16; }
 
-constexpr int kMmdMaxPairsPerLane = 32;  // up to 1024 Cartesian pairs per pass
+constexpr int kMmdMaxPairsPerLane = 32;  // up to 1024 Cartesian pairs per pass (KPL = 32 variant)
 
 __device__ __forceinline__ int eidx(int lb1, int S1, int ax, int i, int j, int t, int la1)
 {
@@ -76,6 +76,8 @@ __device__ __forceinline__ int r_level_off(int S, int s)
 // index of (u+v = k, v) within level s: tri(k) + v
 __device__ __forceinline__ int r_in_level(int u, int v) { return (u + v) * (u + v + 1) / 2 + v; }
 
+// KPL: Cartesian pairs held per lane per pass (8: up to 256 pairs, 32: up to 1024)
+template <int KPL>
 __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
 {
     extern __shared__ double smem[];
@@ -116,17 +118,17 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
         __syncwarp();
 
         const int npairs = nA * nB;
-        for (int pass = 0; pass < npairs; pass += 32 * kMmdMaxPairsPerLane) {
-            double res[kMmdMaxPairsPerLane];
+        for (int pass = 0; pass < npairs; pass += 32 * KPL) {
+            double res[KPL];
 #pragma unroll
-            for (int q = 0; q < kMmdMaxPairsPerLane; q++) res[q] = 0.0;
+            for (int q = 0; q < KPL; q++) res[q] = 0.0;
 
             for (int k = 0; k < nterms; k++) {
                 const double zeta = overlap ? 0.0 : a.pot_alpha[a.pot_prim_off[item.pot] + k];
                 const int npow = overlap ? 3 : a.pot_powers[a.pot_prim_off[item.pot] + k];
-                double accp[kMmdMaxPairsPerLane];
+                double accp[KPL];
 #pragma unroll
-                for (int q = 0; q < kMmdMaxPairsPerLane; q++) accp[q] = 0.0;
+                for (int q = 0; q < KPL; q++) accp[q] = 0.0;
 
                 for (int i = 0; i < npA; i++) {
                     const double ci = cA[i];
@@ -229,7 +231,7 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                             }
                             // ---- Cartesian pairs of this lane
 #pragma unroll
-                            for (int qq = 0; qq < kMmdMaxPairsPerLane; qq++) {
+                            for (int qq = 0; qq < KPL; qq++) {
                                 const int pr = pass + lane + 32 * qq;
                                 if (pr >= npairs) break;
                                 const int m = pr / nB, n = pr % nB;
@@ -282,7 +284,7 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                             }
                             __syncwarp();
 #pragma unroll
-                            for (int qq = 0; qq < kMmdMaxPairsPerLane; qq++) {
+                            for (int qq = 0; qq < KPL; qq++) {
                                 const int pr = pass + lane + 32 * qq;
                                 if (pr >= npairs) break;
                                 const int m = pr / nB, n = pr % nB;
@@ -297,10 +299,10 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                 }
                 const double ck = overlap ? 1.0 : a.pot_coef[a.pot_prim_off[item.pot] + k];
 #pragma unroll
-                for (int qq = 0; qq < kMmdMaxPairsPerLane; qq++) res[qq] += ck * accp[qq];
+                for (int qq = 0; qq < KPL; qq++) res[qq] += ck * accp[qq];
             }
 #pragma unroll
-            for (int qq = 0; qq < kMmdMaxPairsPerLane; qq++) {
+            for (int qq = 0; qq < KPL; qq++) {
                 const int pr = pass + lane + 32 * qq;
                 if (pr < npairs) out[pr] = res[qq];
             }
