@@ -687,6 +687,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         r.pot_coef = at<double>(ib, o_pcoef);
         r.pot_alpha = at<double>(ib, o_palpha);
         r.q_off = at<int64_t>(ib, o_rq);
+        r.n_entries = qtot;
         r.Q = Qd;
         r.S_prev = Spd;
         r.scr = SCd;
@@ -700,7 +701,9 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         const size_t smem = (size_t)(rad_npot + (rad_l1 + 1) + (rad_l2 + 1) + rad_dn) * kRadRow * sizeof(double);
         P.rad = r;
         P.rad_blocks = (int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 16);
-        P.scr_blocks = (int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 32);
+        int scr_occ = 0;
+        GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&scr_occ, radial_screen_flat_kernel, kRadThreads, 0));
+        P.scr_blocks = (int)std::min<int64_t>((qtot + kRadThreads - 1) / kRadThreads, (int64_t)nsm * std::max(scr_occ, 1));
         P.rad_smem = smem;
     }
 
@@ -785,7 +788,8 @@ int plan_execute(Plan &P)
         GRPP_CUDA(cudaGetLastError());
     }
     if (P.rad_blocks > 0) {
-        radial_screen_kernel<<<P.scr_blocks, kRadThreads, 0, s>>>(P.rad);
+        GRPP_CUDA(cudaMemsetAsync(P.rad.walk, 0, (size_t)P.n_radial, s));
+        radial_screen_flat_kernel<<<P.scr_blocks, kRadThreads, 0, s>>>(P.rad);
         GRPP_CUDA(cudaGetLastError());
         GRPP_CUDA(cudaEventRecord(st.ev[4], s));
         if (P.opt.radial_mode == LIBGRPP_B200_RADIAL_LEARNED)

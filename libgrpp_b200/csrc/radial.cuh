@@ -13,12 +13,12 @@
 //     |S_L - S_{L-1}| <= 1e-16 unless |S|/|estimate| < 1e-3, capped at 8191 points.
 //
 // GPU mapping, two kernels:
-//  * radial_screen_kernel: one CTA per task, one thread per entry. A thread
-//    walks the primitive triples (i, j, k) of its entry in libgrpp's order and
-//    stops at the first failing one, exactly as libgrpp does, so the estimate
-//    and the gate decision are those of the reference, and no work is spent on
-//    triples libgrpp never evaluates. One-centre tasks get their analytic
-//    table here and need no grid walk.
+//  * radial_screen_flat_kernel: one thread per (task, entry) over the entries of the
+//    whole batch. A thread walks the primitive triples (i, j, k) of its entry in
+//    libgrpp's order and stops at the first failing one, exactly as libgrpp does,
+//    so the estimate and the gate decision are those of the reference, and no
+//    work is spent on triples libgrpp never evaluates. One-centre tasks get their
+//    analytic table here and need no grid walk.
 //  * radial_walk_kernel: one CTA per task that has entries left. The grid is
 //    walked level by level in chunks of one point per thread; a point's
 //    integrand values
@@ -34,6 +34,9 @@
 namespace grpp {
 
 constexpr int kRadThreads = 128;
+#ifndef GRPP_SCR_MINB
+#define GRPP_SCR_MINB 6  // resident 128-thread blocks per SM asked of the flat screening kernel
+#endif
 constexpr int kRadMaxPrims = 64;     // primitives per shell on the radial path
 constexpr int kRadMaxPots = 24;      // semilocal potentials per centre
 constexpr int kRadMaxTerms = 256;    // potential terms per centre (all semilocal potentials)
@@ -47,6 +50,7 @@ constexpr uint8_t kEntActive = 1, kEntScrOk = 2;
 
 struct RadialArgs {
     int n_items;
+    int64_t n_entries;          // total entries of all items (flat screening)
     const int *item_task;
     const int *task_a, *task_b, *task_c;
     const int *shell_L;
@@ -169,6 +173,212 @@ __device__ inline bool scr_prim(int l1, int l2, int n, double CA2, double CB2, d
            exp(-eta * r0 * r0 - aA * (r0 - CA) * (r0 - CA) - aB * (r0 - CB) * (r0 - CB)) * 0.5 * (1 + erf(sqrt(p) * r0));
     *iters = -*iters - 1;  // negative: the envelope was evaluated
     return false;
+}
+
+// x^n for a small non-negative integer n by binary powering (libgrpp calls pow(r0, n);
+// the estimate only feeds threshold tests, and the two agree to a few ulps)
+__device__ __forceinline__ double ipow(double x, int n)
+{
+    double r = 1.0, b = x;
+    while (n) {
+        if (n & 1) r *= b;
+        b *= b;
+        n >>= 1;
+    }
+    return r;
+}
+
+// M_a(x) / M_b(x) with (a, b) = (1, 0) if l = 0, else (l-1, l) (screening.c:329-346)
+__device__ __forceinline__ double scr_ratio_inl(int l, double x)
+{
+    const int na = l == 0 ? 1 : l - 1, nb = l == 0 ? 0 : l;
+    if (x <= 1e-7) return bessel_small(na, x) / bessel_small(nb, x);
+    if (x <= 16.0) {
+        const int i0 = (int)(round(x * 100) + 1e-5);
+        const double dx = x - i0 * 0.01;
+        const double *row = c_tab.bessel + (size_t)i0 * kBesL * 5;
+        return taylor4(row + 5 * na, dx) / taylor4(row + 5 * nb, dx);
+    }
+    return bessel_asym(na, x) / bessel_asym(nb, x);
+}
+
+// Primitive screening estimate (screening.c:243-318) with CA, CB as distances.
+// Returns true on failure (no fixed point in 4 steps). *iters: steps taken, negative
+// (-(steps)-1) when the envelope was evaluated.
+__device__ __forceinline__ bool scr_prim_flat(int l1, int l2, int n, double CA, double CB, double aA, double aB,
+                                              double k1, double k2, double eta, double *val, int *iters)
+{
+    *val = 0.0;
+    *iters = 0;
+    if (l1 >= 1 && fabs(k1) <= kZeroThresh) return false;
+    if (l2 >= 1 && fabs(k2) <= kZeroThresh) return false;
+    const double p = aA + aB + eta;
+    if (l1 == 0 && l2 == 0 && fabs(k1) <= kZeroThresh && fabs(k2) <= kZeroThresh) {
+        double gi;
+        if (n % 2 == 0) {
+            const int k = n / 2;
+            gi = dfact(2 * k - 1) / (pow(2.0, k + 1) * pow(p, k)) * sqrt(kPi / p);
+        } else {
+            const int k = (n - 1) / 2;
+            double f = 1.0;
+            for (int q = 2; q <= k; q++) f *= q;
+            gi = f / (2.0 * pow(p, k + 1));
+        }
+        *val = exp(-aA * CA * CA - aB * CB * CB) * gi;
+        return false;
+    }
+    const double inv2p = 1.0 / (2.0 * p);
+    double r0 = (aA * CA + aB * CB) / p, r0p;
+    int steps = 0;
+    do {
+        steps++;
+        if (steps == 5) {
+            *iters = steps - 1;
+            return true;
+        }
+        r0p = r0;
+        const double x1 = k1 * r0, x2 = k2 * r0;
+        double s = scr_ratio_inl(l1, x1) * x1 + scr_ratio_inl(l2, x2) * x2 + n;
+        if (l1 > 0) s = s - l1 - 1;
+        if (l2 > 0) s = s - l2 - 1;
+        r0 = sqrt(s * inv2p);
+    } while (fabs(r0 - r0p) > 1e-2);
+    const double d1 = r0 - CA, d2 = r0 - CB;
+    *val = sqrt(kPi / p) * ipow(r0, n) * bessel_scaled(l1, k1 * r0) * bessel_scaled(l2, k2 * r0) *
+           exp(-eta * r0 * r0 - aA * d1 * d1 - aB * d2 * d2) * 0.5 * (1 + erf(sqrt(p) * r0));
+    *iters = -steps - 1;
+    return false;
+}
+
+// Screening of every (task, entry) of a batch, one thread per entry over the flattened
+// entry space (entries of one task are consecutive, tasks in item order): no per-task
+// barrier and no ragged last round. A thread follows screening.c:193-220 for its entry:
+// primitive triples (i, j, k) in libgrpp's order, stopping at the first failure. The
+// outcome per entry is written to Q (value if screened out), scr (estimate) and eflag;
+// walk[item] is set to 1 when any entry of the item needs the grid (walk[] is zeroed
+// by the host before the launch). One-centre tasks get their analytic table.
+__global__ void __launch_bounds__(kRadThreads, GRPP_SCR_MINB) radial_screen_flat_kernel(RadialArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const long long t0 = clock64();
+    unsigned long long c_combo = 0, c_iter = 0, c_final = 0;
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.n_entries; g += stride) {
+        int lo = 0, hi = a.n_items - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(a.q_off + mid) <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        const int item = lo;
+        int e = (int)(g - __ldg(a.q_off + item));
+        const int t = __ldg(a.item_task + item);
+        const int sa = __ldg(a.task_a + t), sb = __ldg(a.task_b + t), c = __ldg(a.task_c + t);
+        const double *Ao = a.shell_origin + 3 * sa, *Bo = a.shell_origin + 3 * sb, *Co = a.centre_origin + 3 * c;
+        double CA2 = 0.0, CB2 = 0.0;
+        for (int d = 0; d < 3; d++) {
+            const double u = __ldg(Co + d) - __ldg(Ao + d), v = __ldg(Co + d) - __ldg(Bo + d);
+            CA2 += u * u;
+            CB2 += v * v;
+        }
+        const int la = __ldg(a.shell_L + sa), lb = __ldg(a.shell_L + sb), dn = la + lb + 1;
+        const int gr = __ldg(a.centre_grpp + c), npot = __ldg(a.grpp_sl_n + gr), slo = __ldg(a.grpp_sl_off + gr);
+        int pot = -1, Lp = 0;
+        for (int p = 0; p < npot; p++) {
+            pot = __ldg(a.sl_pot + slo + p);
+            Lp = __ldg(a.pot_L + pot);
+            const int cnt = (Lp + la + 1) * (Lp + lb + 1) * dn;
+            if (e < cnt) break;
+            e -= cnt;
+        }
+        const int d2 = Lp + lb + 1;
+        const int l1 = e / (d2 * dn), rem = e - l1 * d2 * dn, l2 = rem / dn, N = rem - l2 * dn;
+        const int nk = __ldg(a.pot_nprim + pot), po = __ldg(a.pot_prim_off + pot);
+        if (CA2 < 1e-14 && CB2 < 1e-14) {
+            // analytic one-centre entry (radial_type2_integral.c:126-155): only l1 = l2 = 0 is non-zero
+            double v = 0.0;
+            if (l1 == 0 && l2 == 0) {
+                const int na = __ldg(a.shell_nprim + sa), nb = __ldg(a.shell_nprim + sb);
+                const double *pca = a.prim_coef + __ldg(a.shell_prim_off + sa), *pxa = a.prim_alpha + __ldg(a.shell_prim_off + sa);
+                const double *pcb = a.prim_coef + __ldg(a.shell_prim_off + sb), *pxb = a.prim_alpha + __ldg(a.shell_prim_off + sb);
+                for (int i = 0; i < na; i++) {
+                    const double ci = __ldg(pca + i) * gaussian_norm(la, __ldg(pxa + i));
+                    for (int j = 0; j < nb; j++) {
+                        const double cj = __ldg(pcb + j) * gaussian_norm(lb, __ldg(pxb + j));
+                        for (int k = 0; k < nk; k++) {
+                            const double pp = __ldg(pxa + i) + __ldg(pxb + j) + __ldg(a.pot_alpha + po + k);
+                            const double f = ci * cj * __ldg(a.pot_coef + po + k);
+                            const int n = __ldg(a.pot_powers + po + k) + N;
+                            double gi;
+                            if (n % 2 == 0) {
+                                const int kk = n / 2;
+                                gi = dfact(2 * kk - 1) / (pow(2.0, kk + 1) * pow(pp, kk)) * sqrt(kPi / pp);
+                            } else {
+                                const int kk = (n - 1) / 2;
+                                double fct = 1.0;
+                                for (int q = 2; q <= kk; q++) fct *= q;
+                                gi = fct / (2.0 * pow(pp, kk + 1));
+                            }
+                            v += f * gi;
+                        }
+                    }
+                }
+            }
+            a.Q[g] = v;
+            a.eflag[g] = 0;
+            continue;
+        }
+        const double CA = sqrt(CA2), CB = sqrt(CB2);
+        const int na = __ldg(a.rp_n + sa), nb = __ldg(a.rp_n + sb);
+        const double *ca = a.rp_coef + __ldg(a.rp_off + sa), *xa = a.rp_alpha + __ldg(a.rp_off + sa);
+        const double *cb = a.rp_coef + __ldg(a.rp_off + sb), *xb = a.rp_alpha + __ldg(a.rp_off + sb);
+        // screening.c:193-220: triples in (bra, ket, potential term) order, stop at the first failure
+        double sum = 0.0;
+        bool fail = false;
+        for (int i = 0; i < na && !fail; i++) {
+            const double aA = __ldg(xa + i), ci = __ldg(ca + i), k1 = 2 * aA * CA;
+            for (int j = 0; j < nb && !fail; j++) {
+                const double aB = __ldg(xb + j), cij = ci * __ldg(cb + j), k2 = 2 * aB * CB;
+                for (int k = 0; k < nk; k++) {
+                    double v;
+                    int it;
+                    const bool f = scr_prim_flat(l1, l2, N + __ldg(a.pot_powers + po + k), CA, CB, aA, aB, k1, k2,
+                                                 __ldg(a.pot_alpha + po + k), &v, &it);
+                    c_combo++;
+                    if (it < 0) {
+                        c_final++;
+                        it = -it - 1;
+                    }
+                    c_iter += it;
+                    if (f) {
+                        fail = true;
+                        break;
+                    }
+                    sum += cij * __ldg(a.pot_coef + po + k) * v;
+                }
+            }
+        }
+        a.scr[g] = sum;
+        if (!fail && fabs(sum) < 1e-16) {
+            a.Q[g] = sum;
+            a.eflag[g] = kEntScrOk;
+        } else {
+            a.Q[g] = 0.0;
+            a.eflag[g] = kEntActive | (fail ? 0 : kEntScrOk);
+            a.walk[item] = 1;
+        }
+    }
+    if (a.counters) {
+        unsigned long long v[3] = {c_combo, c_iter, c_final};
+        for (int k = 0; k < 3; k++)
+            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+        if (lane == 0) {
+            atomicAdd(a.counters + kRadCntScrCombos, v[0]);
+            atomicAdd(a.counters + kRadCntScrIters, v[1]);
+            atomicAdd(a.counters + kRadCntScrFinal, v[2]);
+            atomicAdd(a.counters + kRadCntScreenCycles, (unsigned long long)(clock64() - t0));
+        }
+    }
 }
 
 // decode entry index within an item -> (potential, l1, l2, N)
