@@ -12,8 +12,11 @@ path; NCCL/gloo only for the start barrier and the max-over-ranks time).
 
 Reported: value = tasks / device time of the engine's kernels with inputs
 resident in HBM (CUDA events on the engine's stream, L2 flushed between
-steps); e2e = the same tasks through the public batched C-ABI call with host
-inputs and outputs (packing, host->device and device->host copies included).
+steps) for the learned batched form (the walk scheduled by the level model);
+"plain" = the same steps with the plain level-by-level schedule, and
+learned_over_plain their ratio (results are bit-identical); e2e = the same
+tasks through the public batched C-ABI call with host inputs and outputs
+(packing, host->device and device->host copies included).
 --impl reference times libgrpp itself (oracle/_ref, compiled from its
 sources) on this host's cores over a bounded sample of each step's tasks.
 """
@@ -169,6 +172,31 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def time_plans(plans, flush, local):
+    """Execute each plan once (L2 flushed before each); per-kernel ms summed, counters summed."""
+    import torch
+    ms, kms = [], {"ms_type1": 0.0, "ms_screen": 0.0, "ms_walk": 0.0, "ms_predict": 0.0, "ms_assembly": 0.0}
+    cnt, fallbacks = None, 0
+    with ClockSampler(local) as clk:
+        for p in plans:
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            p.execute()
+            st = p.stats()
+            ls = p.learned_stats()
+            ms.append(st["ms_total"])
+            kms["ms_type1"] += st["ms_type1"]
+            kms["ms_screen"] += st["ms_screen"]
+            kms["ms_predict"] += ls["ms_predict"]
+            kms["ms_walk"] += st["ms_radial"] - st["ms_screen"] - ls["ms_predict"]
+            kms["ms_assembly"] += st["ms_assembly"]
+            fallbacks += ls["fallbacks"]
+            c = p.counters()
+            cnt = c if cnt is None else {k: cnt[k] + c[k] for k in c}
+    torch.cuda.synchronize()
+    return float(sum(ms)), kms, cnt, fallbacks, clk.summary()
+
+
 def run_ours(args, rank, world, local):
     import torch
     from libgrpp_b200 import engine
@@ -181,7 +209,7 @@ def run_ours(args, rank, world, local):
     torch.cuda.set_device(local)
     lib = engine.load()
     lib.set_device(local)
-    mode = 1 if args.mode == "learned" else 0
+    modes = {"plain": 0, "learned": 1}
 
     idxs = [(rank + world * s) % 100 for s in range(args.steps)]
     S = system()
@@ -192,48 +220,45 @@ def run_ours(args, rank, world, local):
             sel = np.linspace(0, len(a) - 1, args.tasks_per_step).astype(np.int64)
             a, b, c = a[sel], b[sel], c[sel]
         batches.append(S.batch(a, b, c))
-    plans = [lib.plan(b, mode) for b in batches]
     n_tasks = [len(b.task_a) for b in batches]
-
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    for w in range(args.warmup):
-        plans[w % len(plans)].execute()
-
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ms, kms = [], {"ms_type1": 0.0, "ms_radial": 0.0, "ms_assembly": 0.0, "ms_screen": 0.0}
-    cnt = None
-    with ClockSampler(local) as clk:
+    res = {}
+    for name in ("plain", args.mode) if args.mode == "learned" else ("plain",):
+        plans = [lib.plan(b, modes[name]) for b in batches]
+        for w in range(args.warmup):
+            plans[w % len(plans)].execute()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        total_ms, kms, cnt, fallbacks, clocks = time_plans(plans, flush, local)
+        tasks = float(sum(n_tasks))
+        if dist is not None:
+            t = torch.tensor([total_ms, tasks], dtype=torch.float64, device="cuda")
+            tmax = t.clone()
+            dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+            dist.all_reduce(t, op=dist.ReduceOp.SUM)
+            total_ms, tasks = float(tmax[0]), float(t[1])
+        st0 = plans[0].stats()
+        res[name] = {"value": tasks / (total_ms / 1e3), "ms_per_step": total_ms / len(plans),
+                     "kernel_ms_per_step": {k: v / len(plans) for k, v in kms.items()},
+                     "counters": {k: v / len(plans) for k, v in cnt.items()} if cnt else None,
+                     "fallbacks_per_step": fallbacks / len(plans), "clocks": clocks,
+                     "launches_per_step": (1 if st0["n_type1_items"] else 0) + 1
+                                          + (2 if st0["n_radial"] else 0) + (2 if name == "learned" else 0),
+                     "h2d": st0["h2d_bytes"]}
         for p in plans:
-            flush.fill_(1.0)
-            torch.cuda.synchronize()
-            p.execute()
-            st = p.stats()
-            ms.append(st["ms_total"])
-            for k in kms:
-                kms[k] += st[k]
-            c = p.counters()
-            cnt = c if cnt is None else {k: cnt[k] + c[k] for k in c}
-    torch.cuda.synchronize()
-    total_ms = float(sum(ms))
-    tasks = float(sum(n_tasks))
-    if dist is not None:
-        t = torch.tensor([total_ms, tasks], dtype=torch.float64, device="cuda")
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        total_ms, tasks = float(tmax[0]), float(t[1])
-    value = tasks / (total_ms / 1e3)
+            p.close()
+    main_mode = args.mode
+    R = res[main_mode]
 
     # end to end through the public batched call (host in, host out)
     e2e_batches = batches[: max(1, min(len(batches), args.e2e_steps))]
-    lib.full_grpp_batch(e2e_batches[0], mode)
+    lib.full_grpp_batch(e2e_batches[0], modes[main_mode])
     if dist is not None:
         dist.barrier()
     t0 = time.perf_counter()
     for b in e2e_batches:
-        lib.full_grpp_batch(b, mode)
+        lib.full_grpp_batch(b, modes[main_mode])
     e2e_s = time.perf_counter() - t0
     e2e_tasks = float(sum(len(b.task_a) for b in e2e_batches))
     if dist is not None:
@@ -242,24 +267,26 @@ def run_ours(args, rank, world, local):
         dist.all_reduce(tm, op=dist.ReduceOp.MAX)
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         e2e_s, e2e_tasks = float(tm[0]), float(t[1])
-    st0 = plans[0].stats()
-    h2d = st0["h2d_bytes"]
     d2h = 4 * 8 * int(batches[0].block_offsets()[-1])
 
-    kernel_ms = {k: v / len(plans) for k, v in kms.items()}
-    dominant = max(("ms_type1", "ms_radial", "ms_assembly"), key=kernel_ms.get)
     line = {
-        "metric": METRIC, "value": value, "unit": "tasks/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / len(plans), "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": R["value"], "unit": "tasks/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": R["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config 1)",
-        "config": {"workload": WORKLOAD, "tasks_per_step": n_tasks[0], "radial_mode": args.mode,
+        "config": {"workload": WORKLOAD, "tasks_per_step": n_tasks[0], "radial_mode": main_mode,
                    "l2": "flushed between steps (512 MiB write)", "parallelism": f"task blocks over {world} GPU(s)"},
-        "kernel_ms_per_step": kernel_ms,
-        "gpu_launches": args.steps * (3 if st0["n_radial"] else 2),
-        "e2e": {"value": e2e_tasks / e2e_s, "unit": "tasks/s", "h2d_bytes_per_step": h2d,
+        "kernel_ms_per_step": R["kernel_ms_per_step"],
+        "gpu_launches": args.steps * R["launches_per_step"],
+        "e2e": {"value": e2e_tasks / e2e_s, "unit": "tasks/s", "h2d_bytes_per_step": R["h2d"],
                 "d2h_bytes_per_step": d2h},
-        "clocks": clk.summary(),
+        "clocks": R["clocks"],
     }
+    if main_mode == "learned":
+        P = res["plain"]
+        line["plain"] = {"value": P["value"], "ms_per_step": P["ms_per_step"],
+                         "kernel_ms_per_step": P["kernel_ms_per_step"], "clocks": P["clocks"]}
+        line["learned_over_plain"] = R["value"] / P["value"]
+        line["learned_fallbacks_per_step"] = R["fallbacks_per_step"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
         rate, dt = cpu_reference_rate(lambda: step_tasks(idxs[0]), args.ref_sample, threads)
@@ -267,10 +294,7 @@ def run_ours(args, rank, world, local):
                                 "sample": f"{args.ref_sample} seeded random tasks of the first step's block "
                                           f"({dt:.1f} s on {threads} threads)"}
     peak = lib.fp64_peak()
-    per_step = {k: v / len(plans) for k, v in cnt.items()} if cnt else None
-    line["roofline"] = roofline(args, dominant, kernel_ms, per_step, peak)
-    for p in plans:
-        p.close()
+    line["roofline"] = roofline(R["kernel_ms_per_step"], R["counters"], peak)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -293,22 +317,33 @@ RADIAL_FLOPS = {
 }
 
 
-def radial_flops(counters):
-    return float(sum(RADIAL_FLOPS[k] * counters[k] for k in RADIAL_FLOPS))
+SCREEN_KEYS = ("scr_combos", "scr_iters", "scr_final")
 
 
-def roofline(args, dominant, kernel_ms, counters, peak_tflops):
-    """FP64 roofline of the dominant kernel. bound is "fp64": the radial quadrature is
-    compute bound on the FP64 pipe (no dense contraction, a few kB of input per task)."""
+def kernel_flops(kernel, counters):
+    keys = SCREEN_KEYS if kernel == "ms_screen" else [k for k in RADIAL_FLOPS if k not in SCREEN_KEYS]
+    return float(sum(RADIAL_FLOPS[k] * counters[k] for k in keys))
+
+
+def roofline(kernel_ms, counters, peak_tflops):
+    """FP64 roofline of the dominant kernel (and of the other radial kernel beside it).
+    bound is "fp64": the GRPP path has no dense contraction and a task reads a few kB,
+    so the FP64 pipe, not HBM or the tensor cores, bounds it."""
+    dominant = max(("ms_type1", "ms_screen", "ms_walk", "ms_assembly"), key=kernel_ms.get)
     out = {"bound": "fp64", "kernel": dominant, "unit": "TFLOP/s", "peak": peak_tflops,
-           "peak_source": "measured in this run (FP64 FMA microkernel, all SMs)", "traffic": None}
-    if dominant == "ms_radial" and counters is not None:
-        fl = radial_flops(counters)
-        ach = fl / (kernel_ms["ms_radial"] * 1e-3) / 1e12
-        out.update({"achieved": ach, "frac": ach / peak_tflops if peak_tflops else None,
-                    "flops_per_launch": fl, "counters": counters})
-    else:
-        out.update({"achieved": None, "frac": None})
+           "peak_source": "measured in this run (FP64 FMA microkernel, all SMs)", "traffic": None,
+           "achieved": None, "frac": None}
+    if counters is None:
+        return out
+    per = {}
+    for k in ("ms_screen", "ms_walk"):
+        fl = kernel_flops(k, counters)
+        ach = fl / (kernel_ms[k] * 1e-3) / 1e12 if kernel_ms[k] > 0 else None
+        per[k] = {"flops_per_launch": fl, "achieved": ach, "frac": ach / peak_tflops if ach and peak_tflops else None}
+    if dominant in per:
+        out.update(per[dominant])
+    out["radial_kernels"] = per
+    out["counters"] = counters
     return out
 
 
@@ -318,7 +353,8 @@ def main():
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["plain", "learned"], default="plain")
+    ap.add_argument("--mode", choices=["plain", "learned"], default="learned",
+                    help="headline radial mode; learned also times plain on the same steps")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-sample", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -86,7 +86,7 @@ enum {
 /* radial quadrature modes */
 enum {
     LIBGRPP_B200_RADIAL_PLAIN = 0,   /* level-by-level nested Log3 doubling */
-    LIBGRPP_B200_RADIAL_LEARNED = 1  /* MLP-predicted level + one check level, plain fallback */
+    LIBGRPP_B200_RADIAL_LEARNED = 1  /* walk scheduled by the learned level model (same results) */
 };
 
 /* last error of the calling thread: code and message */
@@ -124,6 +124,54 @@ int libgrpp_b200_plan_stats(const libgrpp_b200_plan_t *plan, double *ms, int64_t
  * terms, r^N powers, entry x point accumulations, screening estimates / iterations / envelopes, levels */
 int libgrpp_b200_plan_counters(const libgrpp_b200_plan_t *plan, uint64_t *counters, int n);
 void libgrpp_b200_plan_destroy(libgrpp_b200_plan_t *plan);
+
+/* Learned grid-level model (no counterpart in libgrpp).
+ *
+ * libgrpp's type 2 radial quadrature (radial_type2_integral.c:242-318) doubles a
+ * nested Log3 grid level by level until every entry of a task has converged; the
+ * deepest level a task needs (0..8, i.e. 31..8191 points) is known only after the
+ * walk. The level model is an MLP (12 features -> 64 -> 64 -> 64 -> 9 levels, BF16
+ * weights, FP32 accumulation) that predicts it. LIBGRPP_B200_RADIAL_LEARNED uses the
+ * prediction to schedule the walk (tasks taken from a work queue, deepest predicted
+ * level first); every task is still walked until libgrpp's own stop rule ends it, so
+ * the results equal those of LIBGRPP_B200_RADIAL_PLAIN bit for bit.
+ *
+ * Parameter vector (FP32, LIBGRPP_B200_LEVEL_MODEL_PARAMS floats):
+ *   mean[12] std[12] W1[64][12] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[9][64] b4[9]
+ * Features of a task (radial work item): la, lb, max projector L, number of semilocal
+ * potentials, log(1+|CA|), log(1+|CB|), log of the min and max exponent of shell A, of
+ * shell B and of the potential terms; normalised as (f - mean) / std. */
+#define LIBGRPP_B200_LEVEL_MODEL_PARAMS 9761
+#define LIBGRPP_B200_LEVEL_FEATURES 12
+
+/* Install the model used by LIBGRPP_B200_RADIAL_LEARNED on the current device. */
+int libgrpp_b200_set_level_model(const float *params);
+
+/* Training data: run the batch with the plain walk; for each task that has semilocal
+ * potentials (in task order; *n_items of them, at most n_tasks) write its features
+ * (12 floats) and the level libgrpp's stop rule ended its walk at (-1 when every
+ * entry was settled by screening or analytically). */
+int libgrpp_b200_level_samples(const libgrpp_b200_batch_t *batch, float *features, int8_t *levels,
+                               int64_t *n_items);
+
+/* Mean cross-entropy and its gradient w.r.t. the (BF16-rounded) weights of the model
+ * on n samples (levels 0..8), computed by the training kernels; grad has
+ * LIBGRPP_B200_LEVEL_MODEL_PARAMS floats (the normalisation slots are 0). */
+int libgrpp_b200_mlp_grad(const float *params, const float *features, const int8_t *levels, int n, float *grad,
+                          float *loss);
+
+/* Adam training on the GPU (forward/backward/update kernels of this library): params
+ * holds the initial weights and the normalisation on entry and the trained FP32
+ * weights on return; epoch_loss[e] receives the mean cross-entropy of epoch e. */
+int libgrpp_b200_mlp_train(const float *features, const int8_t *levels, int64_t n, int epochs, int batch, float lr,
+                           uint32_t seed, float *params, float *epoch_loss);
+
+/* Predicted levels of n feature rows (the BF16 inference path the walk uses). */
+int libgrpp_b200_mlp_predict(const float *params, const float *features, int64_t n, int8_t *levels);
+
+/* Learned-mode statistics of the last execute(): time of the prediction and ordering
+ * kernels (ms) and the number of tasks whose walk went beyond the predicted level + 1. */
+int libgrpp_b200_plan_learned_stats(const libgrpp_b200_plan_t *plan, double *ms_predict, int64_t *fallbacks);
 
 /* Allocation-free type 2 integrals (no counterpart in libgrpp).
  *

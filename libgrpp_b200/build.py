@@ -19,7 +19,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 
 SOURCES = ["engine.cu", "tables.cpp", "capi.cpp", "noalloc.cu"]
-HEADERS = ["grpp_common.cuh", "specfunc.cuh", "mmd.cuh", "radial.cuh", "angular.cuh", "tables.h", "engine.h"]
+HEADERS = ["grpp_common.cuh", "specfunc.cuh", "mmd.cuh", "radial.cuh", "angular.cuh", "level_model.cuh", "tables.h",
+           "engine.h"]
 
 
 def _newer(target, deps):

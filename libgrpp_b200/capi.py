@@ -86,6 +86,14 @@ class LibGRPP:
         self._opt("libgrpp_b200_plan_stats", ct.c_int, [_V, _D, ct.POINTER(ct.c_int64)])
         self._opt("libgrpp_b200_plan_destroy", None, [_V])
         self._opt("libgrpp_b200_plan_counters", ct.c_int, [_V, ct.POINTER(ct.c_uint64), ct.c_int])
+        _F = ct.POINTER(ct.c_float)
+        _B = ct.POINTER(ct.c_int8)
+        self._opt("libgrpp_b200_plan_learned_stats", ct.c_int, [_V, _D, ct.POINTER(ct.c_int64)])
+        self._opt("libgrpp_b200_set_level_model", ct.c_int, [_F])
+        self._opt("libgrpp_b200_level_samples", ct.c_int, [_V, _F, _B, ct.POINTER(ct.c_int64)])
+        self._opt("libgrpp_b200_mlp_grad", ct.c_int, [_F, _F, _B, ct.c_int, _F, _F])
+        self._opt("libgrpp_b200_mlp_train", ct.c_int, [_F, _B, ct.c_int64, ct.c_int, ct.c_int, ct.c_float, ct.c_uint32, _F, _F])
+        self._opt("libgrpp_b200_mlp_predict", ct.c_int, [_F, _F, ct.c_int64, _B])
         self.lib.libgrpp_init()
 
     def _opt(self, name, res, args):
@@ -185,6 +193,8 @@ class LibGRPP:
 
     # ------------------------------------------------------------ batched (GPU engine)
     def full_grpp_batch(self, batch, radial_mode=0):
+        if radial_mode == 1:
+            self.ensure_level_model()
         n = int(batch.block_offsets()[-1])
         outs = [np.zeros(max(n, 1)) for _ in range(4)]
         rc = self.lib.libgrpp_b200_full_grpp_batch(ct.byref(batch.struct), radial_mode, *[_dp(x) for x in outs])
@@ -213,7 +223,73 @@ class LibGRPP:
             raise RuntimeError(self.last_error_message())
         return v.value
 
+    # ------------------------------------------------------------ learned grid-level model
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed ({rc}): {self.last_error_message()}")
+
+    def set_level_model(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(self.lib.libgrpp_b200_set_level_model(p.ctypes.data_as(ct.POINTER(ct.c_float))),
+                    "libgrpp_b200_set_level_model")
+        self._lm_set = True
+
+    def level_samples(self, batch):
+        """(features [n, 12] float32, stop level [n] int8, -1 if not walked) of every radial task."""
+        nt = max(len(batch.task_a), 1)
+        X = np.zeros((nt, 12), dtype=np.float32)
+        y = np.zeros(nt, dtype=np.int8)
+        n = ct.c_int64(0)
+        self._check(self.lib.libgrpp_b200_level_samples(ct.byref(batch.struct), X.ctypes.data_as(ct.POINTER(ct.c_float)),
+                                                        y.ctypes.data_as(ct.POINTER(ct.c_int8)), ct.byref(n)),
+                    "libgrpp_b200_level_samples")
+        return X[: n.value], y[: n.value]
+
+    def mlp_grad(self, params, X, y):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.int8)
+        g = np.zeros_like(p)
+        loss = ct.c_float(0.0)
+        F = ct.POINTER(ct.c_float)
+        self._check(self.lib.libgrpp_b200_mlp_grad(p.ctypes.data_as(F), X.ctypes.data_as(F),
+                                                   y.ctypes.data_as(ct.POINTER(ct.c_int8)), len(y), g.ctypes.data_as(F),
+                                                   ct.byref(loss)), "libgrpp_b200_mlp_grad")
+        return g, float(loss.value)
+
+    def mlp_train(self, params, X, y, epochs=4, batch=2048, lr=2e-3, seed=0):
+        p = np.array(params, dtype=np.float32, copy=True)
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.int8)
+        losses = np.zeros(epochs, dtype=np.float32)
+        F = ct.POINTER(ct.c_float)
+        self._check(self.lib.libgrpp_b200_mlp_train(X.ctypes.data_as(F), y.ctypes.data_as(ct.POINTER(ct.c_int8)), len(y),
+                                                    epochs, batch, lr, seed, p.ctypes.data_as(F), losses.ctypes.data_as(F)),
+                    "libgrpp_b200_mlp_train")
+        return p, losses
+
+    def mlp_predict(self, params, X):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        out = np.zeros(len(X), dtype=np.int8)
+        F = ct.POINTER(ct.c_float)
+        self._check(self.lib.libgrpp_b200_mlp_predict(p.ctypes.data_as(F), X.ctypes.data_as(F), len(X),
+                                                      out.ctypes.data_as(ct.POINTER(ct.c_int8))),
+                    "libgrpp_b200_mlp_predict")
+        return out
+
+    def ensure_level_model(self):
+        """Install the committed level model (libgrpp_b200/level_model.bin) once, for the
+        learned radial mode; callers that set their own model first are left alone."""
+        if getattr(self, "_lm_set", False) or not self.has("libgrpp_b200_set_level_model"):
+            return
+        from . import level_model
+        if os.path.exists(level_model.MODEL_FILE):
+            self.set_level_model(level_model.load()[0])
+
     def plan(self, batch, radial_mode=0) -> "Plan":
+        if radial_mode == 1:
+            self.ensure_level_model()
         return Plan(self, batch, radial_mode)
 
     def last_error(self) -> int:
@@ -276,6 +352,12 @@ class Plan:
         return {"ms_total": ms[0], "ms_type1": ms[1], "ms_radial": ms[2], "ms_assembly": ms[3], "ms_screen": ms[4],
                 "n_tasks": int(cnt[0]), "n_radial": int(cnt[1]), "n_type1_items": int(cnt[2]),
                 "n_entries": int(cnt[3]), "h2d_bytes": int(cnt[4])}
+
+    def learned_stats(self):
+        ms = ct.c_double(0.0)
+        fb = ct.c_int64(0)
+        self.lib.lib.libgrpp_b200_plan_learned_stats(self.h, ct.byref(ms), ct.byref(fb))
+        return {"ms_predict": ms.value, "fallbacks": int(fb.value)}
 
     COUNTERS = ("screen_cycles", "quad_cycles", "items", "points", "bessel", "prim_pts", "term_pts", "pow_pts",
                 "accum", "scr_combos", "scr_iters", "scr_final", "levels")

@@ -707,5 +707,47 @@ int libgrpp_b200_plan_counters(const libgrpp_b200_plan_t *plan, uint64_t *counte
 
 void libgrpp_b200_plan_destroy(libgrpp_b200_plan_t *plan) { grpp::plan_destroy((grpp::Plan *)plan); }
 
+int libgrpp_b200_plan_learned_stats(const libgrpp_b200_plan_t *plan, double *ms_predict, int64_t *fallbacks)
+{
+    if (!plan) return LIBGRPP_B200_ERR_INVALID;
+    const grpp::RunStats *st = grpp::plan_stats((const grpp::Plan *)plan);
+    if (ms_predict) *ms_predict = st->ms_predict;
+    if (fallbacks) *fallbacks = st->fallbacks;
+    return 0;
+}
+
+int libgrpp_b200_set_level_model(const float *params)
+{
+    if (!params) return LIBGRPP_B200_ERR_INVALID;
+    return grpp::set_level_model(params);
+}
+
+int libgrpp_b200_level_samples(const libgrpp_b200_batch_t *b, float *features, int8_t *levels, int64_t *n_items)
+{
+    if (!check_init()) return LIBGRPP_B200_ERR_NOT_INIT;
+    if (!b || !features || !levels || !n_items) return LIBGRPP_B200_ERR_INVALID;
+    return grpp::level_samples(b, features, levels, n_items);
+}
+
+int libgrpp_b200_mlp_grad(const float *params, const float *features, const int8_t *levels, int n, float *grad,
+                          float *loss)
+{
+    if (!params || !features || !levels || !grad || !loss) return LIBGRPP_B200_ERR_INVALID;
+    return grpp::mlp_grad(params, features, levels, n, grad, loss);
+}
+
+int libgrpp_b200_mlp_train(const float *features, const int8_t *levels, int64_t n, int epochs, int batch, float lr,
+                           uint32_t seed, float *params, float *epoch_loss)
+{
+    if (!params || !features || !levels) return LIBGRPP_B200_ERR_INVALID;
+    return grpp::mlp_train(features, levels, n, epochs, batch, lr, seed, params, epoch_loss);
+}
+
+int libgrpp_b200_mlp_predict(const float *params, const float *features, int64_t n, int8_t *levels)
+{
+    if (!params || !features || !levels) return LIBGRPP_B200_ERR_INVALID;
+    return grpp::mlp_predict(params, features, n, levels);
+}
+
 }  // extern "C"
 #pragma GCC visibility pop

@@ -7,7 +7,9 @@
 //                     and <S|U_oc|oc>, <S|oc> Cartesian blocks for every (shell, centre)
 //                     that needs outercore projections
 //   3. oc_proj_kernel Cartesian -> real spherical transform of those blocks
-//   4. radial_kernel  Q tables of every semilocal potential of every task
+//   4. radial kernels Q tables of every semilocal potential of every task: screening,
+//                     then (learned mode) the level model orders the tasks deepest
+//                     predicted level first, then the grid walk
 //   5. final_kernel   per task: T1 + sum type 2 + sum 2/(2L+1) SO + outercore, in
 //                     libgrpp_full_grpp_integrals' accumulation order
 #include <algorithm>
@@ -23,6 +25,7 @@
 #include "mmd.cuh"
 #include "radial.cuh"
 #include "angular.cuh"
+#include "level_model.cuh"
 #include "tables.h"
 #include "engine.h"
 
@@ -80,6 +83,10 @@ struct DeviceState {
     DevBuf in, scratch, out;
     DevBuf atab;
     size_t atab_used = 0;
+    // learned grid-level model (libgrpp_b200_set_level_model): FP32 normalisation, BF16 weights
+    float *lm_norm = nullptr;
+    __nv_bfloat16 *lm_w = nullptr;
+    bool lm_ready = false;
     std::vector<int64_t> atab_off;
     DevBuf atab_off_dev;
     std::mutex mu;
@@ -128,9 +135,9 @@ int init_device_state(DeviceState &st, int device)
     st.atab_off.assign((kMaxL + 2) * (kMaxL + 2), -1);
     GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    GRPP_CUDA(cudaFuncSetAttribute(radial_walk_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-    GRPP_CUDA(cudaFuncSetAttribute(radial_walk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(radial_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_train_smem_bytes()));
     st.device = device;
     st.ready = true;
     return 0;
@@ -283,6 +290,8 @@ struct Plan {
     double *outs[4] = {nullptr, nullptr, nullptr, nullptr};
     int *status = nullptr;
     unsigned long long *counters = nullptr;  // kRadCntNum slots inside the status area
+    int8_t *stop_level = nullptr, *pred_level = nullptr;  // per radial item
+    int *order = nullptr, *lm_ctl = nullptr;               // learned mode: item order; n_order, queue, cursor[9]
     MmdArgs mmd;
     int mmd_blocks = 0, mmd_threads = 128, mmd_kpl = 32;
     size_t mmd_smem = 0;
@@ -580,7 +589,9 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     const int64_t qn = std::max<int64_t>(qtot, 1), cn = std::max<int64_t>(cart_tot, 1), sn = std::max<int64_t>(sph_tot, 1);
     const int64_t nrad = std::max<int64_t>((int64_t)rad_task.size(), 1);
     const int64_t flag_words = (qn + nrad + 2 * 8) / 8 + 1;  // entry flags + per-task walk flags, in doubles
-    const size_t scratch_bytes = (size_t)(3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words) * sizeof(double);
+    // per radial item: stop level, predicted level (int8), order (int); learned-mode control words
+    const int64_t lm_words = (2 * nrad + 4 * nrad + 16 * 4) / 8 + 4;
+    const size_t scratch_bytes = (size_t)(3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words + lm_words) * sizeof(double);
     GRPP_CUDA(bscr->ensure(scratch_bytes));
     GRPP_CUDA(bout->ensure((size_t)4 * std::max<int64_t>(out_tot, 1) * sizeof(double)));
     P.scratch_bytes = (int64_t)scratch_bytes;
@@ -589,6 +600,14 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     int *statusd = (int *)(Usd + sn);
     uint8_t *eflagd = (uint8_t *)(Usd + sn + 32);
     uint8_t *walkd = eflagd + qn;
+    int8_t *stopd = (int8_t *)(Usd + sn + 32 + flag_words);
+    int8_t *predd = stopd + nrad;
+    int *orderd = (int *)(((uintptr_t)(predd + nrad) + 15) & ~(uintptr_t)15);
+    int *lmctld = orderd + nrad;
+    P.stop_level = stopd;
+    P.pred_level = predd;
+    P.order = orderd;
+    P.lm_ctl = lmctld;
     double *o_arep = (double *)bout->p, *o_sx = o_arep + out_tot, *o_sy = o_sx + out_tot, *o_sz = o_sy + out_tot;
 
     int nsm = 0;
@@ -606,7 +625,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
 
     // ---------------------------------------------------------------- 2. MMD
     if (!items.empty()) {
-        MmdArgs m;
+        MmdArgs m{};
         m.items = at<MmdItem>(ib, o_items);
         m.n_items = (int)items.size();
         m.shell_L = at<int>(ib, o_shL);
@@ -640,7 +659,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
 
     // ---------------------------------------------------------------- 3. outercore projections
     if (!blk_shell.empty()) {
-        OcProjArgs o;
+        OcProjArgs o{};
         o.n = (int)blk_shell.size();
         o.blk_shell = at<int>(ib, o_bs);
         o.blk_ocshell = at<int>(ib, o_bo);
@@ -659,7 +678,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
 
     // ---------------------------------------------------------------- 4. radial
     if (!rad_task.empty()) {
-        RadialArgs r;
+        RadialArgs r{};
         r.n_items = (int)rad_task.size();
         r.item_task = at<int>(ib, o_rt);
         r.task_a = at<int>(ib, o_ta);
@@ -691,9 +710,12 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         r.Q = Qd;
         r.S_prev = Spd;
         r.scr = SCd;
-        r.stop_level = nullptr;
+        r.stop_level = stopd;
         r.pred_level = nullptr;
         r.fallback_count = statusd + 4;
+        r.order = nullptr;
+        r.n_order = lmctld;
+        r.queue = lmctld + 1;
         r.status = statusd;
         r.counters = (unsigned long long *)(statusd + 16);
         r.eflag = eflagd;
@@ -709,7 +731,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
 
     // ---------------------------------------------------------------- 5. final assembly
     {
-        FinalArgs f;
+        FinalArgs f{};
         f.n_tasks = (int)nt;
         f.task_a = at<int>(ib, o_ta);
         f.task_b = at<int>(ib, o_tb);
@@ -792,10 +814,25 @@ int plan_execute(Plan &P)
         radial_screen_flat_kernel<<<P.scr_blocks, kRadThreads, 0, s>>>(P.rad);
         GRPP_CUDA(cudaGetLastError());
         GRPP_CUDA(cudaEventRecord(st.ev[4], s));
-        if (P.opt.radial_mode == LIBGRPP_B200_RADIAL_LEARNED)
-            radial_walk_kernel<true><<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(P.rad);
-        else
-            radial_walk_kernel<false><<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(P.rad);
+        RadialArgs ra = P.rad;
+        if (P.opt.radial_mode == LIBGRPP_B200_RADIAL_LEARNED) {
+            if (!st.lm_ready) {
+                set_error(LIBGRPP_B200_ERR_INVALID, "learned radial mode needs a level model (libgrpp_b200_set_level_model)");
+                return LIBGRPP_B200_ERR_INVALID;
+            }
+            // predict every walked task's level, order deepest first, walk from the queue
+            GRPP_CUDA(cudaMemsetAsync(P.lm_ctl, 0, 16 * sizeof(int), s));
+            LevelModelDev lm{st.lm_norm, st.lm_w};
+            const int pblocks = (int)std::min<int64_t>((P.n_radial + 3) / 4, 148 * 16);
+            level_predict_kernel<<<pblocks, 128, 0, s>>>(P.rad, lm, P.pred_level);
+            GRPP_CUDA(cudaGetLastError());
+            level_order_kernel<<<1, 256, 0, s>>>((int)P.n_radial, P.pred_level, P.order, P.lm_ctl, P.lm_ctl + 2);
+            GRPP_CUDA(cudaGetLastError());
+            ra.order = P.order;
+            ra.pred_level = P.pred_level;
+            GRPP_CUDA(cudaEventRecord(st.ev[5], s));
+        }
+        radial_walk_kernel<<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(ra);
         GRPP_CUDA(cudaGetLastError());
     }
     GRPP_CUDA(cudaEventRecord(st.ev[2], s));
@@ -810,6 +847,10 @@ int plan_execute(Plan &P)
     cudaEventElapsedTime(&P.stats.ms_mmd, st.ev[0], st.ev[1]);
     cudaEventElapsedTime(&P.stats.ms_radial, st.ev[1], st.ev[2]);
     if (P.rad_blocks > 0) cudaEventElapsedTime(&P.stats.ms_screen, st.ev[1], st.ev[4]);
+    P.stats.ms_predict = 0.f;
+    if (P.rad_blocks > 0 && P.opt.radial_mode == LIBGRPP_B200_RADIAL_LEARNED)
+        cudaEventElapsedTime(&P.stats.ms_predict, st.ev[4], st.ev[5]);
+    P.stats.fallbacks = hstatus[4];
     cudaEventElapsedTime(&P.stats.ms_final, st.ev[2], st.ev[3]);
     cudaEventElapsedTime(&P.stats.ms_total, st.ev[0], st.ev[3]);
     P.stats.n_tasks = P.n_tasks;
@@ -920,6 +961,264 @@ int measure_fp64_peak(double *tflops)
     cudaEventElapsedTime(&ms, stp->ev[4], stp->ev[5]);
     cudaFree(d);
     *tflops = 2.0 * 8.0 * iters * (double)threads * blocks / (ms * 1e-3) / 1e12;
+    return 0;
+}
+
+// ------------------------------------------------------------------ learned grid-level model
+namespace {
+
+// device copy of a full parameter vector: FP32 normalisation + BF16 weights
+int upload_model(const float *params, float **norm, __nv_bfloat16 **w, cudaStream_t s)
+{
+    float *tmp = nullptr;
+    GRPP_CUDA(cudaMalloc(&tmp, kLmParams * sizeof(float)));
+    GRPP_CUDA(cudaMemcpyAsync(tmp, params, kLmParams * sizeof(float), cudaMemcpyHostToDevice, s));
+    if (!*norm) GRPP_CUDA(cudaMalloc(norm, 2 * kLmFeat * sizeof(float)));
+    if (!*w) GRPP_CUDA(cudaMalloc(w, kLmParams * sizeof(__nv_bfloat16)));
+    GRPP_CUDA(cudaMemcpyAsync(*norm, tmp, 2 * kLmFeat * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    mlp_to_bf16_kernel<<<40, 256, 0, s>>>(tmp, *w, kLmParams);
+    GRPP_CUDA(cudaGetLastError());
+    GRPP_CUDA(cudaStreamSynchronize(s));
+    cudaFree(tmp);
+    return 0;
+}
+
+int check_model_norm(const float *params)
+{
+    for (int k = 0; k < kLmFeat; k++)
+        if (!(params[kLmOffStd + k] > 0.f) || !std::isfinite(params[kLmOffMean + k])) {
+            set_error(LIBGRPP_B200_ERR_INVALID, "level model: feature scales must be positive and means finite");
+            return LIBGRPP_B200_ERR_INVALID;
+        }
+    return 0;
+}
+
+}  // namespace
+
+int set_level_model(const float *params)
+{
+    set_error(0, "");
+    int rc = 0;
+    DeviceState *stp = get_state(rc);
+    if (!stp) return rc;
+    if ((rc = check_model_norm(params))) return rc;
+    std::lock_guard<std::mutex> lk(stp->mu);
+    rc = upload_model(params, &stp->lm_norm, &stp->lm_w, stp->stream);
+    if (rc == 0) stp->lm_ready = true;
+    return rc;
+}
+
+// Plain walk of a batch; per radial item its 12 features and the level libgrpp's
+// adaptive quadrature stopped at (-1 for items whose entries all left at screening).
+int level_samples(const libgrpp_b200_batch_t *b, float *features, int8_t *levels, int64_t *n_items)
+{
+    set_error(0, "");
+    int rc = 0;
+    DeviceState *stp = get_state(rc);
+    if (!stp) return rc;
+    std::lock_guard<std::mutex> lk(stp->mu);
+    RunOptions opt;
+    Plan P;
+    rc = plan_build(*stp, b, opt, false, P);
+    if (rc) return rc;
+    *n_items = P.n_radial;
+    if (P.n_radial == 0) return 0;
+    GRPP_CUDA(cudaMemsetAsync(P.stop_level, -1, (size_t)P.n_radial, stp->stream));
+    rc = plan_execute(P);
+    if (rc) return rc;
+    float *fd = nullptr;
+    GRPP_CUDA(cudaMalloc(&fd, (size_t)P.n_radial * kLmFeat * sizeof(float)));
+    level_features_kernel<<<(int)std::min<int64_t>((P.n_radial + 127) / 128, 4096), 128, 0, stp->stream>>>(P.rad, fd);
+    GRPP_CUDA(cudaGetLastError());
+    GRPP_CUDA(cudaMemcpyAsync(features, fd, (size_t)P.n_radial * kLmFeat * sizeof(float), cudaMemcpyDeviceToHost, stp->stream));
+    GRPP_CUDA(cudaMemcpyAsync(levels, P.stop_level, (size_t)P.n_radial, cudaMemcpyDeviceToHost, stp->stream));
+    GRPP_CUDA(cudaStreamSynchronize(stp->stream));
+    cudaFree(fd);
+    // items the walk skipped keep -1 (their stop level was never written)
+    std::vector<uint8_t> walk((size_t)P.n_radial);
+    GRPP_CUDA(cudaMemcpy(walk.data(), P.rad.walk, (size_t)P.n_radial, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < P.n_radial; i++)
+        if (!walk[i]) levels[i] = -1;
+    return 0;
+}
+
+namespace {
+
+struct MlpDevice {
+    float *X = nullptr, *norm = nullptr, *w = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr, *loss = nullptr;
+    __nv_bfloat16 *wb = nullptr;
+    int8_t *y = nullptr;
+    int *idx = nullptr;
+    ~MlpDevice()
+    {
+        for (void *p : {(void *)X, (void *)norm, (void *)w, (void *)grad, (void *)m, (void *)v, (void *)loss, (void *)wb,
+                        (void *)y, (void *)idx})
+            if (p) cudaFree(p);
+    }
+};
+
+int mlp_setup(MlpDevice &d, const float *params, const float *X, const int8_t *y, int64_t n, cudaStream_t s)
+{
+    GRPP_CUDA(cudaMalloc(&d.X, (size_t)std::max<int64_t>(n, 1) * kLmFeat * sizeof(float)));
+    GRPP_CUDA(cudaMalloc(&d.y, (size_t)std::max<int64_t>(n, 1)));
+    GRPP_CUDA(cudaMalloc(&d.idx, (size_t)std::max<int64_t>(n, 1) * sizeof(int)));
+    GRPP_CUDA(cudaMalloc(&d.norm, 2 * kLmFeat * sizeof(float)));
+    GRPP_CUDA(cudaMalloc(&d.w, kLmParams * sizeof(float)));
+    GRPP_CUDA(cudaMalloc(&d.wb, kLmParams * sizeof(__nv_bfloat16)));
+    GRPP_CUDA(cudaMalloc(&d.grad, kLmParams * sizeof(float)));
+    GRPP_CUDA(cudaMalloc(&d.m, kLmParams * sizeof(float)));
+    GRPP_CUDA(cudaMalloc(&d.v, kLmParams * sizeof(float)));
+    GRPP_CUDA(cudaMalloc(&d.loss, 1024 * sizeof(float)));
+    if (n > 0) {
+        GRPP_CUDA(cudaMemcpyAsync(d.X, X, (size_t)n * kLmFeat * sizeof(float), cudaMemcpyHostToDevice, s));
+        if (y) GRPP_CUDA(cudaMemcpyAsync(d.y, y, (size_t)n, cudaMemcpyHostToDevice, s));
+    }
+    GRPP_CUDA(cudaMemcpyAsync(d.norm, params, 2 * kLmFeat * sizeof(float), cudaMemcpyHostToDevice, s));
+    GRPP_CUDA(cudaMemcpyAsync(d.w, params, kLmParams * sizeof(float), cudaMemcpyHostToDevice, s));
+    mlp_to_bf16_kernel<<<40, 256, 0, s>>>(d.w, d.wb, kLmParams);
+    GRPP_CUDA(cudaGetLastError());
+    GRPP_CUDA(cudaMemsetAsync(d.grad, 0, kLmParams * sizeof(float), s));
+    GRPP_CUDA(cudaMemsetAsync(d.m, 0, kLmParams * sizeof(float), s));
+    GRPP_CUDA(cudaMemsetAsync(d.v, 0, kLmParams * sizeof(float), s));
+    GRPP_CUDA(cudaMemsetAsync(d.loss, 0, 1024 * sizeof(float), s));
+    return 0;
+}
+
+int check_labels(const int8_t *y, int64_t n)
+{
+    for (int64_t i = 0; i < n; i++)
+        if (y[i] < 0 || y[i] >= kLmOut) {
+            set_error(LIBGRPP_B200_ERR_INVALID, "level labels must be 0..8");
+            return LIBGRPP_B200_ERR_INVALID;
+        }
+    return 0;
+}
+
+}  // namespace
+
+// Gradient (w.r.t. the BF16-rounded weights) and mean cross-entropy of the model on n samples.
+int mlp_grad(const float *params, const float *X, const int8_t *y, int n, float *grad, float *loss)
+{
+    set_error(0, "");
+    int rc = 0;
+    DeviceState *stp = get_state(rc);
+    if (!stp) return rc;
+    if (n <= 0) {
+        set_error(LIBGRPP_B200_ERR_INVALID, "mlp_grad needs at least one sample");
+        return LIBGRPP_B200_ERR_INVALID;
+    }
+    if ((rc = check_model_norm(params)) || (rc = check_labels(y, n))) return rc;
+    std::lock_guard<std::mutex> lk(stp->mu);
+    cudaStream_t s = stp->stream;
+    MlpDevice d;
+    if ((rc = mlp_setup(d, params, X, y, n, s))) return rc;
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; i++) idx[i] = i;
+    GRPP_CUDA(cudaMemcpyAsync(d.idx, idx.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+    MlpTrainArgs t{d.X, d.y, d.idx, n, 0, n, d.norm, d.wb, d.grad, d.loss};
+    mlp_train_kernel<<<(n + kLmTrainSamples - 1) / kLmTrainSamples, kLmTrainThreads, mlp_train_smem_bytes(), s>>>(t);
+    GRPP_CUDA(cudaGetLastError());
+    GRPP_CUDA(cudaMemcpyAsync(grad, d.grad, kLmParams * sizeof(float), cudaMemcpyDeviceToHost, s));
+    GRPP_CUDA(cudaMemcpyAsync(loss, d.loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+    GRPP_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < kLmOffW1; i++) grad[i] = 0.f;
+    return 0;
+}
+
+// Adam training of the model on n (features, level) pairs; params in: initial weights and
+// the feature normalisation, out: trained FP32 master weights. epoch_loss[e] = mean
+// cross-entropy seen during epoch e. Minibatches of `batch` samples, reshuffled per epoch.
+int mlp_train(const float *X, const int8_t *y, int64_t n, int epochs, int batch, float lr, uint32_t seed,
+              float *params, float *epoch_loss)
+{
+    set_error(0, "");
+    int rc = 0;
+    DeviceState *stp = get_state(rc);
+    if (!stp) return rc;
+    if (n <= 0 || epochs <= 0 || epochs > 1024 || batch <= 0 || n > (int64_t)INT32_MAX) {
+        set_error(LIBGRPP_B200_ERR_INVALID, "mlp_train: need n in 1..2^31-1, epochs in 1..1024, batch > 0");
+        return LIBGRPP_B200_ERR_INVALID;
+    }
+    if ((rc = check_model_norm(params)) || (rc = check_labels(y, n))) return rc;
+    std::lock_guard<std::mutex> lk(stp->mu);
+    cudaStream_t s = stp->stream;
+    MlpDevice d;
+    if ((rc = mlp_setup(d, params, X, y, n, s))) return rc;
+    std::vector<int> idx((size_t)n);
+    uint64_t state = 0x9E3779B97F4A7C15ull ^ seed;
+    auto rnd = [&state]() {  // splitmix64
+        state += 0x9E3779B97F4A7C15ull;
+        uint64_t z = state;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    const float b1 = 0.9f, b2 = 0.999f;
+    float p1 = 1.f, p2 = 1.f;
+    for (int ep = 0; ep < epochs; ep++) {
+        for (int64_t i = 0; i < n; i++) idx[i] = (int)i;
+        for (int64_t i = n - 1; i > 0; i--) std::swap(idx[i], idx[rnd() % (uint64_t)(i + 1)]);
+        GRPP_CUDA(cudaMemcpyAsync(d.idx, idx.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s));
+        int steps = 0;
+        for (int64_t b0 = 0; b0 < n; b0 += batch) {
+            const int bsz = (int)std::min<int64_t>(batch, n - b0);
+            MlpTrainArgs t{d.X, d.y, d.idx, (int)n, (int)b0, bsz, d.norm, d.wb, d.grad, d.loss + ep};
+            mlp_train_kernel<<<(bsz + kLmTrainSamples - 1) / kLmTrainSamples, kLmTrainThreads, mlp_train_smem_bytes(), s>>>(t);
+            GRPP_CUDA(cudaGetLastError());
+            p1 *= b1;
+            p2 *= b2;
+            AdamArgs ad{d.w, d.wb, d.grad, d.m, d.v, lr, b1, b2, 1e-8f, 1.f - p1, 1.f - p2};
+            mlp_adam_kernel<<<40, 256, 0, s>>>(ad);
+            GRPP_CUDA(cudaGetLastError());
+            steps++;
+        }
+        float l = 0.f;
+        GRPP_CUDA(cudaMemcpyAsync(&l, d.loss + ep, sizeof(float), cudaMemcpyDeviceToHost, s));
+        GRPP_CUDA(cudaStreamSynchronize(s));
+        if (epoch_loss) epoch_loss[ep] = l / (float)steps;
+    }
+    GRPP_CUDA(cudaMemcpyAsync(params + kLmOffW1, d.w + kLmOffW1, kLmNet * sizeof(float), cudaMemcpyDeviceToHost, s));
+    GRPP_CUDA(cudaStreamSynchronize(s));
+    return 0;
+}
+
+namespace {
+__global__ void mlp_predict_kernel(LevelModelDev m, const float *X, int n, int8_t *pred)
+{
+    __shared__ float hbuf[4][2 * kLmHid];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = blockIdx.x * 4 + warp; i < n; i += gridDim.x * 4) {
+        const int l = mlp_forward_warp(m, X + (size_t)i * kLmFeat, hbuf[warp], lane);
+        if (lane == 0) pred[i] = (int8_t)l;
+        __syncwarp();
+    }
+}
+}  // namespace
+
+// Predicted level (argmax) of n feature rows, with the BF16 inference path of the walk.
+int mlp_predict(const float *params, const float *X, int64_t n, int8_t *pred)
+{
+    set_error(0, "");
+    int rc = 0;
+    DeviceState *stp = get_state(rc);
+    if (!stp) return rc;
+    if (n <= 0 || n > (int64_t)INT32_MAX) {
+        set_error(LIBGRPP_B200_ERR_INVALID, "mlp_predict: need n in 1..2^31-1");
+        return LIBGRPP_B200_ERR_INVALID;
+    }
+    if ((rc = check_model_norm(params))) return rc;
+    std::lock_guard<std::mutex> lk(stp->mu);
+    cudaStream_t s = stp->stream;
+    MlpDevice d;
+    if ((rc = mlp_setup(d, params, X, nullptr, n, s))) return rc;
+    int8_t *pd = nullptr;
+    GRPP_CUDA(cudaMalloc(&pd, (size_t)n));
+    LevelModelDev lm{d.norm, d.wb};
+    mlp_predict_kernel<<<(int)std::min<int64_t>((n + 3) / 4, 148 * 16), 128, 0, s>>>(lm, d.X, (int)n, pd);
+    GRPP_CUDA(cudaGetLastError());
+    GRPP_CUDA(cudaMemcpyAsync(pred, pd, (size_t)n, cudaMemcpyDeviceToHost, s));
+    GRPP_CUDA(cudaStreamSynchronize(s));
+    cudaFree(pd);
     return 0;
 }
 

@@ -16,7 +16,7 @@ struct RunOptions {
 struct RunStats {
     int64_t n_tasks = 0, n_radial = 0, n_mmd = 0, n_entries = 0;
     int64_t fallbacks = 0;
-    float ms_total = 0.f, ms_mmd = 0.f, ms_radial = 0.f, ms_final = 0.f, ms_screen = 0.f;
+    float ms_total = 0.f, ms_mmd = 0.f, ms_radial = 0.f, ms_final = 0.f, ms_screen = 0.f, ms_predict = 0.f;
     unsigned long long radial_counters[16] = {0};  // RadialCounter slots (radial.cuh)
 };
 
@@ -42,5 +42,13 @@ const RunStats *plan_stats(const Plan *P);
 int64_t plan_h2d_bytes(const Plan *P);
 int set_device(int device);
 int measure_fp64_peak(double *tflops);
+
+// learned grid-level model (level_model.cuh)
+int set_level_model(const float *params);
+int level_samples(const libgrpp_b200_batch_t *b, float *features, int8_t *levels, int64_t *n_items);
+int mlp_grad(const float *params, const float *X, const int8_t *y, int n, float *grad, float *loss);
+int mlp_train(const float *X, const int8_t *y, int64_t n, int epochs, int batch, float lr, uint32_t seed,
+              float *params, float *epoch_loss);
+int mlp_predict(const float *params, const float *X, int64_t n, int8_t *pred);
 
 }  // namespace grpp

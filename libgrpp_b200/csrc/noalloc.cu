@@ -137,7 +137,7 @@ int setup(int dev)
     void *p = nullptr;
     NA_CUDA(cudaGetSymbolAddress(&p, g_scratch));
     g_scratch_ptr[dev] = (unsigned char *)p;
-    NA_CUDA(cudaFuncSetAttribute(radial_walk_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    NA_CUDA(cudaFuncSetAttribute(radial_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
     NA_CUDA(cudaFuncSetAttribute(final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     g_ready[dev] = true;
     return 0;
@@ -315,7 +315,7 @@ int run(const libgrpp_b200_batch_t *b, double *h_arep)
         NA_CUDA(cudaGetLastError());
     }
     if (!rad_task.empty()) {
-        RadialArgs r;
+        RadialArgs r{};
         memset(&r, 0, sizeof(r));
         r.n_items = (int)rad_task.size();
         r.item_task = (const int *)P(o_rt);
@@ -352,10 +352,10 @@ int run(const libgrpp_b200_batch_t *b, double *h_arep)
         radial_screen_kernel<<<(int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 32), kRadThreads>>>(r);
         NA_CUDA(cudaGetLastError());
         const size_t smem = (size_t)(npot + (l1m + 1) + (l2m + 1) + dn) * kRadRow * sizeof(double);
-        radial_walk_kernel<false><<<(int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 16), kRadThreads, smem>>>(r);
+        radial_walk_kernel<<<(int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 16), kRadThreads, smem>>>(r);
         NA_CUDA(cudaGetLastError());
     }
-    FinalArgs f;
+    FinalArgs f{};
     memset(&f, 0, sizeof(f));
     f.n_tasks = (int)nt;
     f.task_a = (const int *)P(o_ta);

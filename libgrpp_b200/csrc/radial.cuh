@@ -74,6 +74,10 @@ struct RadialArgs {
     int8_t *stop_level;         // per item: deepest level walked (learning labels), may be null
     const int8_t *pred_level;   // per item: predicted level (learned mode), may be null
     int *fallback_count;        // learned mode: items that needed more than predicted+1
+    // learned mode: the walk pops items from this order (deepest predicted level first)
+    const int *order;           // may be null: static round-robin over all items
+    const int *n_order;
+    int *queue;
     int *status;
     // operation counters (accumulated per CTA, one atomic add per item), see kRadCnt*
     unsigned long long *counters;
@@ -607,19 +611,73 @@ __device__ __forceinline__ void bessel_row_acc(int lmax, double x, double e, dou
 }
 
 constexpr int kRadRow = kRadThreads + 1;  // padded row stride of the chunk arrays (no bank conflicts)
+constexpr int kRadGridPts = 8191;         // points of levels 0..8 together
 
-template <bool LEARNED>
+// Level of point f of the nested grid in walk order (level 0: f = 0..30; level L >= 1:
+// f = 2^(L+4)-1 .. 2^(L+5)-2), and the point's index i on that level's grid of nr points.
+__device__ __forceinline__ void walk_point(int f, int &level, int &i, int &nr)
+{
+    const int lg = 31 - __clz(f + 1);  // floor(log2(f + 1))
+    level = lg > 4 ? lg - 4 : 0;
+    if (level == 0) {
+        i = f + 1;
+        nr = 31;
+    } else {
+        i = 2 * (f - ((1 << (level + 4)) - 1)) + 1;
+        nr = (1 << (level + 5)) - 1;
+    }
+}
+
+// last walk-order point of level L
+__device__ __forceinline__ int level_last_point(int L) { return (1 << (L + 5)) - 2; }
+
+// The nested Log3 grid of every task with entries left, one CTA per task.
+// Points are taken in walk order (level 0, then the new points of level 1, 2, ...)
+// in chunks of kRadThreads. Per chunk, thread t evaluates point f0 + t once for all
+// potentials and orders still needed (w U_p, F^A_l, F^B_l, r^N into shared memory);
+// then every thread advances the entries it owns over the chunk's points, in the
+// reference's order and association, applying libgrpp's per-level rules
+// (radial_type2_integral.c:285-315) when an entry passes the last point of a level:
+//   level 0: continue; forced refinement while |S|/|estimate| < 1e-3 (estimate valid);
+//   converged when |S_L - S_{L-1}| <= 1e-16; otherwise S_prev = S_L, S = S_L / 2.
+// An entry therefore ends with exactly the sum the level-by-level walk gives it.
+// The walk of a task stops at the first chunk boundary after which no entry is active;
+// points evaluated past that are never added. The orders, powers and potentials
+// evaluated per point shrink with the set of active entries.
 __global__ void __launch_bounds__(kRadThreads, 4) radial_walk_kernel(RadialArgs a)
 {
     __shared__ RadialShared sh;
+    __shared__ int s_need[2][4];  // per buffer: max l1, max l2, max N of active entries, potential mask
+    __shared__ int s_lvl;         // deepest level at which an entry converged
     extern __shared__ double chunk[];  // [npot + l1max+1 + l2max+1 + dn][kRadRow]
+    __shared__ int s_item;
     const int tid = threadIdx.x, lane = tid & 31;
-    for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
-        if (!a.walk[item]) continue;
+    int next_static = blockIdx.x;
+    for (;;) {
+        int item;
+        if (a.order) {
+            // work queue: one pop per CTA (every loop iteration below ends with a barrier)
+            __syncthreads();
+            if (tid == 0) {
+                const int k = atomicAdd(a.queue, 1);
+                s_item = k < *a.n_order ? a.order[k] : -1;
+            }
+            __syncthreads();
+            item = s_item;
+            if (item < 0) break;
+        } else {
+            item = next_static;
+            next_static += gridDim.x;
+            if (item >= a.n_items) break;
+            if (!a.walk[item]) continue;
+        }
         __syncthreads();
+        if (tid < 8) s_need[tid >> 2][tid & 3] = tid == 3 || tid == 7 ? 0 : -1;
+        if (tid == 0) s_lvl = 0;
         load_task(a, item, sh, tid, kRadThreads);
         const int64_t qo = a.q_off[item];
-        double *Q = a.Q + qo, *Sp = a.S_prev + qo, *SC = a.scr + qo;
+        double *Q = a.Q + qo, *Sp = a.S_prev + qo;
+        const double *SC = a.scr + qo;
         uint8_t *EF = a.eflag + qo;
         const int nE = sh.n_entries, np_a = sh.np_a, np_b = sh.np_b;
         const int npot = sh.npot, l1m = sh.l1max_all, l2m = sh.l2max_all, dn = sh.d_n;
@@ -628,95 +686,145 @@ __global__ void __launch_bounds__(kRadThreads, 4) radial_walk_kernel(RadialArgs 
         double *cf2 = cf1 + (l1m + 1) * kRadRow;   // [l2m+1][kRadRow]
         double *crn = cf2 + (l2m + 1) * kRadRow;   // [dn][kRadRow]
         const long long t0 = clock64();
-        unsigned long long c_pts = 0, c_acc = 0;
-        int level_reached = 0, nr = 31;
-        for (int level = 0; level <= kRadMaxLevel; level++) {
-            if (level > 0) nr = 2 * nr + 1;
-            const int npts = level == 0 ? nr : (nr + 1) / 2;  // new points of this level
-            level_reached = level;
-            if (level > 0) {
-                for (int e = tid; e < nE; e += kRadThreads)
-                    if (EF[e] & kEntActive) {
-                        const double s = Q[e];
-                        Sp[e] = s;
-                        Q[e] = 0.5 * s;
-                    }
-            }
-            for (int p0 = 0; p0 < npts; p0 += kRadThreads) {
-                const int np = min(kRadThreads, npts - p0);
-                __syncthreads();
-                if (tid < np) {
-                    const int i = level == 0 ? (p0 + tid + 1) : 2 * (p0 + tid) + 1;
-                    double r, w;
-                    log3_point(i, nr, r, w);
-                    const double r2 = r * r;
-                    for (int pp = 0; pp < npot; pp++) {
-                        double u = 0.0;
-                        for (int k = 0; k < sh.pn[pp]; k++) {
-                            const int tk = sh.poff[pp] + k;
-                            u += sh.tcoef[tk] * pow(r, sh.tpow[tk] - 2) * exp(-sh.talpha[tk] * r2);
-                        }
-                        cwu[pp * kRadRow + tid] = w * u;
-                    }
-                    for (int l = 0; l <= l1m; l++) cf1[l * kRadRow + tid] = 0.0;
-                    for (int l = 0; l <= l2m; l++) cf2[l * kRadRow + tid] = 0.0;
-                    const double dA2 = (r - sh.CA) * (r - sh.CA), dB2 = (r - sh.CB) * (r - sh.CB);
-#pragma unroll 1
-                    for (int q = 0; q < np_a; q++)
-                        bessel_row_acc(l1m, sh.ka[q] * r, sh.ca[q] * exp(-sh.xa[q] * dA2), cf1 + tid, kRadRow);
-#pragma unroll 1
-                    for (int q = 0; q < np_b; q++)
-                        bessel_row_acc(l2m, sh.kb[q] * r, sh.cb[q] * exp(-sh.xb[q] * dB2), cf2 + tid, kRadRow);
-                    for (int n = 0; n < dn; n++) crn[n * kRadRow + tid] = pow(r, n);
-                    c_pts++;
-                }
-                __syncthreads();
-                for (int e = tid; e < nE; e += kRadThreads) {
-                    if (!(EF[e] & kEntActive)) continue;
+        unsigned long long c_acc = 0;
+        // what the entries active after screening need from each point
+        {
+            int n1 = -1, n2 = -1, nN = -1, mask = 0;
+            for (int e = tid; e < nE; e += kRadThreads)
+                if (EF[e] & kEntActive) {
                     int p, l1, l2, N;
                     decode_entry(sh, e, p, l1, l2, N);
-                    const double *pwu = cwu + p * kRadRow, *p1 = cf1 + l1 * kRadRow, *p2 = cf2 + l2 * kRadRow,
-                                 *pn = crn + N * kRadRow;
-                    double s = Q[e];
-                    for (int q = 0; q < np; q++)
-                        s = __dadd_rn(s, __dmul_rn(__dmul_rn(__dmul_rn(pwu[q], p1[q]), p2[q]), pn[q]));
-                    Q[e] = s;
-                    c_acc += np;
+                    n1 = max(n1, l1);
+                    n2 = max(n2, l2);
+                    nN = max(nN, N);
+                    mask |= 1 << p;
                 }
-            }
-            // convergence bookkeeping (radial_type2_integral.c:285-315)
-            int active = 0;
-            for (int e = tid; e < nE; e += kRadThreads) {
-                const uint8_t f = EF[e];
-                if (!(f & kEntActive)) continue;
-                if (level == 0) {
-                    active = 1;
-                    continue;
-                }
-                const double s = Q[e];
-                if ((f & kEntScrOk) && (fabs(s) / fabs(SC[e]) < 0.001)) {
-                    active = 1;
-                    continue;
-                }
-                if (fabs(s - Sp[e]) <= 1e-16) EF[e] = f & ~kEntActive;
-                else active = 1;
-            }
-            if (!__syncthreads_or(active)) break;
+            atomicMax(&s_need[1][0], n1);
+            atomicMax(&s_need[1][1], n2);
+            atomicMax(&s_need[1][2], nN);
+            atomicOr(&s_need[1][3], mask);
         }
-        if (tid == 0 && a.stop_level) a.stop_level[item] = (int8_t)level_reached;
-        if (a.counters) {
-            unsigned long long v[2] = {c_pts, c_acc};
-            for (int k = 0; k < 2; k++)
-                for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-            if (lane == 0) {
-                atomicAdd(a.counters + kRadCntPoints, v[0]);
-                atomicAdd(a.counters + kRadCntBessel, v[0] * (unsigned long long)(np_a * (l1m + 1) + np_b * (l2m + 1)));
-                atomicAdd(a.counters + kRadCntPrimPts, v[0] * (unsigned long long)(np_a + np_b));
-                atomicAdd(a.counters + kRadCntTermPts, v[0] * (unsigned long long)sh.nterm_tot);
-                atomicAdd(a.counters + kRadCntPowPts, v[0] * (unsigned long long)dn);
-                atomicAdd(a.counters + kRadCntAccum, v[1]);
+        int any = 1, chunk_no = 0;
+        for (int f0 = 0; f0 < kRadGridPts; f0 += kRadThreads, chunk_no++) {
+            const int np = min(kRadThreads, kRadGridPts - f0);
+            any = __syncthreads_or(any);
+            if (!any) break;
+            const int nb = (chunk_no + 1) & 1;  // buffer written by the previous chunk (the scan for chunk 0)
+            const int u1 = s_need[nb][0], u2 = s_need[nb][1], uN = s_need[nb][2], umask = s_need[nb][3];
+            // this chunk's buffer: nobody reads or writes it between the two barriers
+            if (tid < 4) s_need[chunk_no & 1][tid] = tid == 3 ? 0 : -1;
+            if (tid < np) {
+                int lev, i, nr;
+                walk_point(f0 + tid, lev, i, nr);
+                double r, w;
+                log3_point(i, nr, r, w);
+                const double r2 = r * r, ir = 1.0 / r, ir2 = 1.0 / r2;
+                for (int pp = 0; pp < npot; pp++) {
+                    if (!((umask >> pp) & 1)) continue;
+                    double u = 0.0;
+                    for (int k = 0; k < sh.pn[pp]; k++) {
+                        const int tk = sh.poff[pp] + k;
+                        const double ex = exp(-sh.talpha[tk] * r2);
+                        if (ex == 0.0) continue;  // the term adds an exact zero
+                        const int pw = sh.tpow[tk];
+                        const double rp = pw == 2 ? 1.0 : (pw == 1 ? ir : ir2);  // r^(n-2)
+                        u += sh.tcoef[tk] * rp * ex;
+                    }
+                    cwu[pp * kRadRow + tid] = w * u;
+                }
+                for (int l = 0; l <= u1; l++) cf1[l * kRadRow + tid] = 0.0;
+                for (int l = 0; l <= u2; l++) cf2[l * kRadRow + tid] = 0.0;
+                const double dA2 = (r - sh.CA) * (r - sh.CA), dB2 = (r - sh.CB) * (r - sh.CB);
+                if (u1 >= 0) {
+#pragma unroll 1
+                    for (int q = 0; q < np_a; q++) {
+                        const double e = sh.ca[q] * exp(-sh.xa[q] * dA2);
+                        if (e != 0.0) bessel_row_acc(u1, sh.ka[q] * r, e, cf1 + tid, kRadRow);
+                    }
+                }
+                if (u2 >= 0) {
+#pragma unroll 1
+                    for (int q = 0; q < np_b; q++) {
+                        const double e = sh.cb[q] * exp(-sh.xb[q] * dB2);
+                        if (e != 0.0) bessel_row_acc(u2, sh.kb[q] * r, e, cf2 + tid, kRadRow);
+                    }
+                }
+                double rn = 1.0;
+                for (int n = 0; n <= uN; n++) {
+                    crn[n * kRadRow + tid] = rn;
+                    rn *= r;
+                }
             }
+            __syncthreads();
+            int lev0, i0, nr0;
+            walk_point(f0, lev0, i0, nr0);
+            int my_active = 0, n1 = -1, n2 = -1, nN = -1, mask = 0, my_lvl = 0;
+            for (int e = tid; e < nE; e += kRadThreads) {
+                uint8_t fl = EF[e];
+                if (!(fl & kEntActive)) continue;
+                int p, l1, l2, N;
+                decode_entry(sh, e, p, l1, l2, N);
+                const double *pwu = cwu + p * kRadRow, *p1 = cf1 + l1 * kRadRow, *p2 = cf2 + l2 * kRadRow,
+                             *pn = crn + N * kRadRow;
+                double s = Q[e], sp = Sp[e];
+                int q = 0, L = lev0;
+                while (q < np) {
+                    const int lend = level_last_point(L);
+                    const int qe = min(np, lend - f0 + 1);
+                    for (; q < qe; q++) s = __dadd_rn(s, __dmul_rn(__dmul_rn(__dmul_rn(pwu[q], p1[q]), p2[q]), pn[q]));
+                    if (f0 + qe - 1 != lend) break;  // level continues in the next chunk
+                    // end of level L for this entry (radial_type2_integral.c:285-315)
+                    const bool forced = L == 0 || ((fl & kEntScrOk) && (fabs(s) / fabs(SC[e]) < 0.001));
+                    if (!forced && fabs(s - sp) <= 1e-16) {
+                        fl &= ~kEntActive;
+                        my_lvl = max(my_lvl, L);
+                        break;
+                    }
+                    if (L < kRadMaxLevel) {
+                        sp = s;
+                        s = 0.5 * s;
+                    }
+                    L++;
+                }
+                c_acc += q;
+                Q[e] = s;
+                Sp[e] = sp;
+                EF[e] = fl;
+                if (fl & kEntActive) {
+                    my_active = 1;
+                    n1 = max(n1, l1);
+                    n2 = max(n2, l2);
+                    nN = max(nN, N);
+                    mask |= 1 << p;
+                }
+            }
+            if (my_active) {
+                atomicMax(&s_need[chunk_no & 1][0], n1);
+                atomicMax(&s_need[chunk_no & 1][1], n2);
+                atomicMax(&s_need[chunk_no & 1][2], nN);
+                atomicOr(&s_need[chunk_no & 1][3], mask);
+            }
+            if (my_lvl) atomicMax(&s_lvl, my_lvl);
+            any = my_active;
+        }
+        any = __syncthreads_or(any);
+        // deepest level walked: the cap if entries are still active, else the last convergence
+        const int level_reached = any ? kRadMaxLevel : s_lvl;
+        if (tid == 0 && a.stop_level) a.stop_level[item] = (int8_t)level_reached;
+        if (tid == 0 && a.pred_level && level_reached > a.pred_level[item] + 1) atomicAdd(a.fallback_count, 1);
+        if (a.counters) {
+            unsigned long long v = c_acc;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) atomicAdd(a.counters + kRadCntAccum, v);
             if (tid == 0) {
+                // algorithmic work of the shared grid up to the stop level (every point once,
+                // every order and potential term at every point)
+                const unsigned long long pts = (unsigned long long)((1 << (level_reached + 5)) - 1);
+                atomicAdd(a.counters + kRadCntPoints, pts);
+                atomicAdd(a.counters + kRadCntBessel, pts * (unsigned long long)(np_a * (l1m + 1) + np_b * (l2m + 1)));
+                atomicAdd(a.counters + kRadCntPrimPts, pts * (unsigned long long)(np_a + np_b));
+                atomicAdd(a.counters + kRadCntTermPts, pts * (unsigned long long)sh.nterm_tot);
+                atomicAdd(a.counters + kRadCntPowPts, pts * (unsigned long long)dn);
                 atomicAdd(a.counters + kRadCntQuadCycles, (unsigned long long)(clock64() - t0));
                 atomicAdd(a.counters + kRadCntItems, 1ull);
                 atomicAdd(a.counters + kRadCntLevels, (unsigned long long)(level_reached + 1));

@@ -16,11 +16,20 @@ Fixtures (npz): the flattened task description (``b_*`` arrays), the task list,
 the reference's per-task blocks (``ref_arep`` ... ``ref_so_z``) and their
 sensitivity to last-bit input changes (``env_*``: the largest change of each
 element when the reference is re-run with exponents, coefficients and
-coordinates moved by 4 units of roundoff). H2O and Cs
+coordinates moved by up to 4 units of roundoff: uniformly scaled, and
+independently per primitive with a seeded random draw, tests/util.py
+``perturbed``). H2O and Cs
 hold every task; ThO, UO2 and KCs hold a seeded sample of shell pairs x all
 centres (the full matrices are tens of MB). H2O also holds libgrpp's
 shipped GRPP gradient matrices d V / d R_atom (36 lower triangles from
 test/H2O/{arep,so_x,so_y,so_z}_grad_{0,1,2}{x,y,z}.txt).
+
+Two more fixtures pin the engine on the seeded synthetic workloads it is
+benchmarked on (libgrpp_b200.synthetic): config1.npz, 512 seeded tasks of the
+config-1 task list (64 atoms, s..g shells, U_L + projectors l = 0..4), and
+config2.npz, 384 seeded tasks of config 2 (full GRPP: U_L, projectors,
+spin-orbit and outercore terms, basis up to h). Their reference values and
+envelopes come from the same compiled libgrpp.
 """
 from __future__ import annotations
 
@@ -35,6 +44,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
+from libgrpp_b200 import synthetic  # noqa: E402
 from libgrpp_b200.capi import LibGRPP  # noqa: E402
 from libgrpp_b200.formats import read_lower_triangle, read_system  # noqa: E402
 from tests.util import envelope  # noqa: E402
@@ -76,6 +86,38 @@ def sample_tasks(system, n_pairs, seed):
     return a, b, c
 
 
+# synthetic fixture -> (generator, number of seeded tasks, sampling seed)
+SYNTHETIC = {"config1": (synthetic.config1, 512, 11), "config2": (synthetic.config2, 384, 12)}
+
+
+def write_fixture(name, system, a, b, c, outs, env, extra=None):
+    batch = system.batch(a, b, c)
+    data = dict(batch_arrays(batch))
+    data.update(task_a=a, task_b=b, task_c=c, n_basis=system.n_basis(),
+                basis_offsets=system.basis_offsets(), cart_order=system.cart_order)
+    for m, comp in enumerate(COMPS):
+        data["ref_" + comp] = outs[m]
+        data["env_" + comp] = env[m]
+    if extra:
+        data.update(extra)
+    out = os.path.join(HERE, f"{name.lower()}.npz")
+    np.savez_compressed(out, **data)
+    return out
+
+
+def make_synthetic(lib, name):
+    gen, n, seed = SYNTHETIC[name]
+    system = gen()
+    a, b, c = system.all_tasks()
+    sel = np.sort(np.random.default_rng(seed).choice(len(a), n, replace=False))
+    a, b, c = a[sel], b[sel], c[sel]
+    outs, env = envelope(lib, system.batch(a, b, c))
+    n_ill = sum(int(np.sum(e > 1e-10)) for e in env)
+    out = write_fixture(name, system, a, b, c, outs, env)
+    print(f"{name}: {len(a)} tasks -> {os.path.relpath(out, ROOT)} ({os.path.getsize(out) / 1e3:.0f} kB); "
+          f"{n_ill} elements move by more than 1e-10 under 4-ulp input changes")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default="/root/reference")
@@ -83,6 +125,10 @@ def main():
     ap.add_argument("--pairs", type=int, default=48)
     args = ap.parse_args()
     lib = LibGRPP(os.path.join(ROOT, "oracle", "_ref", "libgrpp_ref.so"))
+    for name in SYNTHETIC:
+        if args.only and name not in args.only:
+            continue
+        make_synthetic(lib, name)
     for name, (full, tol) in FIXTURES.items():
         if args.only and name not in args.only:
             continue

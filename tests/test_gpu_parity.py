@@ -20,7 +20,7 @@ from tests.util import COMPS, envelope, load_fixture, parity, system_from_fixtur
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name", ["h2o", "cs", "kcs", "tho", "uo2"])
+@pytest.mark.parametrize("name", ["h2o", "cs", "kcs", "tho", "uo2", "config1", "config2"])
 def test_fixture_blocks(gpu_lib, name):
     batch, z = load_fixture(name)
     outs = gpu_lib.full_grpp_batch(batch)

@@ -47,6 +47,20 @@ def load_fixture(name: str):
     return BatchArrays(**arrays), z
 
 
+def fixture_subset(batch, z, idx):
+    """Tasks idx of a fixture: the sub-batch and, per component, the reference blocks and envelopes."""
+    idx = np.asarray(idx)
+    off = batch.block_offsets()
+    d = {k: v for k, v in batch.__dict__.items() if not k.startswith("_")}
+    for k in ("task_a", "task_b", "task_c"):
+        d[k] = np.ascontiguousarray(d[k][idx])
+    sub = BatchArrays(**d)
+    sel = np.concatenate([np.arange(off[t], off[t + 1]) for t in idx])
+    ref = {c: z["ref_" + c][sel] for c in COMPS}
+    env = {c: z["env_" + c][sel] for c in COMPS}
+    return sub, ref, env
+
+
 def max_abs(a, b):
     return float(np.max(np.abs(np.asarray(a) - np.asarray(b)))) if len(a) else 0.0
 
@@ -102,12 +116,19 @@ def perturbed(batch: BatchArrays, mode: int) -> BatchArrays:
     """The same workload with inputs moved by a few units in the last place:
     mode 1 scales every exponent by (1 + 4u); mode 2 scales contraction and
     potential coefficients by (1 - 4u), (1 + 4u) and every coordinate by (1 + 4u)
-    (coincident centres stay coincident)."""
+    (coincident centres stay coincident); modes 3 and 4 move every exponent and
+    coefficient independently by a seeded random whole number of units in [-4, 4]
+    (a uniform scaling can leave a cancelling sum's rounding pattern unchanged,
+    independent changes do not)."""
     d = {k: v for k, v in batch.__dict__.items() if not k.startswith("_")}
     d = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
     if mode == 1:
         d["prim_alpha"] = d["prim_alpha"] * (1 + 4 * U)
         d["pot_alpha"] = d["pot_alpha"] * (1 + 4 * U)
+    elif mode in (3, 4):
+        rng = np.random.default_rng(mode)
+        for k in ("prim_alpha", "pot_alpha", "prim_coef", "pot_coef"):
+            d[k] = d[k] * (1 + rng.integers(-4, 5, d[k].shape) * U)
     else:
         d["prim_coef"] = d["prim_coef"] * (1 - 4 * U)
         d["pot_coef"] = d["pot_coef"] * (1 + 4 * U)
@@ -116,13 +137,13 @@ def perturbed(batch: BatchArrays, mode: int) -> BatchArrays:
     return BatchArrays(**d)
 
 
-def envelope(lib, batch: BatchArrays, base=None, nthreads=8):
+def envelope(lib, batch: BatchArrays, base=None, nthreads=8, modes=(1, 2, 3, 4)):
     """Per-element sensitivity of a CPU library's result to last-bit input changes:
-    max over the two perturbations of |result(perturbed) - result|."""
+    max over the perturbations of |result(perturbed) - result|."""
     if base is None:
         base = lib.driver_full_batch(batch, nthreads=nthreads)
     env = [np.zeros_like(x) for x in base]
-    for mode in (1, 2):
+    for mode in modes:
         p = lib.driver_full_batch(perturbed(batch, mode), nthreads=nthreads)
         for m in range(4):
             env[m] = np.maximum(env[m], np.abs(p[m] - base[m]))
