@@ -125,6 +125,21 @@ int libgrpp_b200_plan_stats(const libgrpp_b200_plan_t *plan, double *ms, int64_t
 int libgrpp_b200_plan_counters(const libgrpp_b200_plan_t *plan, uint64_t *counters, int n);
 void libgrpp_b200_plan_destroy(libgrpp_b200_plan_t *plan);
 
+/* Density-contracted GRPP gradient (no counterpart in libgrpp, whose driver forms one
+ * gradient matrix per atom coordinate, test_libgrpp_c/main.c:529-620):
+ *   g[m][atom][k] += sum over tasks (A, B, C) sum_ij D[bf_off[A]+i][bf_off[B]+j] d V^m_ij / d R_atom,k
+ * for the four matrices m = arep, so_x, so_y, so_z of libgrpp_full_grpp_integrals and
+ * every atom: the same quantity as libgrpp_full_grpp_integrals_gradient contracted
+ * with D for each atom of A, B and C (the only atoms that can contribute,
+ * grpp_integrals_gradient.c:311-321). shell_atom[n_shells] and centre_atom[n_centres]
+ * map shells and centres to atoms, atom_xyz[3*n_atoms] are their positions (a shell's
+ * origin and its atom's position coincide), bf_off[n_shells] is each shell's first
+ * basis function, D is n_bf x n_bf row-major, g is [4][n_atoms][3] and is accumulated
+ * into. Shells of the tasks must have L <= 9. Returns a status code. */
+int libgrpp_b200_grpp_gradient_contract(const libgrpp_b200_batch_t *batch, int radial_mode, const int *shell_atom,
+                                        const int *centre_atom, const double *atom_xyz, int n_atoms, const int *bf_off,
+                                        int n_bf, const double *D, double *g);
+
 /* Learned grid-level model (no counterpart in libgrpp).
  *
  * libgrpp's type 2 radial quadrature (radial_type2_integral.c:242-318) doubles a

@@ -89,6 +89,8 @@ class LibGRPP:
         _F = ct.POINTER(ct.c_float)
         _B = ct.POINTER(ct.c_int8)
         self._opt("libgrpp_b200_plan_learned_stats", ct.c_int, [_V, _D, ct.POINTER(ct.c_int64)])
+        self._opt("libgrpp_b200_grpp_gradient_contract", ct.c_int,
+                  [_V, ct.c_int, _I, _I, _D, ct.c_int, _I, ct.c_int, _D, _D])
         self._opt("libgrpp_b200_set_level_model", ct.c_int, [_F])
         self._opt("libgrpp_b200_level_samples", ct.c_int, [_V, _F, _B, ct.POINTER(ct.c_int64)])
         self._opt("libgrpp_b200_mlp_grad", ct.c_int, [_F, _F, _B, ct.c_int, _F, _F])
@@ -222,6 +224,23 @@ class LibGRPP:
         if rc != 0:
             raise RuntimeError(self.last_error_message())
         return v.value
+
+    def grad_contract(self, system, batch, D, radial_mode=0):
+        """d tr(D V^m) / d R for the four matrices m over the batch's tasks: [4, n_atoms, 3]
+        (libgrpp_b200_grpp_gradient_contract; same quantity as the oracle's driver_grad_contract)."""
+        if radial_mode == 1:
+            self.ensure_level_model()
+        nat = len(system.atoms)
+        g = np.zeros((4, nat, 3))
+        sa = np.ascontiguousarray(system.shell_atom, dtype=np.int32)
+        ca = np.ascontiguousarray(system.centre_atom, dtype=np.int32)
+        xyz = np.ascontiguousarray(system.atoms, dtype=np.float64)
+        bo = np.ascontiguousarray(system.basis_offsets()[:-1], dtype=np.int32)
+        Dm = np.ascontiguousarray(D, dtype=np.float64)
+        rc = self.lib.libgrpp_b200_grpp_gradient_contract(ct.byref(batch.struct), radial_mode, _ip(sa), _ip(ca), _dp(xyz),
+                                                          nat, _ip(bo), int(Dm.shape[0]), _dp(Dm), _dp(g))
+        self._check(rc, "libgrpp_b200_grpp_gradient_contract")
+        return g
 
     # ------------------------------------------------------------ learned grid-level model
     def _check(self, rc, what):

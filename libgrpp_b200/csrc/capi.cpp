@@ -9,6 +9,7 @@
 //    makes concurrent calls on one GRPP object race); the result is the same;
 //  * misuse is reported through libgrpp_b200_last_error() with the outputs
 //    zeroed, instead of assert().
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -55,6 +56,8 @@ std::mutex g_init_mu;
 constexpr int kMaxPots = 100;  // grpp.c:12
 
 double gaussian_norm(int L, double a) { return std::pow(2 * a / M_PI, 0.75) * std::pow(4 * a, 0.5 * L); }
+
+int ncart_h(int L) { return (L + 1) * (L + 2) / 2; }
 
 // Flat batch assembled from libgrpp objects.
 struct Builder {
@@ -706,6 +709,165 @@ int libgrpp_b200_plan_counters(const libgrpp_b200_plan_t *plan, uint64_t *counte
 }
 
 void libgrpp_b200_plan_destroy(libgrpp_b200_plan_t *plan) { grpp::plan_destroy((grpp::Plan *)plan); }
+
+int libgrpp_b200_grpp_gradient_contract(const libgrpp_b200_batch_t *b, int radial_mode, const int *shell_atom,
+                                        const int *centre_atom, const double *atom_xyz, int n_atoms, const int *bf_off,
+                                        int n_bf, const double *D, double *g)
+{
+    if (!check_init()) return LIBGRPP_B200_ERR_NOT_INIT;
+    grpp::set_error(0, "");
+    auto invalid = [](const char *m) {
+        grpp::set_error(LIBGRPP_B200_ERR_INVALID, m);
+        return LIBGRPP_B200_ERR_INVALID;
+    };
+    if (!b || !shell_atom || !centre_atom || !atom_xyz || !bf_off || !D || !g || n_atoms <= 0 || n_bf <= 0)
+        return invalid("gradient contraction: null argument or empty size");
+    const int ns = b->n_shells;
+    const int kGL = grpp::kGradMaxL, Lmax_grad = kGL - 1;  // the L+1 shell must stay within the engine's limit
+    // one component order per L: the batch's own lists (must agree within an L), else the generator
+    std::vector<std::vector<int>> lists(kGL + 1);
+    for (int s = 0; s < ns; s++) {
+        const int L = b->shell_L[s];
+        if (L < 0 || L > kGL) return invalid("gradient contraction: shell angular momentum outside 0..10");
+        std::vector<int> cl(b->cart_list + 3 * b->shell_cart_off[s], b->cart_list + 3 * b->shell_cart_off[s] + 3 * ncart_h(L));
+        if (lists[L].empty()) lists[L] = cl;
+        else if (lists[L] != cl) return invalid("gradient contraction: shells of one L use different Cartesian orders");
+    }
+    for (int L = 0; L <= kGL; L++)
+        if (lists[L].empty()) {
+            lists[L].resize(3 * ncart_h(L));
+            libgrpp_params.cartesian_generator(L, lists[L].data());
+        }
+    auto find = [&](int L, int x, int y, int z) {
+        for (int i = 0; i < ncart_h(L); i++)
+            if (lists[L][3 * i] == x && lists[L][3 * i + 1] == y && lists[L][3 * i + 2] == z) return i;
+        return -1;
+    };
+    std::vector<int> tab((size_t)(kGL + 1) * grpp::kGradTabCart * 9, 0);
+    for (int L = 0; L < kGL; L++)
+        for (int i = 0; i < ncart_h(L); i++)
+            for (int k = 0; k < 3; k++) {
+                int c[3] = {lists[L][3 * i], lists[L][3 * i + 1], lists[L][3 * i + 2]};
+                int *e = tab.data() + ((L * grpp::kGradTabCart + i) * 3 + k) * 3;
+                e[0] = c[k];
+                c[k] += 1;
+                e[1] = find(L + 1, c[0], c[1], c[2]);
+                c[k] -= 2;
+                e[2] = c[k] >= 0 && L > 0 ? find(L - 1, c[0], c[1], c[2]) : -1;
+            }
+    // differentiated shells (diff_gaussian.c:35-63): L+1 with 2a N_L/N_{L+1}, L-1 with N_L/N_{L-1}
+    std::vector<int> sL(b->shell_L, b->shell_L + ns), snp(b->shell_nprim, b->shell_nprim + ns),
+        spo(b->shell_prim_off, b->shell_prim_off + ns), sco(b->shell_cart_off, b->shell_cart_off + ns);
+    int nprim_tot = 0, ncart_tot = 0;
+    for (int s = 0; s < ns; s++) {
+        nprim_tot = std::max(nprim_tot, spo[s] + snp[s]);
+        ncart_tot = std::max(ncart_tot, sco[s] + ncart_h(sL[s]));
+    }
+    std::vector<double> pc(b->prim_coef, b->prim_coef + nprim_tot), pa(b->prim_alpha, b->prim_alpha + nprim_tot),
+        so(b->shell_origin, b->shell_origin + 3 * ns);
+    std::vector<int> cart(b->cart_list, b->cart_list + 3 * ncart_tot);
+    std::vector<int> up(ns, -1), dn(ns, -1);
+    std::vector<uint8_t> used(ns, 0);
+    for (int64_t t = 0; t < b->n_tasks; t++) {
+        const int a = b->task_a[t], bb = b->task_b[t], c = b->task_c[t];
+        if (a < 0 || a >= ns || bb < 0 || bb >= ns || c < 0 || c >= b->n_centres) return invalid("task index out of range");
+        if (sL[a] > Lmax_grad || sL[bb] > Lmax_grad) return invalid("gradient contraction: shell L must be <= 9");
+        if (shell_atom[a] < 0 || shell_atom[a] >= n_atoms || shell_atom[bb] < 0 || shell_atom[bb] >= n_atoms ||
+            centre_atom[c] < 0 || centre_atom[c] >= n_atoms)
+            return invalid("gradient contraction: atom index out of range");
+        if (bf_off[a] < 0 || bf_off[a] + ncart_h(sL[a]) > n_bf || bf_off[bb] < 0 || bf_off[bb] + ncart_h(sL[bb]) > n_bf)
+            return invalid("gradient contraction: basis offset outside the density matrix");
+        used[a] = used[bb] = 1;
+    }
+    auto add_shell = [&](int s, int L, bool raise) {
+        const int idx = (int)sL.size();
+        sL.push_back(L);
+        snp.push_back(snp[s]);
+        spo.push_back((int)pc.size());
+        sco.push_back((int)cart.size() / 3);
+        for (int q = 0; q < 3 * ncart_h(L); q++) cart.push_back(lists[L][q]);
+        for (int i = 0; i < snp[s]; i++) {
+            const double al = pa[spo[s] + i];
+            const double f = raise ? 2.0 * al * gaussian_norm(sL[s], al) / gaussian_norm(L, al)
+                                   : gaussian_norm(sL[s], al) / gaussian_norm(L, al);
+            pc.push_back(pc[spo[s] + i] * f);
+            pa.push_back(al);
+        }
+        for (int d = 0; d < 3; d++) so.push_back(so[3 * s + d]);
+        return idx;
+    };
+    for (int s = 0; s < ns; s++)
+        if (used[s]) {
+            up[s] = add_shell(s, sL[s] + 1, true);
+            if (sL[s] > 0) dn[s] = add_shell(s, sL[s] - 1, false);
+        }
+    libgrpp_b200_batch_t sub = *b;
+    sub.n_shells = (int)sL.size();
+    sub.shell_L = sL.data();
+    sub.shell_nprim = snp.data();
+    sub.shell_prim_off = spo.data();
+    sub.prim_coef = pc.data();
+    sub.prim_alpha = pa.data();
+    sub.shell_origin = so.data();
+    sub.shell_cart_off = sco.data();
+    sub.cart_list = cart.data();
+    grpp::RunOptions opt;
+    opt.radial_mode = radial_mode;
+    const int64_t chunk = 16384;
+    std::vector<int> ta, tb, tc;
+    std::vector<grpp::GradTaskHost> gt;
+    std::vector<double> out24;
+    for (int64_t t0 = 0; t0 < b->n_tasks; t0 += chunk) {
+        const int64_t t1 = std::min<int64_t>(b->n_tasks, t0 + chunk);
+        ta.clear();
+        tb.clear();
+        tc.clear();
+        gt.clear();
+        auto add = [&](int x, int y, int c) {
+            ta.push_back(x);
+            tb.push_back(y);
+            tc.push_back(c);
+            return (int)ta.size() - 1;
+        };
+        for (int64_t t = t0; t < t1; t++) {
+            const int a = b->task_a[t], bb = b->task_b[t], c = b->task_c[t];
+            grpp::GradTaskHost h;
+            h.t_ad = dn[a] >= 0 ? add(dn[a], bb, c) : -1;
+            h.t_au = add(up[a], bb, c);
+            h.t_bd = dn[bb] >= 0 ? add(a, dn[bb], c) : -1;
+            h.t_bu = add(a, up[bb], c);
+            h.la = sL[a];
+            h.lb = sL[bb];
+            h.d_row = bf_off[a];
+            h.d_col = bf_off[bb];
+            gt.push_back(h);
+        }
+        sub.n_tasks = (int64_t)ta.size();
+        sub.task_a = ta.data();
+        sub.task_b = tb.data();
+        sub.task_c = tc.data();
+        out24.assign((size_t)(t1 - t0) * 24, 0.0);
+        const int rc = grpp::run_grad_contract(&sub, opt, gt.data(), t1 - t0, tab.data(), D, n_bf, out24.data());
+        if (rc) return rc;
+        // which atoms receive which side, with which sign (grpp_integrals_gradient.c:280-393)
+        for (int64_t t = t0; t < t1; t++) {
+            const int a = b->task_a[t], bb = b->task_b[t], c = b->task_c[t];
+            const double *A = b->shell_origin + 3 * a, *B = b->shell_origin + 3 * bb, *C = b->centre_origin + 3 * c;
+            const int atoms[3] = {shell_atom[a], shell_atom[bb], centre_atom[c]};
+            const double *o = out24.data() + (t - t0) * 24;
+            for (int q = 0; q < 3; q++) {
+                const int at = atoms[q];
+                if ((q > 0 && atoms[0] == at) || (q > 1 && atoms[1] == at)) continue;
+                for (const GradContribution &tcn : gradient_terms(A, B, C, atom_xyz + 3 * at)) {
+                    const int side = tcn.diff_bra ? 0 : 1;
+                    for (int k = 0; k < 3; k++)
+                        for (int m = 0; m < 4; m++) g[((size_t)m * n_atoms + at) * 3 + k] += tcn.factor * o[side * 12 + k * 4 + m];
+                }
+            }
+        }
+    }
+    return 0;
+}
 
 int libgrpp_b200_plan_learned_stats(const libgrpp_b200_plan_t *plan, double *ms_predict, int64_t *fallbacks)
 {

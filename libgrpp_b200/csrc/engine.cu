@@ -26,6 +26,7 @@
 #include "radial.cuh"
 #include "angular.cuh"
 #include "level_model.cuh"
+#include "gradient.cuh"
 #include "tables.h"
 #include "engine.h"
 
@@ -1219,6 +1220,65 @@ int mlp_predict(const float *params, const float *X, int64_t n, int8_t *pred)
     GRPP_CUDA(cudaMemcpyAsync(pred, pd, (size_t)n, cudaMemcpyDeviceToHost, s));
     GRPP_CUDA(cudaStreamSynchronize(s));
     cudaFree(pd);
+    return 0;
+}
+
+// Density-contracted gradient pieces of a task list whose GRPP blocks come from the
+// sub-task batch `sub` (the differentiated shell pairs): out24[t] = G[side][k][m] of
+// task t (gradient.cuh). cart_tab: [kMaxL+1][kGradMaxCart][3][3] component table.
+int run_grad_contract(const libgrpp_b200_batch_t *sub, const RunOptions &opt, const GradTaskHost *tasks,
+                      int64_t n_tasks, const int *cart_tab, const double *D, int64_t n_bf, double *out24)
+{
+    set_error(0, "");
+    int rc = 0;
+    DeviceState *stp = get_state(rc);
+    if (!stp) return rc;
+    std::lock_guard<std::mutex> lk(stp->mu);
+    cudaStream_t s = stp->stream;
+    Plan P;
+    rc = plan_build(*stp, sub, opt, false, P);
+    if (rc) return rc;
+    rc = plan_execute(P);
+    if (rc) return rc;
+    if (n_tasks == 0) return 0;
+    static_assert(kGradMaxL == kMaxL && kGradTabCart == kGradMaxCart, "gradient component table");
+    const size_t tab_n = (size_t)(kMaxL + 1) * kGradMaxCart * 9;
+    const size_t bytes = n_tasks * sizeof(GradTask) + tab_n * sizeof(int) + (size_t)n_bf * n_bf * sizeof(double) +
+                         (size_t)n_tasks * 24 * sizeof(double) + 4 * 256;
+    void *buf = nullptr;
+    GRPP_CUDA(cudaMalloc(&buf, bytes));
+    char *q = (char *)buf;
+    auto take = [&q](size_t n) {
+        char *r = q;
+        q += (n + 255) & ~(size_t)255;
+        return r;
+    };
+    GradTask *td = (GradTask *)take(n_tasks * sizeof(GradTask));
+    int *tabd = (int *)take(tab_n * sizeof(int));
+    double *Dd = (double *)take((size_t)n_bf * n_bf * sizeof(double));
+    double *gd = (double *)take((size_t)n_tasks * 24 * sizeof(double));
+    static_assert(sizeof(GradTask) == sizeof(GradTaskHost), "GradTask layout");
+    GRPP_CUDA(cudaMemcpyAsync(td, tasks, n_tasks * sizeof(GradTask), cudaMemcpyHostToDevice, s));
+    GRPP_CUDA(cudaMemcpyAsync(tabd, cart_tab, tab_n * sizeof(int), cudaMemcpyHostToDevice, s));
+    GRPP_CUDA(cudaMemcpyAsync(Dd, D, (size_t)n_bf * n_bf * sizeof(double), cudaMemcpyHostToDevice, s));
+    GradArgs ga{};
+    ga.tasks = td;
+    ga.n_tasks = (int)n_tasks;
+    ga.cart_tab = tabd;
+    ga.sub_off = P.fin.task_out_off;
+    for (int m = 0; m < 4; m++) ga.out[m] = P.outs[m];
+    ga.D = Dd;
+    ga.n_bf = n_bf;
+    ga.g = gd;
+    grad_contract_kernel<<<(int)std::min<int64_t>((n_tasks + 3) / 4, 148 * 32), 128, 0, s>>>(ga);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out24, gd, (size_t)n_tasks * 24 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(buf);
+    if (e != cudaSuccess) {
+        set_error(LIBGRPP_B200_ERR_CUDA, std::string("gradient contraction: ") + cudaGetErrorString(e));
+        return LIBGRPP_B200_ERR_CUDA;
+    }
     return 0;
 }
 

@@ -43,6 +43,17 @@ int64_t plan_h2d_bytes(const Plan *P);
 int set_device(int device);
 int measure_fp64_peak(double *tflops);
 
+// density-contracted gradient (gradient.cuh): one entry per task of the original list
+struct GradTaskHost {
+    int t_ad, t_au, t_bd, t_bu;  // sub-task indices of (A-1,B) (A+1,B) (A,B-1) (A,B+1); -1 if L = 0
+    int la, lb;
+    int64_t d_row, d_col;        // basis offsets of shells A and B
+};
+constexpr int kGradMaxL = 10;      // component table rows L = 0..10 (the engine's kMaxL)
+constexpr int kGradTabCart = 66;   // components of L = 10
+int run_grad_contract(const libgrpp_b200_batch_t *sub, const RunOptions &opt, const GradTaskHost *tasks,
+                      int64_t n_tasks, const int *cart_tab, const double *D, int64_t n_bf, double *out24);
+
 // learned grid-level model (level_model.cuh)
 int set_level_model(const float *params);
 int level_samples(const libgrpp_b200_batch_t *b, float *features, int8_t *levels, int64_t *n_items);

@@ -17,7 +17,7 @@ the reference's per-task blocks (``ref_arep`` ... ``ref_so_z``) and their
 sensitivity to last-bit input changes (``env_*``: the largest change of each
 element when the reference is re-run with exponents, coefficients and
 coordinates moved by up to 4 units of roundoff: uniformly scaled, and
-independently per primitive with a seeded random draw, tests/util.py
+independently per primitive in eight seeded random draws, tests/util.py
 ``perturbed``). H2O and Cs
 hold every task; ThO, UO2 and KCs hold a seeded sample of shell pairs x all
 centres (the full matrices are tens of MB). H2O also holds libgrpp's
@@ -29,7 +29,13 @@ benchmarked on (libgrpp_b200.synthetic): config1.npz, 512 seeded tasks of the
 config-1 task list (64 atoms, s..g shells, U_L + projectors l = 0..4), and
 config2.npz, 384 seeded tasks of config 2 (full GRPP: U_L, projectors,
 spin-orbit and outercore terms, basis up to h). Their reference values and
-envelopes come from the same compiled libgrpp.
+envelopes come from the same compiled libgrpp. config3.npz pins the
+density-contracted gradient d tr(D V)/dR on a seeded task sample of a small
+config-2-type system (3 heavy atoms + 3 H, basis up to f) with a random
+symmetric D; its reference is the oracle's driver over the restated
+libgrpp_full_grpp_integrals_gradient (pinned against libgrpp's 36 shipped H2O
+gradient matrices), because the compiled libgrpp gradient reads past its L-1
+block and can return NaN (grpp_integrals_gradient.c:452-466).
 """
 from __future__ import annotations
 
@@ -118,6 +124,30 @@ def make_synthetic(lib, name):
           f"{n_ill} elements move by more than 1e-10 under 4-ulp input changes")
 
 
+def make_gradient_fixture(n_tasks=160, seed=13):
+    from tests.util import grad_envelope, load_oracle
+    orc = load_oracle()
+    system = synthetic.config2(seed=3, n_heavy=3, n_h=3, lmax=3, box=8.0)
+    D = synthetic.config3_density(system, seed=3)
+    a, b, c = system.all_tasks()
+    sel = np.sort(np.random.default_rng(seed).choice(len(a), n_tasks, replace=False))
+    a, b, c = a[sel], b[sel], c[sel]
+    batch = system.batch(a, b, c)
+    g, env = grad_envelope(orc, system, batch, D)
+    assert np.all(np.isfinite(g))
+    out = os.path.join(HERE, "config3.npz")
+    data = dict(batch_arrays(batch))
+    data.update(task_a=a, task_b=b, task_c=c, n_basis=system.n_basis(), basis_offsets=system.basis_offsets(),
+                cart_order=system.cart_order, atoms=system.atoms, shell_atom=system.shell_atom,
+                centre_atom=system.centre_atom, D=D, ref_grad=g, env_grad=env)
+    for comp in COMPS:  # no per-task blocks in this fixture
+        data["ref_" + comp] = np.zeros(0)
+        data["env_" + comp] = np.zeros(0)
+    np.savez_compressed(out, **data)
+    print(f"config3: {len(a)} tasks, gradient [4, {len(system.atoms)}, 3] -> {os.path.relpath(out, ROOT)} "
+          f"({os.path.getsize(out) / 1e3:.0f} kB); max |g| {np.abs(g).max():.3e}, max env {env.max():.3e}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default="/root/reference")
@@ -129,6 +159,8 @@ def main():
         if args.only and name not in args.only:
             continue
         make_synthetic(lib, name)
+    if not args.only or "config3" in args.only:
+        make_gradient_fixture()
     for name, (full, tol) in FIXTURES.items():
         if args.only and name not in args.only:
             continue

@@ -116,7 +116,7 @@ def perturbed(batch: BatchArrays, mode: int) -> BatchArrays:
     """The same workload with inputs moved by a few units in the last place:
     mode 1 scales every exponent by (1 + 4u); mode 2 scales contraction and
     potential coefficients by (1 - 4u), (1 + 4u) and every coordinate by (1 + 4u)
-    (coincident centres stay coincident); modes 3 and 4 move every exponent and
+    (coincident centres stay coincident); modes 3 and above move every exponent and
     coefficient independently by a seeded random whole number of units in [-4, 4]
     (a uniform scaling can leave a cancelling sum's rounding pattern unchanged,
     independent changes do not)."""
@@ -125,7 +125,7 @@ def perturbed(batch: BatchArrays, mode: int) -> BatchArrays:
     if mode == 1:
         d["prim_alpha"] = d["prim_alpha"] * (1 + 4 * U)
         d["pot_alpha"] = d["pot_alpha"] * (1 + 4 * U)
-    elif mode in (3, 4):
+    elif mode >= 3:
         rng = np.random.default_rng(mode)
         for k in ("prim_alpha", "pot_alpha", "prim_coef", "pot_coef"):
             d[k] = d[k] * (1 + rng.integers(-4, 5, d[k].shape) * U)
@@ -137,7 +137,10 @@ def perturbed(batch: BatchArrays, mode: int) -> BatchArrays:
     return BatchArrays(**d)
 
 
-def envelope(lib, batch: BatchArrays, base=None, nthreads=8, modes=(1, 2, 3, 4)):
+ENV_MODES = (1, 2) + tuple(range(3, 11))  # two uniform and eight independent random perturbations
+
+
+def envelope(lib, batch: BatchArrays, base=None, nthreads=8, modes=ENV_MODES):
     """Per-element sensitivity of a CPU library's result to last-bit input changes:
     max over the perturbations of |result(perturbed) - result|."""
     if base is None:
@@ -165,3 +168,19 @@ def parity(got, want, env=None, abs_tol=1e-10, rel_tol=1e-9, env_factor=4.0):
     max_rel = float(np.max(err[big] / np.abs(want[big]))) if big.any() else 0.0
     n_env = int(np.sum(~strict_ok & (err <= tol)))
     return ok, float(err.max()) if err.size else 0.0, max_rel, n_env
+
+
+def grad_envelope(lib, system, batch, D, nthreads=8, modes=ENV_MODES):
+    """The oracle's density-contracted gradient and its sensitivity to last-bit input
+    changes (the perturbations of ``perturbed``; coordinates of atoms move with the
+    shells and centres in mode 2)."""
+    import copy
+    base = lib.driver_grad_contract(system, batch, D, nthreads=nthreads)
+    env = np.zeros_like(base)
+    for mode in modes:
+        sp = copy.copy(system)
+        if mode == 2:
+            sp.atoms = np.asarray(system.atoms) * (1 + 4 * U)
+        g = lib.driver_grad_contract(sp, perturbed(batch, mode), D, nthreads=nthreads)
+        env = np.maximum(env, np.abs(g - base))
+    return base, env
