@@ -347,6 +347,115 @@ def roofline(kernel_ms, counters, peak_tflops):
     return out
 
 
+def config4_tasks(n_mol):
+    from libgrpp_b200 import synthetic
+    M, (a, b, c) = synthetic.merge_systems(synthetic.config4()[:n_mol])
+    return M, a, b, c
+
+
+def run_config4(args, rank, world, local):
+    """Uneven batch: the first --molecules molecules of config 4 (2..24 atoms each, full
+    GRPP, basis l <= 6, projectors l <= 5) as one class-sorted task list, run as chunks of
+    65536 tasks; a step is one pass over all chunks, learned and plain timed alike."""
+    import torch
+    from libgrpp_b200 import engine
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    lib = engine.load()
+    M, a, b, c = config4_tasks(args.molecules)
+    chunks = [M.batch(a[i:i + 65536], b[i:i + 65536], c[i:i + 65536]) for i in range(0, len(a), 65536)]
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    res, outs = {}, {}
+    for name, mode in (("plain", 0), ("learned", 1)):
+        plans = [lib.plan(ch, mode) for ch in chunks]
+        for p in plans[: max(1, args.warmup)]:
+            p.execute()
+        tot = 0.0
+        fb = 0
+        with ClockSampler(local) as clk:
+            for _ in range(args.steps):
+                for p in plans:
+                    flush.fill_(1.0)
+                    torch.cuda.synchronize()
+                    p.execute()
+                    tot += p.stats()["ms_total"]
+                    fb += p.learned_stats()["fallbacks"]
+        outs[name] = [np.concatenate([p.outputs()[m] for p in plans]) for m in range(4)]
+        res[name] = {"value": args.steps * len(a) / (tot / 1e3), "ms_per_step": tot / args.steps,
+                     "fallbacks_per_step": fb / args.steps, "clocks": clk.summary()}
+        for p in plans:
+            p.close()
+    max_err = max(float(np.max(np.abs(x - y))) for x, y in zip(outs["learned"], outs["plain"]))
+    line = {"metric": METRIC, "value": res["learned"]["value"], "unit": "tasks/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["learned"]["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config 4)",
+            "config": {"workload": f"config4: first {args.molecules} of 512 molecules (2..24 atoms, full GRPP, l <= 6), "
+                                   f"{len(a)} tasks sorted by (la, lb, lpot), {len(chunks)} chunks of 65536",
+                       "l2": "flushed before every chunk"},
+            "plain": res["plain"], "learned_over_plain": res["learned"]["value"] / res["plain"]["value"],
+            "learned_fallback_rate": res["learned"]["fallbacks_per_step"] / len(a),
+            "max_abs_diff_learned_vs_plain": max_err, "clocks": res["learned"]["clocks"]}
+    if not args.no_cpu_baseline:
+        from libgrpp_b200.capi import LibGRPP
+        ref = LibGRPP(os.path.join(ROOT, "oracle", "_ref", "libgrpp_ref.so"))
+        sel = np.sort(np.random.default_rng(0).choice(len(a), args.ref_sample, replace=False))
+        threads = host_threads()
+        t0 = time.perf_counter()
+        ref.driver_full_batch(M.batch(a[sel], b[sel], c[sel]), nthreads=threads)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": args.ref_sample / dt, "unit": "tasks/s", "cores": threads, "kind": "reference",
+                                "sample": f"{args.ref_sample} seeded random tasks of the batch ({dt:.1f} s)"}
+    print(json.dumps(line), flush=True)
+
+
+def run_config3(args, rank, world, local):
+    """Density-contracted gradient d tr(D V)/dR (all four matrices, all atoms) of the
+    config-2 system (16 heavy atoms + 32 H, basis up to h) with a random symmetric D,
+    over its first --tasks class-sorted tasks (shell pair x centre)."""
+    import torch
+    from libgrpp_b200 import engine, synthetic
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    lib = engine.load()
+    S = synthetic.config2()
+    D = synthetic.config3_density(S)
+    a, b, c = synthetic.sort_tasks(S, *S.all_tasks())
+    n = min(args.tasks, len(a))
+    batch = S.batch(a[:n], b[:n], c[:n])
+    res = {}
+    for name, mode in (("plain", 0), ("learned", 1)):
+        lib.grad_contract(S, S.batch(a[:512], b[:512], c[:512]), D, radial_mode=mode)
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            g = lib.grad_contract(S, batch, D, radial_mode=mode)
+            times.append(time.perf_counter() - t0)
+        dt = float(np.median(times))  # wall clock of a host-in/host-out call: the median of the steps
+        res[name] = {"value": n / dt, "seconds_per_step": dt, "seconds_all_steps": times,
+                     "max_abs_grad": float(np.abs(g).max())}
+    line = {"metric": "shell-pair x RPP-centre gradient tasks/s (d tr(D V)/dR, 4 matrices, FP64)",
+            "value": res["learned"]["value"], "unit": "tasks/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "ms_per_step": 1e3 * res["learned"]["seconds_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config 2 system, D seed 3)",
+            "config": {"workload": f"config3: first {n} of {len(a)} class-sorted tasks of config 2, host in / host out "
+                                   "(libgrpp_b200_grpp_gradient_contract, wall clock)"},
+            "plain": res["plain"], "learned_over_plain": res["learned"]["value"] / res["plain"]["value"]}
+    if not args.no_cpu_baseline:
+        from libgrpp_b200.capi import LibGRPP
+        ref = LibGRPP(os.path.join(ROOT, "oracle", "_build", "libgrpp_oracle.so"))
+        sel = np.sort(np.random.default_rng(0).choice(n, args.ref_sample, replace=False))
+        threads = host_threads()
+        t0 = time.perf_counter()
+        ref.driver_grad_contract(S, S.batch(a[sel], b[sel], c[sel]), D, nthreads=threads)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": args.ref_sample / dt, "unit": "tasks/s", "cores": threads, "kind": "port",
+                                "sample": f"{args.ref_sample} seeded random tasks, the oracle's restated "
+                                          f"libgrpp_full_grpp_integrals_gradient per atom ({dt:.1f} s)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -360,10 +469,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tasks-per-step", type=int, default=0,
                     help="evenly spaced subset of each step's tasks (profiling runs); 0 = the full block")
+    ap.add_argument("--workload", choices=["config1", "config3", "config4"], default="config1",
+                    help="config1 (default, the headline), config3 (density-contracted gradient), "
+                         "config4 (uneven multi-molecule batch)")
+    ap.add_argument("--molecules", type=int, default=16, help="config4: molecules in the batch")
+    ap.add_argument("--tasks", type=int, default=65536, help="config3: tasks differentiated")
     args = ap.parse_args()
     rank, world, local = get_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.workload == "config4":
+        run_config4(args, rank, world, local)
+    elif args.workload == "config3":
+        run_config3(args, rank, world, local)
     else:
         run_ours(args, rank, world, local)
 

@@ -876,6 +876,11 @@ int plan_download(Plan &P, double *h_arep, double *h_sx, double *h_sy, double *h
     return 0;
 }
 
+// Large batches run as consecutive chunks of tasks whose radial tables together stay
+// below kChunkEntries entries (24 bytes of device scratch each) and kChunkTasks tasks;
+// outputs land at each chunk's offset in the caller's arrays.
+constexpr int64_t kChunkEntries = int64_t(1) << 27, kChunkTasks = int64_t(1) << 20;
+
 int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double *h_arep, double *h_sx, double *h_sy,
                    double *h_sz, RunStats *stats)
 {
@@ -884,13 +889,60 @@ int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double 
     DeviceState *stp = get_state(rc);
     if (!stp) return rc;
     std::lock_guard<std::mutex> lk(stp->mu);
-    Plan P;
-    rc = plan_build(*stp, b, opt, false, P);
-    if (rc) return rc;
-    rc = plan_execute(P);
-    if (rc) return rc;
-    rc = plan_download(P, h_arep, h_sx, h_sy, h_sz);
-    if (stats) *stats = P.stats;
+    for (int64_t t = 0; t < b->n_tasks; t++)
+        CHECK_INPUT(b->task_a[t] >= 0 && b->task_a[t] < b->n_shells && b->task_b[t] >= 0 && b->task_b[t] < b->n_shells &&
+                        b->task_c[t] >= 0 && b->task_c[t] < b->n_centres,
+                    "task index out of range");
+    for (int c = 0; c < b->n_centres; c++) CHECK_INPUT(b->centre_grpp[c] >= 0 && b->centre_grpp[c] < b->n_grpps, "centre GRPP index out of range");
+    for (int g = 0; g < b->n_grpps; g++) {
+        CHECK_INPUT(b->grpp_n_arep[g] >= 0 && b->grpp_n_so[g] >= 0, "negative potential count in a GRPP");
+        for (int q = 0; q < b->grpp_n_arep[g]; q++) {
+            const int pot = b->grpp_pot_list[b->grpp_arep_off[g] + q];
+            CHECK_INPUT(pot >= 0 && pot < b->n_pots, "GRPP potential index out of range");
+        }
+        for (int q = 0; q < b->grpp_n_so[g]; q++) {
+            const int pot = b->grpp_pot_list[b->grpp_so_off[g] + q];
+            CHECK_INPUT(pot >= 0 && pot < b->n_pots, "GRPP potential index out of range");
+        }
+    }
+    // radial entries of a task: sum over the centre's semilocal potentials of (L+la+1)(L+lb+1)(la+lb+1)
+    RunStats total;
+    int64_t t0 = 0, out0 = 0;
+    while (t0 < b->n_tasks || (t0 == 0 && b->n_tasks == 0)) {
+        int64_t t1 = t0, ent = 0;
+        while (t1 < b->n_tasks && t1 - t0 < kChunkTasks) {
+            const int la = b->shell_L[b->task_a[t1]], lb = b->shell_L[b->task_b[t1]], g = b->centre_grpp[b->task_c[t1]];
+            int64_t e = 0;
+            for (int q = 0; q < b->grpp_n_arep[g] + b->grpp_n_so[g]; q++) {
+                const int pot = q < b->grpp_n_arep[g] ? b->grpp_pot_list[b->grpp_arep_off[g] + q]
+                                                      : b->grpp_pot_list[b->grpp_so_off[g] + q - b->grpp_n_arep[g]];
+                const int L = b->pot_L[pot];
+                e += (int64_t)(L + la + 1) * (L + lb + 1) * (la + lb + 1);
+            }
+            if (t1 > t0 && ent + e > kChunkEntries) break;
+            ent += e;
+            t1++;
+        }
+        libgrpp_b200_batch_t v = *b;
+        v.n_tasks = t1 - t0;
+        v.task_a = b->task_a + t0;
+        v.task_b = b->task_b + t0;
+        v.task_c = b->task_c + t0;
+        Plan P;
+        rc = plan_build(*stp, &v, opt, false, P);
+        if (rc) return rc;
+        rc = plan_execute(P);
+        if (rc) return rc;
+        rc = plan_download(P, h_arep ? h_arep + out0 : nullptr, h_sx ? h_sx + out0 : nullptr,
+                           h_sy ? h_sy + out0 : nullptr, h_sz ? h_sz + out0 : nullptr);
+        if (rc) return rc;
+        out0 += P.out_tot;
+        total.n_tasks += P.stats.n_tasks;
+        total.ms_total += P.stats.ms_total;
+        if (b->n_tasks == 0) break;
+        t0 = t1;
+    }
+    if (stats) *stats = total;
     return rc;
 }
 

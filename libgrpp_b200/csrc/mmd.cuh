@@ -56,7 +56,18 @@ __host__ __device__ inline int mmd_r_size(int smax)
     for (int s = 0; s <= smax; s++) tot += (s + 1) * (s + 2) / 2 * (smax - s + 1);
     return tot;
 }
-__host__ __device__ inline int mmd_ws_size(int lmax, int smax) { return mmd_e_size(lmax) + mmd_r_size(smax) + 2 * (smax + 2) + 16; }
+// R^0_tuv (t+u+v <= S) in rows (t, u) of consecutive v: tet(S) = (S+1)(S+2)(S+3)/6 values
+__host__ __device__ inline int mmd_tet(int m) { return (m + 1) * (m + 2) * (m + 3) / 6; }
+__host__ __device__ inline int mmd_ws_size(int lmax, int smax)
+{
+    return mmd_e_size(lmax) + mmd_r_size(smax) + mmd_tet(smax) + 2 * (smax + 2) + 16;
+}
+
+// start of row (t, u) in the R^0 layout: rows ordered t-major, then u
+__device__ __forceinline__ int r0_row(int S, int t, int u)
+{
+    return mmd_tet(S) - mmd_tet(S - t) + u * (S - t + 1) - u * (u - 1) / 2;
+}
 
 constexpr int kMmdMaxPairsPerLane = 32;  // up to 1024 Cartesian pairs per pass (KPL = 32 variant)
 
@@ -86,7 +97,8 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
     const int ws = mmd_ws_size(a.lmax, a.smax);
     double *E = smem + warp * ws;
     double *R = E + mmd_e_size(a.lmax);
-    double *aux = R + mmd_r_size(a.smax);
+    double *R0 = R + mmd_r_size(a.smax);
+    double *aux = R0 + mmd_tet(a.smax);
     int *lvl = (int *)(aux + (a.smax + 2));
 
     for (int it = blockIdx.x * wpb + warp; it < a.n_items; it += gridDim.x * wpb) {
@@ -192,6 +204,7 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                 const bool isg = npow == 0;
                                 const double q2 = isg ? 2.0 * q : -2.0 * q;
                                 if (lane <= S) R[lane] = pow(q2, lane) * aux[lane];  // level 0: n = 0..S
+                                if (lane == 0) R0[0] = R[0];
                                 __syncwarp();
                                 for (int s = 1; s <= S; s++) {
                                     const int ne = (s + 1) * (s + 2) / 2, nn = S - s + 1, tot = ne * nn;
@@ -224,6 +237,7 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                         if (isg) val += X * (r1n1 - 2.0 * q * r1n);
                                         else val += X * r1n1;
                                         R[o + n * ne + idx] = val;
+                                        if (n == 0) R0[r0_row(S, t, u) + v] = val;
                                     }
                                     __syncwarp();
                                 }
@@ -243,14 +257,14 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                           E[eidx(lb1, S1, 2, az, bz, 0, la1)] * pow(kPi / q, 1.5);
                                 } else {
                                     double s = 0.0;
+                                    const double *ez = E + eidx(lb1, S1, 2, az, bz, 0, la1);
+                                    const int vz = az + bz;
                                     for (int t = 0; t <= ax + bx; t++) {
                                         const double ex = E[eidx(lb1, S1, 0, ax, bx, t, la1)];
                                         for (int u = 0; u <= ay + by; u++) {
-                                            const double ey = E[eidx(lb1, S1, 1, ay, by, u, la1)];
-                                            for (int v = 0; v <= az + bz; v++) {
-                                                const double ez = E[eidx(lb1, S1, 2, az, bz, v, la1)];
-                                                s += ex * ey * ez * R[lvl[t + u + v] + r_in_level(u, v)];
-                                            }
+                                            const double exy = ex * E[eidx(lb1, S1, 1, ay, by, u, la1)];
+                                            const double *r0 = R0 + r0_row(S, t, u);
+                                            for (int v = 0; v <= vz; v++) s += exy * ez[v] * r0[v];
                                         }
                                     }
                                     buf = s * pref;

@@ -150,3 +150,27 @@ def sort_tasks(system: System, a, b, c):
     key = (La[a] * 16 + La[b]) * 16 + lpot[cg[c]]
     o = np.lexsort((c, b, a, key))
     return a[o], b[o], c[o]
+
+
+def merge_systems(systems):
+    """One System holding independent molecules side by side (shells, GRPPs, centres and
+    atoms concatenated; all must share one Cartesian order), and its task list: every
+    ordered shell pair x centre within each molecule, sorted by class (la, lb, lpot)."""
+    shells, grpps, centres, shell_atom, centre_atom, atoms = [], [], [], [], [], []
+    ta, tb, tc = [], [], []
+    for S in systems:
+        s0, g0, c0, a0 = len(shells), len(grpps), len(centres), len(atoms)
+        shells += list(S.shells)
+        grpps += list(S.grpps)
+        centres += [(o, gi + g0) for o, gi in S.centres]
+        shell_atom.append(np.asarray(S.shell_atom) + a0)
+        centre_atom.append(np.asarray(S.centre_atom) + a0)
+        atoms += list(np.asarray(S.atoms))
+        a, b, c = S.all_tasks()
+        ta.append(a + s0)
+        tb.append(b + s0)
+        tc.append(c + c0)
+    M = System(shells, grpps, centres, systems[0].cart_order, np.concatenate(shell_atom).astype(np.int32),
+               np.concatenate(centre_atom).astype(np.int32), np.array(atoms))
+    a, b, c = sort_tasks(M, np.concatenate(ta), np.concatenate(tb), np.concatenate(tc))
+    return M, (a.astype(np.int32), b.astype(np.int32), c.astype(np.int32))

@@ -106,3 +106,20 @@ def test_h2o_gradients(gpu_lib):
     got = G[:, :, :, tri[0], tri[1]]
     ok, ab, rel, _ = parity(got.ravel(), z["ref_grad_lower"].ravel())
     assert ok, (ab, rel)
+
+
+def test_large_batch_runs_in_chunks(gpu_lib):
+    """A batch whose radial tables exceed one chunk (2^27 entries) through the batched
+    entry point, which splits it, equals the same tasks run as one plan."""
+    S = synthetic.config1()
+    a, b, c = S.all_tasks()
+    La = np.array([s.L for s in S.shells])
+    gg = np.where((La[a] == 4) & (La[b] == 4))[0][:80000]  # 2295 entries per g x g task
+    batch = S.batch(a[gg], b[gg], c[gg])
+    chunked = gpu_lib.full_grpp_batch(batch)
+    plan = gpu_lib.plan(batch, 0)
+    plan.execute()
+    whole = plan.outputs()
+    plan.close()
+    for x, y in zip(chunked, whole):
+        assert np.array_equal(x, y)
