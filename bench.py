@@ -172,6 +172,26 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def rank_blocks(rank: int, world: int, steps: int, n_blocks: int = 100):
+    """Block pairs (of the config-1 task list) that rank `rank` of `world` runs in its
+    `steps` steps: r, r + N, r + 2N, ... mod n_blocks; ranks never share a block while
+    steps * world <= n_blocks."""
+    return [(rank + world * s) % n_blocks for s in range(steps)]
+
+
+def reduce_time_and_work(dist, elapsed, work, device):
+    """(max over ranks of elapsed, sum over ranks of work): the job's time is the slowest
+    rank's, its work everyone's. dist is torch.distributed (None on one rank)."""
+    if dist is None:
+        return float(elapsed), float(work)
+    import torch
+    t = torch.tensor([elapsed, work], dtype=torch.float64, device=device)
+    tmax = t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(tmax[0]), float(t[1])
+
+
 def time_plans(plans, flush, local):
     """Execute each plan once (L2 flushed before each); per-kernel ms summed, counters summed."""
     import torch
@@ -211,7 +231,7 @@ def run_ours(args, rank, world, local):
     lib.set_device(local)
     modes = {"plain": 0, "learned": 1}
 
-    idxs = [(rank + world * s) % 100 for s in range(args.steps)]
+    idxs = rank_blocks(rank, world, args.steps)
     S = system()
     batches = []
     for i in idxs:
@@ -231,13 +251,7 @@ def run_ours(args, rank, world, local):
             dist.barrier()
         torch.cuda.synchronize()
         total_ms, kms, cnt, fallbacks, clocks = time_plans(plans, flush, local)
-        tasks = float(sum(n_tasks))
-        if dist is not None:
-            t = torch.tensor([total_ms, tasks], dtype=torch.float64, device="cuda")
-            tmax = t.clone()
-            dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-            dist.all_reduce(t, op=dist.ReduceOp.SUM)
-            total_ms, tasks = float(tmax[0]), float(t[1])
+        total_ms, tasks = reduce_time_and_work(dist, total_ms, float(sum(n_tasks)), "cuda")
         st0 = plans[0].stats()
         res[name] = {"value": tasks / (total_ms / 1e3), "ms_per_step": total_ms / len(plans),
                      "kernel_ms_per_step": {k: v / len(plans) for k, v in kms.items()},
@@ -260,13 +274,7 @@ def run_ours(args, rank, world, local):
     for b in e2e_batches:
         lib.full_grpp_batch(b, modes[main_mode])
     e2e_s = time.perf_counter() - t0
-    e2e_tasks = float(sum(len(b.task_a) for b in e2e_batches))
-    if dist is not None:
-        t = torch.tensor([e2e_s, e2e_tasks], dtype=torch.float64, device="cuda")
-        tm = t.clone()
-        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        e2e_s, e2e_tasks = float(tm[0]), float(t[1])
+    e2e_s, e2e_tasks = reduce_time_and_work(dist, e2e_s, float(sum(len(b.task_a) for b in e2e_batches)), "cuda")
     d2h = 4 * 8 * int(batches[0].block_offsets()[-1])
 
     line = {
