@@ -192,18 +192,24 @@ __device__ __forceinline__ double ipow(double x, int n)
     return r;
 }
 
-// M_a(x) / M_b(x) with (a, b) = (1, 0) if l = 0, else (l-1, l) (screening.c:329-346)
-__device__ __forceinline__ double scr_ratio_inl(int l, double x)
+// M_a(x) and M_b(x) with (a, b) = (1, 0) if l = 0, else (l-1, l) (screening.c:329-346):
+// the numerator and denominator of the ratio the fixed-point step uses
+__device__ __forceinline__ void scr_ratio_parts(int l, double x, double &num, double &den)
 {
     const int na = l == 0 ? 1 : l - 1, nb = l == 0 ? 0 : l;
-    if (x <= 1e-7) return bessel_small(na, x) / bessel_small(nb, x);
-    if (x <= 16.0) {
+    if (x <= 1e-7) {
+        num = bessel_small(na, x);
+        den = bessel_small(nb, x);
+    } else if (x <= 16.0) {
         const int i0 = (int)(round(x * 100) + 1e-5);
         const double dx = x - i0 * 0.01;
         const double *row = c_tab.bessel + (size_t)i0 * kBesL * 5;
-        return taylor4(row + 5 * na, dx) / taylor4(row + 5 * nb, dx);
+        num = taylor4(row + 5 * na, dx);
+        den = taylor4(row + 5 * nb, dx);
+    } else {
+        num = bessel_asym(na, x);
+        den = bessel_asym(nb, x);
     }
-    return bessel_asym(na, x) / bessel_asym(nb, x);
 }
 
 // Primitive screening estimate (screening.c:243-318) with CA, CB as distances.
@@ -231,8 +237,10 @@ __device__ __forceinline__ bool scr_prim_flat(int l1, int l2, int n, double CA, 
         *val = exp(-aA * CA * CA - aB * CB * CB) * gi;
         return false;
     }
-    const double inv2p = 1.0 / (2.0 * p);
-    double r0 = (aA * CA + aB * CB) / p, r0p;
+    // one reciprocal of p serves the start point, the fixed-point step and the envelope
+    // (libgrpp divides by p three times; the estimate only feeds threshold tests)
+    const double inv_p = 1.0 / p, inv2p = 0.5 * inv_p;
+    double r0 = (aA * CA + aB * CB) * inv_p, r0p;
     int steps = 0;
     do {
         steps++;
@@ -242,14 +250,18 @@ __device__ __forceinline__ bool scr_prim_flat(int l1, int l2, int n, double CA, 
         }
         r0p = r0;
         const double x1 = k1 * r0, x2 = k2 * r0;
-        double s = scr_ratio_inl(l1, x1) * x1 + scr_ratio_inl(l2, x2) * x2 + n;
+        double n1, d1, n2, d2;
+        scr_ratio_parts(l1, x1, n1, d1);
+        scr_ratio_parts(l2, x2, n2, d2);
+        // M_a1/M_b1 x1 + M_a2/M_b2 x2 over one common denominator
+        double s = (n1 * x1 * d2 + n2 * x2 * d1) / (d1 * d2) + n;
         if (l1 > 0) s = s - l1 - 1;
         if (l2 > 0) s = s - l2 - 1;
         r0 = sqrt(s * inv2p);
     } while (fabs(r0 - r0p) > 1e-2);
-    const double d1 = r0 - CA, d2 = r0 - CB;
-    *val = sqrt(kPi / p) * ipow(r0, n) * bessel_scaled(l1, k1 * r0) * bessel_scaled(l2, k2 * r0) *
-           exp(-eta * r0 * r0 - aA * d1 * d1 - aB * d2 * d2) * 0.5 * (1 + erf(sqrt(p) * r0));
+    const double e1 = r0 - CA, e2 = r0 - CB;
+    *val = sqrt(kPi * inv_p) * ipow(r0, n) * bessel_scaled(l1, k1 * r0) * bessel_scaled(l2, k2 * r0) *
+           exp(-eta * r0 * r0 - aA * e1 * e1 - aB * e2 * e2) * 0.5 * (1 + erf(sqrt(p) * r0));
     *iters = -steps - 1;
     return false;
 }
