@@ -56,11 +56,14 @@ __host__ __device__ inline int mmd_r_size(int smax)
     for (int s = 0; s <= smax; s++) tot += (s + 1) * (s + 2) / 2 * (smax - s + 1);
     return tot;
 }
+constexpr int kMmdMaxPrims = 64;     // primitives per shell (the engine's limit)
+constexpr double kPi15 = 5.568327996831708;  // pi^(3/2), correctly rounded
+
 // R^0_tuv (t+u+v <= S) in rows (t, u) of consecutive v: tet(S) = (S+1)(S+2)(S+3)/6 values
 __host__ __device__ inline int mmd_tet(int m) { return (m + 1) * (m + 2) * (m + 3) / 6; }
 __host__ __device__ inline int mmd_ws_size(int lmax, int smax)
 {
-    return mmd_e_size(lmax) + mmd_r_size(smax) + mmd_tet(smax) + 2 * (smax + 2) + 16;
+    return mmd_e_size(lmax) + mmd_r_size(smax) + mmd_tet(smax) + 2 * (smax + 2) + 16 + 2 * kMmdMaxPrims;
 }
 
 // start of row (t, u) in the R^0 layout: rows ordered t-major, then u
@@ -100,6 +103,7 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
     double *R0 = R + mmd_r_size(a.smax);
     double *aux = R0 + mmd_tet(a.smax);
     int *lvl = (int *)(aux + (a.smax + 2));
+    double *normA = aux + 2 * (a.smax + 2) + 16, *normB = normA + kMmdMaxPrims;  // per item
 
     for (int it = blockIdx.x * wpb + warp; it < a.n_items; it += gridDim.x * wpb) {
         const MmdItem item = a.items[it];
@@ -119,7 +123,7 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
         const int nterms = overlap ? 1 : a.pot_nprim[item.pot];
         double *out = a.out[item.out_kind] + item.out_off;
 
-        __syncwarp();  // the previous item's readers of lvl are done
+        __syncwarp();  // the previous item's readers of lvl and the norms are done
         if (lane == 0) {
             int o = 0;
             for (int s = 0; s <= S; s++) {
@@ -127,6 +131,9 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                 o += (s + 1) * (s + 2) / 2 * (S - s + 1);
             }
         }
+        // primitive norms depend on (shell, primitive) only: once per item, one per lane
+        for (int q = lane; q < npA; q += 32) normA[q] = gaussian_norm(la, xA[q]);
+        for (int q = lane; q < npB; q += 32) normB[q] = gaussian_norm(lb, xB[q]);
         __syncwarp();
 
         const int npairs = nA * nB;
@@ -149,19 +156,34 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                         const double cj = cB[j];
                         if (fabs(cj) < kZeroThresh && !overlap) continue;
                         const double al = xA[i], be = xB[j];
-                        const double NA = gaussian_norm(la, al), NB = gaussian_norm(lb, be);
+                        const double NA = normA[i], NB = normB[j];
                         double pref;
                         if (!overlap) {
                             // ---- Hermite E by wavefronts (type1_mcmurchie_davidson.c:569-622)
                             const double q = al + be + zeta;
-                            const double muab = al * be / q, muac = al * zeta / q, mubc = be * zeta / q;
+                            // the same scalars as every lane computing them, one per lane:
+                            // lanes 0-2 the three mu, lanes 3-5 Q[x,y,z]; then lanes 0-8 the nine
+                            // exponentials, K[d] = e(d,ab) e(d,ac) e(d,bc) in that order
+                            double sc = 0.0;
+                            if (lane < 3) sc = (lane == 0 ? al * be : (lane == 1 ? al * zeta : be * zeta)) / q;
+                            else if (lane < 6) sc = (al * A[lane - 3] + be * B[lane - 3] + zeta * C[lane - 3]) / q;
+                            const double muab = __shfl_sync(0xffffffffu, sc, 0), muac = __shfl_sync(0xffffffffu, sc, 1),
+                                         mubc = __shfl_sync(0xffffffffu, sc, 2);
                             double Q[3], K[3];
-#pragma unroll
-                            for (int d = 0; d < 3; d++) {
-                                Q[d] = (al * A[d] + be * B[d] + zeta * C[d]) / q;
-                                const double xab = A[d] - B[d], xac = A[d] - C[d], xbc = B[d] - C[d];
-                                K[d] = exp(-muab * xab * xab) * exp(-muac * xac * xac) * exp(-mubc * xbc * xbc);
+                            Q[0] = __shfl_sync(0xffffffffu, sc, 3);
+                            Q[1] = __shfl_sync(0xffffffffu, sc, 4);
+                            Q[2] = __shfl_sync(0xffffffffu, sc, 5);
+                            double ev = 0.0;
+                            if (lane < 9) {
+                                const int d = lane / 3, m = lane % 3;
+                                const double dd = m == 0 ? A[d] - B[d] : (m == 1 ? A[d] - C[d] : B[d] - C[d]);
+                                const double mu = m == 0 ? muab : (m == 1 ? muac : mubc);
+                                ev = exp(-mu * dd * dd);
                             }
+#pragma unroll
+                            for (int d = 0; d < 3; d++)
+                                K[d] = __shfl_sync(0xffffffffu, ev, 3 * d) * __shfl_sync(0xffffffffu, ev, 3 * d + 1) *
+                                       __shfl_sync(0xffffffffu, ev, 3 * d + 2);
                             for (int w = 0; w <= S; w++) {
                                 // entries (axis, i, j=w-i, t<=w)
                                 const int ilo = max(0, w - lb), ihi = min(la, w);
@@ -188,6 +210,7 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                 }
                                 __syncwarp();
                             }
+                            const double p15 = npow == 2 ? pow(kPi / q, 1.5) : 0.0;  // once per primitive triple
                             if (npow == 2) {
                                 pref = 0.0;
                             } else {
@@ -213,7 +236,7 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                     for (int e = lane; e < tot; e += 32) {
                                         const int n = e / ne, idx = e % ne;
                                         // decode idx -> (u+v = kk, v), t = s - kk
-                                        int kk = (int)((sqrt(8.0 * idx + 1.0) - 1.0) * 0.5);
+                                        int kk = (int)((sqrtf((float)(8 * idx + 1)) - 1.0f) * 0.5f);  // corrected below
                                         while ((kk + 1) * (kk + 2) / 2 <= idx) kk++;
                                         while (kk * (kk + 1) / 2 > idx) kk--;
                                         const int v = idx - kk * (kk + 1) / 2, u = kk - v, t = s - kk;
@@ -241,7 +264,7 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                     }
                                     __syncwarp();
                                 }
-                                pref = npow == 1 ? NA * NB * 2.0 * kPi / q : NA * NB * 2.0 * pow(kPi, 1.5) / sqrt(q);
+                                pref = npow == 1 ? NA * NB * 2.0 * kPi / q : NA * NB * 2.0 * kPi15 / sqrt(q);
                             }
                             // ---- Cartesian pairs of this lane
 #pragma unroll
@@ -254,7 +277,7 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                 double buf;
                                 if (npow == 2) {
                                     buf = NA * NB * E[eidx(lb1, S1, 0, ax, bx, 0, la1)] * E[eidx(lb1, S1, 1, ay, by, 0, la1)] *
-                                          E[eidx(lb1, S1, 2, az, bz, 0, la1)] * pow(kPi / q, 1.5);
+                                          E[eidx(lb1, S1, 2, az, bz, 0, la1)] * p15;
                                 } else {
                                     double s = 0.0;
                                     const double *ez = E + eidx(lb1, S1, 2, az, bz, 0, la1);
