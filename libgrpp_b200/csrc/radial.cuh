@@ -310,6 +310,23 @@ __global__ void __launch_bounds__(kRadThreads, GRPP_SCR_MINB) radial_screen_flat
         const int d2 = Lp + lb + 1;
         const int l1 = e / (d2 * dn), rem = e - l1 * d2 * dn, l2 = rem / dn, N = rem - l2 * dn;
         const int nk = __ldg(a.pot_nprim + pot), po = __ldg(a.pot_prim_off + pot);
+        // libgrpp tabulates the whole (l1, l2, N) box but its angular sums read only entries
+        // with N = n1 + n2 (n1 <= la, n2 <= lb), l1 in [max(L-n1,0), L+n1] of the parity of
+        // L+n1, l2 likewise (type2_integrals.c:169-184, spin_orbit_integrals.c:189-204). Every
+        // other entry is left out: it cannot change an output, and every entry's walk and
+        // stop level are its own (radial_type2_integral.c:242-318).
+        bool used = false;
+        for (int n1 = max(0, N - lb); n1 <= min(la, N) && !used; n1++) {
+            const int n2 = N - n1;
+            used = l1 >= max(Lp - n1, 0) && l1 <= Lp + n1 && ((Lp + n1 - l1) & 1) == 0 && l2 >= max(Lp - n2, 0) &&
+                   l2 <= Lp + n2 && ((Lp + n2 - l2) & 1) == 0;
+        }
+        if (!used) {
+            a.Q[g] = 0.0;
+            a.scr[g] = 0.0;
+            a.eflag[g] = 0;
+            continue;
+        }
         if (CA2 < 1e-14 && CB2 < 1e-14) {
             // analytic one-centre entry (radial_type2_integral.c:126-155): only l1 = l2 = 0 is non-zero
             double v = 0.0;
