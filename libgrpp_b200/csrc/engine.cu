@@ -222,6 +222,28 @@ double one_centre_prim(int L, double a1, double a2, int n, double zeta)
     return host_factorial(k) / (2.0 * std::pow(a, k + 1));
 }
 
+// Entry offsets (l1 d2 dn + l2 dn + N) within a potential's (l1, l2, N) block that the
+// type 2 and spin-orbit angular sums read (type2_integrals.c:169-184,
+// spin_orbit_integrals.c:189-204): N = n1 + n2, n1 <= la, n2 <= lb, l1 in
+// [max(L-n1, 0), L+n1] of the parity of L+n1, l2 likewise.
+std::vector<uint16_t> used_entries(int L, int la, int lb)
+{
+    const int d2 = L + lb + 1, dn = la + lb + 1;
+    std::vector<uint16_t> out;
+    for (int l1 = 0; l1 <= L + la; l1++)
+        for (int l2 = 0; l2 <= L + lb; l2++)
+            for (int N = 0; N < dn; N++) {
+                bool used = false;
+                for (int n1 = std::max(0, N - lb); n1 <= std::min(la, N) && !used; n1++) {
+                    const int n2 = N - n1;
+                    used = l1 >= std::max(L - n1, 0) && l1 <= L + n1 && ((L + n1 - l1) & 1) == 0 &&
+                           l2 >= std::max(L - n2, 0) && l2 <= L + n2 && ((L + n2 - l2) & 1) == 0;
+                }
+                if (used) out.push_back((uint16_t)((l1 * d2 + l2) * dn + N));
+            }
+    return out;
+}
+
 struct PotView {
     int L, J;
     std::vector<int> pw;
@@ -464,8 +486,11 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     std::vector<int> proj_a(nt, -1), proj_b(nt, -1);
     std::vector<MmdItem> items;
     std::vector<int> rad_task;
-    std::vector<int64_t> rad_qoff;
-    int64_t qtot = 0;
+    std::vector<int64_t> rad_qoff, rad_uoff;
+    int64_t qtot = 0, utot = 0;
+    std::vector<int2> ucls((kMaxL + 1) * (kMaxL + 1) * (kMaxL + 1), int2{0, 0});
+    std::vector<uint8_t> ucls_set(ucls.size(), 0);
+    std::vector<uint16_t> ulist;
     out_off[0] = 0;
     int mmd_lmax = 0, mmd_smax = 0;
     int rad_l1 = 0, rad_l2 = 0, rad_dn = 1, rad_npot = 0;
@@ -490,10 +515,19 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
             q_off[t] = qtot;
             rad_task.push_back((int)t);
             rad_qoff.push_back(qtot);
+            rad_uoff.push_back(utot);
             int e = 0;
             for (int i = 0; i < g_sl_n[g]; i++) {
                 const int L = p_L[sl_pot[g_sl_off[g] + i]];
                 e += (L + la + 1) * (L + lb + 1) * (la + lb + 1);
+                const int key = (L * (kMaxL + 1) + la) * (kMaxL + 1) + lb;
+                if (!ucls_set[key]) {
+                    const std::vector<uint16_t> u = used_entries(L, la, lb);
+                    ucls[key] = int2{(int)ulist.size(), (int)u.size()};
+                    ulist.insert(ulist.end(), u.begin(), u.end());
+                    ucls_set[key] = 1;
+                }
+                utot += ucls[key].y;
                 rad_l1 = std::max(rad_l1, L + la);
                 rad_l2 = std::max(rad_l2, L + lb);
                 fin_lam = std::max(fin_lam, L + std::max(la, lb));
@@ -575,7 +609,8 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     const size_t o_cor = pk.add(c_or), o_cg = pk.add(c_g);
     const size_t o_ta = pk.add(ta), o_tb = pk.add(tb), o_tc = pk.add(tc), o_too = pk.add(out_off), o_thul = pk.add(has_ul),
                  o_tqo = pk.add(q_off), o_tpa = pk.add(proj_a), o_tpb = pk.add(proj_b);
-    const size_t o_items = pk.add(items), o_rt = pk.add(rad_task), o_rq = pk.add(rad_qoff);
+    const size_t o_items = pk.add(items), o_rt = pk.add(rad_task), o_rq = pk.add(rad_qoff), o_ru = pk.add(rad_uoff),
+                 o_ucls = pk.add(ucls), o_ulist = pk.add(ulist);
     const size_t o_bs = pk.add(blk_shell), o_bo = pk.add(blk_oc), o_bco = pk.add(blk_cart_off), o_bso = pk.add(blk_sph_off),
                  o_poffp = pk.add(proj_off);
     std::vector<int8_t> stop_dummy;
@@ -708,6 +743,10 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         r.pot_alpha = at<double>(ib, o_palpha);
         r.q_off = at<int64_t>(ib, o_rq);
         r.n_entries = qtot;
+        r.u_off = at<int64_t>(ib, o_ru);
+        r.n_used = utot;
+        r.ucls = at<int2>(ib, o_ucls);
+        r.ulist = at<uint16_t>(ib, o_ulist);
         r.Q = Qd;
         r.S_prev = Spd;
         r.scr = SCd;
@@ -726,7 +765,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         P.rad_blocks = (int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 16);
         int scr_occ = 0;
         GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&scr_occ, radial_screen_flat_kernel, kRadThreads, 0));
-        P.scr_blocks = (int)std::min<int64_t>((qtot + kRadThreads - 1) / kRadThreads, (int64_t)nsm * std::max(scr_occ, 1));
+        P.scr_blocks = (int)std::min<int64_t>((utot + kRadThreads - 1) / kRadThreads, (int64_t)nsm * std::max(scr_occ, 1));
         P.rad_smem = smem;
     }
 
@@ -812,8 +851,11 @@ int plan_execute(Plan &P)
     }
     if (P.rad_blocks > 0) {
         GRPP_CUDA(cudaMemsetAsync(P.rad.walk, 0, (size_t)P.n_radial, s));
-        radial_screen_flat_kernel<<<P.scr_blocks, kRadThreads, 0, s>>>(P.rad);
-        GRPP_CUDA(cudaGetLastError());
+        GRPP_CUDA(cudaMemsetAsync(P.rad.eflag, 0, (size_t)P.n_entries, s));  // unread entries stay inactive
+        if (P.scr_blocks > 0) {
+            radial_screen_flat_kernel<<<P.scr_blocks, kRadThreads, 0, s>>>(P.rad);
+            GRPP_CUDA(cudaGetLastError());
+        }
         GRPP_CUDA(cudaEventRecord(st.ev[4], s));
         RadialArgs ra = P.rad;
         if (P.opt.radial_mode == LIBGRPP_B200_RADIAL_LEARNED) {

@@ -67,6 +67,12 @@ struct RadialArgs {
     const int *pot_L, *pot_nprim, *pot_prim_off, *pot_powers;
     const double *pot_coef, *pot_alpha;
     const int64_t *q_off;       // per item
+    // entries the angular sums read, per item: u_off[item] = first used index; per class
+    // (L, la, lb) ucls = {offset into ulist, count}; ulist = entry offsets within a potential's block
+    const int64_t *u_off;
+    int64_t n_used;
+    const int2 *ucls;
+    const uint16_t *ulist;
     double *Q;                  // table values (running sums during the walk)
     double *S_prev, *scr;       // per entry scratch, same indexing as Q
     uint8_t *eflag;             // per entry: kEntActive | kEntScrOk
@@ -279,15 +285,15 @@ __global__ void __launch_bounds__(kRadThreads, GRPP_SCR_MINB) radial_screen_flat
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const long long t0 = clock64();
     unsigned long long c_combo = 0, c_iter = 0, c_final = 0;
-    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.n_entries; g += stride) {
+    for (int64_t gu = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gu < a.n_used; gu += stride) {
         int lo = 0, hi = a.n_items - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (__ldg(a.q_off + mid) <= g) lo = mid;
+            if (__ldg(a.u_off + mid) <= gu) lo = mid;
             else hi = mid - 1;
         }
         const int item = lo;
-        int e = (int)(g - __ldg(a.q_off + item));
+        int ku = (int)(gu - __ldg(a.u_off + item));
         const int t = __ldg(a.item_task + item);
         const int sa = __ldg(a.task_a + t), sb = __ldg(a.task_b + t), c = __ldg(a.task_c + t);
         const double *Ao = a.shell_origin + 3 * sa, *Bo = a.shell_origin + 3 * sb, *Co = a.centre_origin + 3 * c;
@@ -299,34 +305,29 @@ __global__ void __launch_bounds__(kRadThreads, GRPP_SCR_MINB) radial_screen_flat
         }
         const int la = __ldg(a.shell_L + sa), lb = __ldg(a.shell_L + sb), dn = la + lb + 1;
         const int gr = __ldg(a.centre_grpp + c), npot = __ldg(a.grpp_sl_n + gr), slo = __ldg(a.grpp_sl_off + gr);
-        int pot = -1, Lp = 0;
+        // libgrpp tabulates the whole (l1, l2, N) box of every potential, but its angular sums
+        // read only the entries with N = n1 + n2 (n1 <= la, n2 <= lb), l1 in [max(L-n1,0), L+n1]
+        // of the parity of L+n1, l2 likewise (type2_integrals.c:169-184,
+        // spin_orbit_integrals.c:189-204). Only those are screened and walked: the others cannot
+        // change an output, and every entry's walk and stop level are its own
+        // (radial_type2_integral.c:242-318). The host lists them per class (L, la, lb).
+        int pot = -1, Lp = 0, e = 0;
+        int64_t pe = 0;
         for (int p = 0; p < npot; p++) {
             pot = __ldg(a.sl_pot + slo + p);
             Lp = __ldg(a.pot_L + pot);
-            const int cnt = (Lp + la + 1) * (Lp + lb + 1) * dn;
-            if (e < cnt) break;
-            e -= cnt;
+            const int2 cls = a.ucls[(Lp * (kMaxL + 1) + la) * (kMaxL + 1) + lb];
+            if (ku < cls.y) {
+                e = a.ulist[cls.x + ku];
+                break;
+            }
+            ku -= cls.y;
+            pe += (Lp + la + 1) * (Lp + lb + 1) * dn;
         }
+        const int64_t g = __ldg(a.q_off + item) + pe + e;
         const int d2 = Lp + lb + 1;
         const int l1 = e / (d2 * dn), rem = e - l1 * d2 * dn, l2 = rem / dn, N = rem - l2 * dn;
         const int nk = __ldg(a.pot_nprim + pot), po = __ldg(a.pot_prim_off + pot);
-        // libgrpp tabulates the whole (l1, l2, N) box but its angular sums read only entries
-        // with N = n1 + n2 (n1 <= la, n2 <= lb), l1 in [max(L-n1,0), L+n1] of the parity of
-        // L+n1, l2 likewise (type2_integrals.c:169-184, spin_orbit_integrals.c:189-204). Every
-        // other entry is left out: it cannot change an output, and every entry's walk and
-        // stop level are its own (radial_type2_integral.c:242-318).
-        bool used = false;
-        for (int n1 = max(0, N - lb); n1 <= min(la, N) && !used; n1++) {
-            const int n2 = N - n1;
-            used = l1 >= max(Lp - n1, 0) && l1 <= Lp + n1 && ((Lp + n1 - l1) & 1) == 0 && l2 >= max(Lp - n2, 0) &&
-                   l2 <= Lp + n2 && ((Lp + n2 - l2) & 1) == 0;
-        }
-        if (!used) {
-            a.Q[g] = 0.0;
-            a.scr[g] = 0.0;
-            a.eflag[g] = 0;
-            continue;
-        }
         if (CA2 < 1e-14 && CB2 < 1e-14) {
             // analytic one-centre entry (radial_type2_integral.c:126-155): only l1 = l2 = 0 is non-zero
             double v = 0.0;
