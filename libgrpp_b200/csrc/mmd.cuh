@@ -184,6 +184,9 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                             for (int d = 0; d < 3; d++)
                                 K[d] = __shfl_sync(0xffffffffu, ev, 3 * d) * __shfl_sync(0xffffffffu, ev, 3 * d + 1) *
                                        __shfl_sync(0xffffffffu, ev, 3 * d + 2);
+                            // K[d] scales every Hermite coefficient of axis d: when one underflowed to
+                            // exactly 0 the triple adds exact zeros (warp-uniform test)
+                            if (K[0] == 0.0 || K[1] == 0.0 || K[2] == 0.0) continue;
                             for (int w = 0; w <= S; w++) {
                                 // entries (axis, i, j=w-i, t<=w)
                                 const int ilo = max(0, w - lb), ihi = min(la, w);
