@@ -124,6 +124,10 @@ int libgrpp_b200_plan_stats(const libgrpp_b200_plan_t *plan, double *ms, int64_t
  * terms, r^N powers, entry x point accumulations, screening estimates / iterations / envelopes, levels */
 int libgrpp_b200_plan_counters(const libgrpp_b200_plan_t *plan, uint64_t *counters, int n);
 void libgrpp_b200_plan_destroy(libgrpp_b200_plan_t *plan);
+/* on != 0: later executes also count the type 1 kernel's operations (slots 13-14 of
+ * libgrpp_b200_plan_counters: primitive triples, FP64 operations) in a slower build of
+ * that kernel; the radial counters are always kept. */
+int libgrpp_b200_plan_set_counting(libgrpp_b200_plan_t *plan, int on);
 
 /* Density-contracted GRPP gradient (no counterpart in libgrpp, whose driver forms one
  * gradient matrix per atom coordinate, test_libgrpp_c/main.c:529-620):

@@ -86,6 +86,7 @@ class LibGRPP:
         self._opt("libgrpp_b200_plan_stats", ct.c_int, [_V, _D, ct.POINTER(ct.c_int64)])
         self._opt("libgrpp_b200_plan_destroy", None, [_V])
         self._opt("libgrpp_b200_plan_counters", ct.c_int, [_V, ct.POINTER(ct.c_uint64), ct.c_int])
+        self._opt("libgrpp_b200_plan_set_counting", ct.c_int, [_V, ct.c_int])
         _F = ct.POINTER(ct.c_float)
         _B = ct.POINTER(ct.c_int8)
         self._opt("libgrpp_b200_plan_learned_stats", ct.c_int, [_V, _D, ct.POINTER(ct.c_int64)])
@@ -198,7 +199,7 @@ class LibGRPP:
         if radial_mode == 1:
             self.ensure_level_model()
         n = int(batch.block_offsets()[-1])
-        outs = [np.zeros(max(n, 1)) for _ in range(4)]
+        outs = [np.empty(max(n, 1)) for _ in range(4)]  # the call writes every element
         rc = self.lib.libgrpp_b200_full_grpp_batch(ct.byref(batch.struct), radial_mode, *[_dp(x) for x in outs])
         if rc != 0:
             raise RuntimeError(f"libgrpp_b200_full_grpp_batch failed ({rc}): {self.last_error_message()}")
@@ -372,6 +373,9 @@ class Plan:
                 "n_tasks": int(cnt[0]), "n_radial": int(cnt[1]), "n_type1_items": int(cnt[2]),
                 "n_entries": int(cnt[3]), "h2d_bytes": int(cnt[4])}
 
+    def set_counting(self, on: bool):
+        self.lib.lib.libgrpp_b200_plan_set_counting(self.h, 1 if on else 0)
+
     def learned_stats(self):
         ms = ct.c_double(0.0)
         fb = ct.c_int64(0)
@@ -379,7 +383,7 @@ class Plan:
         return {"ms_predict": ms.value, "fallbacks": int(fb.value)}
 
     COUNTERS = ("screen_cycles", "quad_cycles", "items", "points", "bessel", "prim_pts", "term_pts", "pow_pts",
-                "accum", "scr_combos", "scr_iters", "scr_final", "levels")
+                "accum", "scr_combos", "scr_iters", "scr_final", "levels", "mmd_triples", "mmd_flops")
 
     def counters(self):
         c = np.zeros(len(self.COUNTERS), dtype=np.uint64)

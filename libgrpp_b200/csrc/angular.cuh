@@ -237,6 +237,7 @@ struct FinalSmem {
     int n_omega;     // per side
     int n_q;
     int n_v;
+    int n_w;         // W[j][abc][comp] of the factored re-centring sum (0: not used)
 };
 
 __device__ __forceinline__ double lmat_val(int L, int comp, int m1, int m2)
@@ -324,6 +325,22 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                     }
                     (side ? rshB : rshA)[l * rs + mu + l] = v;
                 }
+            }
+            // The binomial factor of a re-centring term is F_A(abc) F_B(def) (binomials times powers
+            // of CA, CB components), so the sum over (a..f) factors as sum_abc F_A W[abc] with
+            // W[abc] = sum_def F_B V[abc][def]. libgrpp skips terms whose factor is below its
+            // threshold (1e-13; 1e-14 for spin-orbit); when a lower bound of every non-zero factor
+            // clears twice that, only exact zeros are skipped and the factored sum has the same
+            // terms. Otherwise the term-by-term loop runs.
+            bool fact = sm.n_w > 0;
+            if (fact) {
+                double mA = 1.0, mB = 1.0;
+                for (int d = 0; d < 3; d++) {
+                    const double xa = fabs(powA[d][la]), xb = fabs(powB[d][lb]);
+                    if (sCA[d] != 0.0 && xa < 1.0) mA *= xa;
+                    if (sCB[d] != 0.0 && xb < 1.0) mB *= xb;
+                }
+                fact = mA * mB >= 2e-13;
             }
             const int64_t qbase = a.task_q_off[t];
             int64_t qoff = 0;
@@ -459,6 +476,64 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                         }
                     }
                     __syncthreads();
+                    if (fact) {
+                        double *W = V + sm.n_v;
+                        const int nrow = r1 - r0;
+                        for (int e = tid; e < nB * nrow; e += kFinThreads) {
+                            const int j = e / nrow, ar = e % nrow;
+                            const int bx = cB[3 * j], by = cB[3 * j + 1], bz = cB[3 * j + 2];
+                            double w0 = 0.0, w1 = 0.0, w2 = 0.0;
+                            for (int dd = 0; dd <= bx; dd++)
+                                for (int ee = 0; ee <= by; ee++)
+                                    for (int ff = 0; ff <= bz; ff++) {
+                                        const double fb = c_tab.binom[bx * kBinN + dd] * c_tab.binom[by * kBinN + ee] *
+                                                          c_tab.binom[bz * kBinN + ff] * powB[0][bx - dd] * powB[1][by - ee] *
+                                                          powB[2][bz - ff];
+                                        if (fb == 0.0) continue;
+                                        const double *vv = V + (ar * nabB + abc_index(lb, dd, ee, ff)) * ncomp;
+                                        w0 += fb * vv[0];
+                                        if (so) {
+                                            w1 += fb * vv[1];
+                                            w2 += fb * vv[2];
+                                        }
+                                    }
+                            double *ww = W + (j * nrow + ar) * ncomp;
+                            ww[0] = w0;
+                            if (so) {
+                                ww[1] = w1;
+                                ww[2] = w2;
+                            }
+                        }
+                        __syncthreads();
+#pragma unroll
+                        for (int q = 0; q < kFinElemPerThread; q++) {
+                            const int el = tid + q * kFinThreads;
+                            if (el >= nel) continue;
+                            const int i = el / nB, j = el % nB;
+                            const int ax = cA[3 * i], ay = cA[3 * i + 1], az = cA[3 * i + 2];
+                            double g0 = gam[0][q], g1 = gam[1][q], g2 = gam[2][q];
+                            for (int aa = 0; aa <= ax; aa++)
+                                for (int bb = 0; bb <= ay; bb++)
+                                    for (int cc = 0; cc <= az; cc++) {
+                                        const int abc = abc_index(la, aa, bb, cc);
+                                        if (abc < r0 || abc >= r1) continue;
+                                        const double fa = c_tab.binom[ax * kBinN + aa] * c_tab.binom[ay * kBinN + bb] *
+                                                          c_tab.binom[az * kBinN + cc] * powA[0][ax - aa] * powA[1][ay - bb] *
+                                                          powA[2][az - cc];
+                                        if (fa == 0.0) continue;
+                                        const double *ww = W + (j * nrow + abc - r0) * ncomp;
+                                        g0 += fa * ww[0];
+                                        if (so) {
+                                            g1 += fa * ww[1];
+                                            g2 += fa * ww[2];
+                                        }
+                                    }
+                            gam[0][q] = g0;
+                            gam[1][q] = g1;
+                            gam[2][q] = g2;
+                        }
+                        continue;
+                    }
                     // Cartesian pairs: binomial re-centring sums over (a..f) in the reference's loop order
 #pragma unroll
                     for (int q = 0; q < kFinElemPerThread; q++) {

@@ -710,6 +710,13 @@ int libgrpp_b200_plan_counters(const libgrpp_b200_plan_t *plan, uint64_t *counte
 
 void libgrpp_b200_plan_destroy(libgrpp_b200_plan_t *plan) { grpp::plan_destroy((grpp::Plan *)plan); }
 
+int libgrpp_b200_plan_set_counting(libgrpp_b200_plan_t *plan, int on)
+{
+    if (!plan) return LIBGRPP_B200_ERR_INVALID;
+    grpp::plan_set_counting((grpp::Plan *)plan, on != 0);
+    return 0;
+}
+
 int libgrpp_b200_grpp_gradient_contract(const libgrpp_b200_batch_t *b, int radial_mode, const int *shell_atom,
                                         const int *centre_atom, const double *atom_xyz, int n_atoms, const int *bf_off,
                                         int n_bf, const double *D, double *g)

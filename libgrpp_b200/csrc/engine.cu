@@ -22,8 +22,8 @@
 
 #include "grpp_common.cuh"
 #include "specfunc.cuh"
-#include "mmd.cuh"
 #include "radial.cuh"
+#include "mmd.cuh"
 #include "angular.cuh"
 #include "level_model.cuh"
 #include "gradient.cuh"
@@ -134,8 +134,10 @@ int init_device_state(DeviceState &st, int device)
     GRPP_CUDA(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking));
     for (auto &e : st.ev) GRPP_CUDA(cudaEventCreate(&e));
     st.atab_off.assign((kMaxL + 2) * (kMaxL + 2), -1);
-    GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(radial_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_train_smem_bytes()));
@@ -328,6 +330,7 @@ struct Plan {
     int fin_blocks = 0;
     size_t fin_smem = 0;
     RunStats stats;
+    bool count_ops = false;  // run the type 1 kernel's counting instantiation
 };
 
 int64_t batch_output_size(const libgrpp_b200_batch_t *b)
@@ -498,6 +501,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     std::map<std::pair<int, int>, int> proj_map;
     std::vector<std::pair<int, int>> projs;
     std::vector<std::pair<int, int>> atab_need;
+    std::vector<uint8_t> atab_flag((kMaxL + 1) * (kMaxL + 1), 0);  // (L, l) pairs seen
     for (int64_t t = 0; t < nt; t++) {
         const int A = ta[t], B = tb[t], C = tc[t], g = b->centre_grpp[C];
         const int la = sh_L[A], lb = sh_L[B];
@@ -532,8 +536,8 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
                 rad_l2 = std::max(rad_l2, L + lb);
                 fin_lam = std::max(fin_lam, L + std::max(la, lb));
                 fin_nq = std::max(fin_nq, (L + la + 1) * (L + lb + 1) * (la + lb + 1));
-                atab_need.push_back({L, la});
-                atab_need.push_back({L, lb});
+                atab_flag[L * (kMaxL + 1) + la] = 1;
+                atab_flag[L * (kMaxL + 1) + lb] = 1;
             }
             CHECK_INPUT(e <= kRadMaxEntries, "radial table larger than 16384 entries for one task");
             CHECK_INPUT(std::max(rad_l1, rad_l2) <= kRadMaxLam && la + lb + 1 <= kRadMaxN, "angular momentum too high for the radial path");
@@ -583,8 +587,9 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     const int64_t out_tot = out_off[nt];
 
     // angular tensors
-    std::sort(atab_need.begin(), atab_need.end());
-    atab_need.erase(std::unique(atab_need.begin(), atab_need.end()), atab_need.end());
+    for (int L = 0; L <= kMaxL; L++)
+        for (int l = 0; l <= kMaxL; l++)
+            if (atab_flag[L * (kMaxL + 1) + l]) atab_need.push_back({L, l});
     for (auto &lp : atab_need) {
         rc = ensure_atab(st, lp.first, lp.second);
         if (rc) return rc;
@@ -684,6 +689,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         m.lmax = mmd_lmax;
         m.smax = mmd_smax;
         m.status = statusd;
+        m.counters = (unsigned long long *)(statusd + 16);
         const int wpb = 4;
         const size_t smem = (size_t)wpb * mmd_ws_size(mmd_lmax, mmd_smax) * sizeof(double);
         P.mmd = m;
@@ -812,7 +818,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         f.so_y = o_sy;
         f.so_z = o_sz;
         f.status = statusd;
-        FinalSmem fs;
+        FinalSmem fs{};
         fs.rsh_stride = 2 * fin_lam + 1;
         fs.n_rsh = (fin_lam + 1) * fs.rsh_stride;
         int n_om = 1, nabmax = 1;
@@ -823,7 +829,12 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         fs.n_omega = n_om;
         fs.n_q = fin_nq;
         fs.n_v = std::max(6144, 3 * nabmax);
-        const size_t smem = (size_t)(2 * fs.n_rsh + 2 * fs.n_omega + fs.n_q + fs.n_v) * sizeof(double);
+        // W for the factored re-centring sum: ncart(lb) x n_abc(la) x 3, if it fits in 64 kB
+        int lmax_task = 0;
+        for (int i = 0; i < ns; i++) lmax_task = std::max(lmax_task, sh_L[i]);
+        const int nw = ncart(lmax_task) * nabmax * 3;
+        fs.n_w = nw * (int)sizeof(double) <= 64 * 1024 ? nw : 0;
+        const size_t smem = (size_t)(2 * fs.n_rsh + 2 * fs.n_omega + fs.n_q + fs.n_v + fs.n_w) * sizeof(double);
         P.fin = f;
         P.fin_smem_layout = fs;
         P.fin_blocks = (int)std::min<int64_t>(nt, (int64_t)nsm * 8);
@@ -840,8 +851,13 @@ int plan_execute(Plan &P)
     GRPP_CUDA(cudaMemsetAsync(P.status, 0, 16 * sizeof(int) + kRadCntNum * sizeof(unsigned long long), s));
     GRPP_CUDA(cudaEventRecord(st.ev[0], s));
     if (P.mmd_blocks > 0) {
-        if (P.mmd_kpl == 8) mmd_kernel<8><<<P.mmd_blocks, P.mmd_threads, P.mmd_smem, s>>>(P.mmd);
-        else mmd_kernel<32><<<P.mmd_blocks, P.mmd_threads, P.mmd_smem, s>>>(P.mmd);
+        if (P.count_ops) {
+            if (P.mmd_kpl == 8) mmd_kernel<8, true><<<P.mmd_blocks, P.mmd_threads, P.mmd_smem, s>>>(P.mmd);
+            else mmd_kernel<32, true><<<P.mmd_blocks, P.mmd_threads, P.mmd_smem, s>>>(P.mmd);
+        } else {
+            if (P.mmd_kpl == 8) mmd_kernel<8, false><<<P.mmd_blocks, P.mmd_threads, P.mmd_smem, s>>>(P.mmd);
+            else mmd_kernel<32, false><<<P.mmd_blocks, P.mmd_threads, P.mmd_smem, s>>>(P.mmd);
+        }
         GRPP_CUDA(cudaGetLastError());
     }
     GRPP_CUDA(cudaEventRecord(st.ev[1], s));
@@ -1004,6 +1020,8 @@ Plan *plan_create(const libgrpp_b200_batch_t *b, const RunOptions &opt)
     }
     return P;
 }
+
+void plan_set_counting(Plan *P, bool on) { P->count_ops = on; }
 
 int plan_run(Plan *P)
 {

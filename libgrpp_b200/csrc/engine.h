@@ -36,6 +36,7 @@ int64_t batch_output_size(const libgrpp_b200_batch_t *b);
 struct Plan;
 Plan *plan_create(const libgrpp_b200_batch_t *b, const RunOptions &opt);
 int plan_run(Plan *P);
+void plan_set_counting(Plan *P, bool on);
 int plan_outputs(Plan *P, double *arep, double *so_x, double *so_y, double *so_z);
 void plan_destroy(Plan *P);
 const RunStats *plan_stats(const Plan *P);

@@ -20,6 +20,7 @@
 
 #include "grpp_common.cuh"
 #include "specfunc.cuh"
+#include "radial.cuh"  // RadialCounter slots shared with the type 1 kernel
 
 namespace grpp {
 
@@ -45,7 +46,17 @@ struct MmdArgs {
     int smax;            // max la+lb over the items (sizes the shared workspace)
     int lmax;            // max l over the items
     int *status;
+    unsigned long long *counters;  // kRadCntMmdTriples / kRadCntMmdFlops slots (may be null)
 };
+
+// FP64 operations of one primitive triple, by phase (FMA = 2, exp/div/sqrt/pow = 1):
+// setup (q, 3 mu, 3 Q, 9 exponentials, K) 40; a Hermite coefficient 5; an auxiliary
+// function value 16 (Boys, 6th-order Taylor) or 100 per G_n series; an R^n_tuv entry 5;
+// a term E_x E_y E_z R of the contraction 3, plus 3 per Cartesian pair.
+__host__ __device__ inline unsigned long long mmd_e_count(int la, int lb)
+{
+    return 3ull * ((la + 1) * (lb + 1) + (lb + 1) * la * (la + 1) / 2 + (la + 1) * lb * (lb + 1) / 2);
+}
 
 // shared workspace per warp, in doubles
 __host__ __device__ inline int mmd_e_size(int lmax) { return 3 * (lmax + 1) * (lmax + 1) * (2 * lmax + 1); }
@@ -91,7 +102,8 @@ __device__ __forceinline__ int r_level_off(int S, int s)
 __device__ __forceinline__ int r_in_level(int u, int v) { return (u + v) * (u + v + 1) / 2 + v; }
 
 // KPL: Cartesian pairs held per lane per pass (8: up to 256 pairs, 32: up to 1024)
-template <int KPL>
+// COUNT: keep the operation counters (a separate instantiation, so the timed kernel carries none)
+template <int KPL, bool COUNT>
 __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
 {
     extern __shared__ double smem[];
@@ -105,6 +117,7 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
     int *lvl = (int *)(aux + (a.smax + 2));
     double *normA = aux + 2 * (a.smax + 2) + 16, *normB = normA + kMmdMaxPrims;  // per item
 
+    unsigned long long c_trip = 0, c_fl = 0;  // operation counters of this lane
     for (int it = blockIdx.x * wpb + warp; it < a.n_items; it += gridDim.x * wpb) {
         const MmdItem item = a.items[it];
         const int la = a.shell_L[item.bra], lb = a.shell_L[item.ket];
@@ -138,6 +151,17 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
 
         const int npairs = nA * nB;
         for (int pass = 0; pass < npairs; pass += 32 * KPL) {
+            // operations of one primitive triple's contraction over this pass's Cartesian pairs (counters)
+            const int pend = min(npairs, pass + 32 * KPL);
+            unsigned long long contract_fl = 0;
+            if (COUNT) {
+                for (int pr = pass + lane; pr < pend; pr += 32) {
+                    const int m = pr / nB, n = pr % nB;
+                    contract_fl += 3ull * (ca[3 * m] + cb[3 * n] + 1) * (ca[3 * m + 1] + cb[3 * n + 1] + 1) *
+                                       (ca[3 * m + 2] + cb[3 * n + 2] + 1) + 3ull;
+                }
+                for (int o = 16; o > 0; o >>= 1) contract_fl += __shfl_xor_sync(0xffffffffu, contract_fl, o);
+            }
             double res[KPL];
 #pragma unroll
             for (int q = 0; q < KPL; q++) res[q] = 0.0;
@@ -187,6 +211,15 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                             // K[d] scales every Hermite coefficient of axis d: when one underflowed to
                             // exactly 0 the triple adds exact zeros (warp-uniform test)
                             if (K[0] == 0.0 || K[1] == 0.0 || K[2] == 0.0) continue;
+                            if (COUNT && lane == 0) {
+                                c_trip++;
+                                c_fl += 40 + 5 * mmd_e_count(la, lb);
+                                if (npow != 2)
+                                    c_fl += (npow == 1 ? 16ull * (S + 1) : 100ull) + 2ull * (S + 1) +
+                                            5ull * (mmd_r_size(S) - (S + 1)) + contract_fl;
+                                else
+                                    c_fl += 4ull * (pend - pass);
+                            }
                             for (int w = 0; w <= S; w++) {
                                 // entries (axis, i, j=w-i, t<=w)
                                 const int ilo = max(0, w - lb), ihi = min(la, w);
@@ -323,6 +356,10 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                     }
                             }
                             __syncwarp();
+                            if (COUNT && lane == 0) {
+                                c_trip++;
+                                c_fl += 12ull * (la + 1) * (lb + 1) + 10 + 4ull * (pend - pass);  // Obara-Saika + pairs
+                            }
 #pragma unroll
                             for (int qq = 0; qq < KPL; qq++) {
                                 const int pr = pass + lane + 32 * qq;
@@ -348,6 +385,16 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
             }
         }
         __syncwarp();
+    }
+    if (COUNT && a.counters) {
+        for (int o = 16; o > 0; o >>= 1) {
+            c_trip += __shfl_down_sync(0xffffffffu, c_trip, o);
+            c_fl += __shfl_down_sync(0xffffffffu, c_fl, o);
+        }
+        if (lane == 0) {
+            atomicAdd(a.counters + kRadCntMmdTriples, c_trip);
+            atomicAdd(a.counters + kRadCntMmdFlops, c_fl);
+        }
     }
 }
 

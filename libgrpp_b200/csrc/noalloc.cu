@@ -386,7 +386,7 @@ int run(const libgrpp_b200_batch_t *b, double *h_arep)
     f.atab = (const double *)P(o_atab);
     f.arep = (double *)P(o_arep);
     f.so_x = f.so_y = f.so_z = (double *)P(o_dummy);  // no spin-orbit potentials: written with zeros
-    FinalSmem fs;
+    FinalSmem fs{};
     fs.rsh_stride = 2 * fin_lam + 1;
     fs.n_rsh = (fin_lam + 1) * fs.rsh_stride;
     int n_om = 1, nabmax = 1;

@@ -104,6 +104,8 @@ enum RadialCounter {
     kRadCntScrIters,           // fixed-point iterations of the screening
     kRadCntScrFinal,           // screening envelopes evaluated
     kRadCntLevels,             // grid levels walked (sum over tasks)
+    kRadCntMmdTriples,         // type 1 / overlap primitive triples evaluated (mmd_kernel)
+    kRadCntMmdFlops,           // their FP64 operations by the model of mmd_kernel's counting
     kRadCntNum
 };
 
