@@ -32,6 +32,8 @@
 
 namespace grpp {
 
+constexpr size_t kFinSmemMax = 200 * 1024;  // dynamic shared memory of the assembly kernel
+
 // ------------------------------------------------------------------ errors
 namespace {
 thread_local int t_err = 0;
@@ -139,7 +141,7 @@ int init_device_state(DeviceState &st, int device)
     GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(radial_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-    GRPP_CUDA(cudaFuncSetAttribute(final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRPP_CUDA(cudaFuncSetAttribute(final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFinSmemMax));
     GRPP_CUDA(cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_train_smem_bytes()));
     st.device = device;
     st.ready = true;
@@ -692,6 +694,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         m.counters = (unsigned long long *)(statusd + 16);
         const int wpb = 4;
         const size_t smem = (size_t)wpb * mmd_ws_size(mmd_lmax, mmd_smax) * sizeof(double);
+        CHECK_INPUT(smem <= 200 * 1024, "type 1 workspace of this batch's angular momenta exceeds one block's shared memory");
         P.mmd = m;
         P.mmd_kpl = ncart(mmd_lmax) * ncart(mmd_lmax) <= 256 ? 8 : 32;
         P.mmd_blocks = (int)std::min<int64_t>(((int64_t)items.size() + wpb - 1) / wpb, (int64_t)nsm * 16);
@@ -767,6 +770,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         r.eflag = eflagd;
         r.walk = walkd;
         const size_t smem = (size_t)(rad_npot + (rad_l1 + 1) + (rad_l2 + 1) + rad_dn) * kRadRow * sizeof(double);
+        CHECK_INPUT(smem <= 160 * 1024, "radial grid chunk of this batch exceeds one block's shared memory");
         P.rad = r;
         P.rad_blocks = (int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 16);
         int scr_occ = 0;
@@ -833,8 +837,10 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         int lmax_task = 0;
         for (int i = 0; i < ns; i++) lmax_task = std::max(lmax_task, sh_L[i]);
         const int nw = ncart(lmax_task) * nabmax * 3;
-        fs.n_w = nw * (int)sizeof(double) <= 64 * 1024 ? nw : 0;
-        const size_t smem = (size_t)(2 * fs.n_rsh + 2 * fs.n_omega + fs.n_q + fs.n_v + fs.n_w) * sizeof(double);
+        const size_t smem_base = (size_t)(2 * fs.n_rsh + 2 * fs.n_omega + fs.n_q + fs.n_v) * sizeof(double);
+        CHECK_INPUT(smem_base <= kFinSmemMax, "assembly tables of this batch exceed the shared memory of one block");
+        fs.n_w = smem_base + (size_t)nw * sizeof(double) <= kFinSmemMax ? nw : 0;
+        const size_t smem = smem_base + (size_t)fs.n_w * sizeof(double);
         P.fin = f;
         P.fin_smem_layout = fs;
         P.fin_blocks = (int)std::min<int64_t>(nt, (int64_t)nsm * 8);
