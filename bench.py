@@ -222,11 +222,12 @@ def run_ours(args, rank, world, local):
     from libgrpp_b200 import engine
 
     dist = None
+    torch.cuda.set_device(local)  # before the process group, so NCCL binds this rank's GPU
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
     lib = engine.load()
     lib.set_device(local)
     modes = {"plain": 0, "learned": 1}
