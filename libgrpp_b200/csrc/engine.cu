@@ -693,10 +693,11 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         m.status = statusd;
         m.counters = (unsigned long long *)(statusd + 16);
         const int wpb = 4;
-        const size_t smem = (size_t)wpb * mmd_ws_size(mmd_lmax, mmd_smax) * sizeof(double);
+        P.mmd_kpl = ncart(mmd_lmax) * ncart(mmd_lmax) <= 256 ? 8 : 32;
+        // per warp: the workspace, then 32 x KPL pair descriptors (8 bytes each)
+        const size_t smem = (size_t)wpb * (mmd_ws_size(mmd_lmax, mmd_smax) + 32 * P.mmd_kpl) * sizeof(double);
         CHECK_INPUT(smem <= 200 * 1024, "type 1 workspace of this batch's angular momenta exceeds one block's shared memory");
         P.mmd = m;
-        P.mmd_kpl = ncart(mmd_lmax) * ncart(mmd_lmax) <= 256 ? 8 : 32;
         P.mmd_blocks = (int)std::min<int64_t>(((int64_t)items.size() + wpb - 1) / wpb, (int64_t)nsm * 16);
         P.mmd_threads = 32 * wpb;
         P.mmd_smem = smem;

@@ -116,6 +116,11 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
     double *aux = R0 + mmd_tet(a.smax);
     int *lvl = (int *)(aux + (a.smax + 2));
     double *normA = aux + 2 * (a.smax + 2) + 16, *normB = normA + kMmdMaxPrims;  // per item
+    // lane-private descriptors of the Cartesian pairs of the current pass (after all warps'
+    // workspaces): x = E row of axis x | E row of axis y << 16, y = E row of axis z |
+    // (ax+bx) << 16 | (ay+by) << 21 | (az+bz) << 26 — each pair is decoded once per pass,
+    // not once per primitive triple
+    int2 *pdesc = reinterpret_cast<int2 *>(smem + wpb * ws) + warp * 32 * KPL;
 
     unsigned long long c_trip = 0, c_fl = 0;  // operation counters of this lane
     for (int it = blockIdx.x * wpb + warp; it < a.n_items; it += gridDim.x * wpb) {
@@ -161,6 +166,17 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                        (ca[3 * m + 2] + cb[3 * n + 2] + 1) + 3ull;
                 }
                 for (int o = 16; o > 0; o >>= 1) contract_fl += __shfl_xor_sync(0xffffffffu, contract_fl, o);
+            }
+#pragma unroll
+            for (int qq = 0; qq < KPL; qq++) {
+                const int pr = pass + lane + 32 * qq;
+                if (pr >= npairs) break;
+                const int m = pr / nB, n = pr % nB;
+                const int ax = ca[3 * m], ay = ca[3 * m + 1], az = ca[3 * m + 2];
+                const int bx = cb[3 * n], by = cb[3 * n + 1], bz = cb[3 * n + 2];
+                pdesc[qq * 32 + lane] =
+                    make_int2(eidx(lb1, S1, 0, ax, bx, 0, la1) | (eidx(lb1, S1, 1, ay, by, 0, la1) << 16),
+                              eidx(lb1, S1, 2, az, bz, 0, la1) | ((ax + bx) << 16) | ((ay + by) << 21) | ((az + bz) << 26));
             }
             double res[KPL];
 #pragma unroll
@@ -307,21 +323,19 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                             for (int qq = 0; qq < KPL; qq++) {
                                 const int pr = pass + lane + 32 * qq;
                                 if (pr >= npairs) break;
-                                const int m = pr / nB, n = pr % nB;
-                                const int ax = ca[3 * m], ay = ca[3 * m + 1], az = ca[3 * m + 2];
-                                const int bx = cb[3 * n], by = cb[3 * n + 1], bz = cb[3 * n + 2];
+                                const int2 dsc = pdesc[qq * 32 + lane];
+                                const int offx = dsc.x & 0xffff, offy = (int)((unsigned)dsc.x >> 16), offz = dsc.y & 0xffff;
+                                const int tx = (dsc.y >> 16) & 31, uy = (dsc.y >> 21) & 31, vz = (dsc.y >> 26) & 31;
                                 double buf;
                                 if (npow == 2) {
-                                    buf = NA * NB * E[eidx(lb1, S1, 0, ax, bx, 0, la1)] * E[eidx(lb1, S1, 1, ay, by, 0, la1)] *
-                                          E[eidx(lb1, S1, 2, az, bz, 0, la1)] * p15;
+                                    buf = NA * NB * E[offx] * E[offy] * E[offz] * p15;
                                 } else {
                                     double s = 0.0;
-                                    const double *ez = E + eidx(lb1, S1, 2, az, bz, 0, la1);
-                                    const int vz = az + bz;
-                                    for (int t = 0; t <= ax + bx; t++) {
-                                        const double ex = E[eidx(lb1, S1, 0, ax, bx, t, la1)];
-                                        for (int u = 0; u <= ay + by; u++) {
-                                            const double exy = ex * E[eidx(lb1, S1, 1, ay, by, u, la1)];
+                                    const double *ez = E + offz;
+                                    for (int t = 0; t <= tx; t++) {
+                                        const double ex = E[offx + t];
+                                        for (int u = 0; u <= uy; u++) {
+                                            const double exy = ex * E[offy + u];
                                             const double *r0 = R0 + r0_row(S, t, u);
                                             for (int v = 0; v <= vz; v++) s += exy * ez[v] * r0[v];
                                         }
@@ -364,10 +378,9 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                             for (int qq = 0; qq < KPL; qq++) {
                                 const int pr = pass + lane + 32 * qq;
                                 if (pr >= npairs) break;
-                                const int m = pr / nB, n = pr % nB;
-                                const double buf = NA * NB * E[eidx(lb1, S1, 0, ca[3 * m], cb[3 * n], 0, la1)] *
-                                                   E[eidx(lb1, S1, 1, ca[3 * m + 1], cb[3 * n + 1], 0, la1)] *
-                                                   E[eidx(lb1, S1, 2, ca[3 * m + 2], cb[3 * n + 2], 0, la1)];
+                                const int2 dsc = pdesc[qq * 32 + lane];
+                                const double buf = NA * NB * E[dsc.x & 0xffff] * E[(int)((unsigned)dsc.x >> 16)] *
+                                                   E[dsc.y & 0xffff];
                                 accp[qq] += (ci * cj) * buf;
                             }
                         }
