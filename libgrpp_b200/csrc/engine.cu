@@ -492,7 +492,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     std::vector<MmdItem> items;
     std::vector<int> rad_task;
     std::vector<int64_t> rad_qoff, rad_uoff;
-    int64_t qtot = 0, utot = 0;
+    int64_t qtot = 0, utot = 0, rad_list_max = 0;
     std::vector<int2> ucls((kMaxL + 1) * (kMaxL + 1) * (kMaxL + 1), int2{0, 0});
     std::vector<uint8_t> ucls_set(ucls.size(), 0);
     std::vector<uint16_t> ulist;
@@ -523,6 +523,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
             rad_qoff.push_back(qtot);
             rad_uoff.push_back(utot);
             int e = 0;
+            int64_t item_used = 0;
             for (int i = 0; i < g_sl_n[g]; i++) {
                 const int L = p_L[sl_pot[g_sl_off[g] + i]];
                 e += (L + la + 1) * (L + lb + 1) * (la + lb + 1);
@@ -534,6 +535,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
                     ucls_set[key] = 1;
                 }
                 utot += ucls[key].y;
+                item_used += ucls[key].y;
                 rad_l1 = std::max(rad_l1, L + la);
                 rad_l2 = std::max(rad_l2, L + lb);
                 fin_lam = std::max(fin_lam, L + std::max(la, lb));
@@ -544,6 +546,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
             CHECK_INPUT(e <= kRadMaxEntries, "radial table larger than 16384 entries for one task");
             CHECK_INPUT(std::max(rad_l1, rad_l2) <= kRadMaxLam && la + lb + 1 <= kRadMaxN, "angular momentum too high for the radial path");
             qtot += e;
+            rad_list_max = std::max(rad_list_max, item_used);
             rad_dn = std::max(rad_dn, la + lb + 1);
             rad_npot = std::max(rad_npot, g_sl_n[g]);
         }
@@ -770,8 +773,12 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         r.counters = (unsigned long long *)(statusd + 16);
         r.eflag = eflagd;
         r.walk = walkd;
-        const size_t smem = (size_t)(rad_npot + (rad_l1 + 1) + (rad_l2 + 1) + rad_dn) * kRadRow * sizeof(double);
+        const int chunk_doubles = (rad_npot + (rad_l1 + 1) + (rad_l2 + 1) + rad_dn) * kRadRow;
+        // two lists of active entries (uint16), sized for the task with most entries read
+        const size_t smem = (size_t)chunk_doubles * sizeof(double) + (size_t)((4 * rad_list_max + 7) / 8) * 8;
         CHECK_INPUT(smem <= 160 * 1024, "radial grid chunk of this batch exceeds one block's shared memory");
+        r.list_max = (int)rad_list_max;
+        r.chunk_doubles = chunk_doubles;
         P.rad = r;
         P.rad_blocks = (int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 16);
         int scr_occ = 0;

@@ -67,6 +67,9 @@ struct RadialArgs {
     const int *pot_L, *pot_nprim, *pot_prim_off, *pot_powers;
     const double *pot_coef, *pot_alpha;
     const int64_t *q_off;       // per item
+    // walk: two lists of active entry indices (uint16) of up to list_max entries each, after
+    // chunk_doubles doubles of point arrays in dynamic shared memory; list_max = 0: no lists
+    int list_max, chunk_doubles;
     // entries the angular sums read, per item: u_off[item] = first used index; per class
     // (L, la, lb) ucls = {offset into ulist, count}; ulist = entry offsets within a potential's block
     const int64_t *u_off;
@@ -683,7 +686,11 @@ __global__ void __launch_bounds__(kRadThreads, 4) radial_walk_kernel(RadialArgs 
     __shared__ int s_lvl;         // deepest level at which an entry converged
     extern __shared__ double chunk[];  // [npot + l1max+1 + l2max+1 + dn][kRadRow]
     __shared__ int s_item;
+    __shared__ int s_cnt[2];      // lengths of the two active-entry lists
     const int tid = threadIdx.x, lane = tid & 31;
+    const bool use_list = a.list_max > 0;
+    uint16_t *lists[2] = {reinterpret_cast<uint16_t *>(chunk + a.chunk_doubles),
+                          reinterpret_cast<uint16_t *>(chunk + a.chunk_doubles) + a.list_max};
     int next_static = blockIdx.x;
     for (;;) {
         int item;
@@ -705,7 +712,10 @@ __global__ void __launch_bounds__(kRadThreads, 4) radial_walk_kernel(RadialArgs 
         }
         __syncthreads();
         if (tid < 8) s_need[tid >> 2][tid & 3] = tid == 3 || tid == 7 ? 0 : -1;
-        if (tid == 0) s_lvl = 0;
+        if (tid == 0) {
+            s_lvl = 0;
+            s_cnt[0] = 0;
+        }
         load_task(a, item, sh, tid, kRadThreads);
         const int64_t qo = a.q_off[item];
         double *Q = a.Q + qo, *Sp = a.S_prev + qo;
@@ -730,6 +740,7 @@ __global__ void __launch_bounds__(kRadThreads, 4) radial_walk_kernel(RadialArgs 
                     n2 = max(n2, l2);
                     nN = max(nN, N);
                     mask |= 1 << p;
+                    if (use_list) lists[0][atomicAdd(&s_cnt[0], 1)] = (uint16_t)e;
                 }
             atomicMax(&s_need[1][0], n1);
             atomicMax(&s_need[1][1], n2);
@@ -745,6 +756,8 @@ __global__ void __launch_bounds__(kRadThreads, 4) radial_walk_kernel(RadialArgs 
             const int u1 = s_need[nb][0], u2 = s_need[nb][1], uN = s_need[nb][2], umask = s_need[nb][3];
             // this chunk's buffer: nobody reads or writes it between the two barriers
             if (tid < 4) s_need[chunk_no & 1][tid] = tid == 3 ? 0 : -1;
+            // the list this chunk writes (read last by the chunk before the previous one)
+            if (tid == 0) s_cnt[(chunk_no + 1) & 1] = 0;
             if (tid < np) {
                 int lev, i, nr;
                 walk_point(f0 + tid, lev, i, nr);
@@ -791,7 +804,12 @@ __global__ void __launch_bounds__(kRadThreads, 4) radial_walk_kernel(RadialArgs 
             int lev0, i0, nr0;
             walk_point(f0, lev0, i0, nr0);
             int my_active = 0, n1 = -1, n2 = -1, nN = -1, mask = 0, my_lvl = 0;
-            for (int e = tid; e < nE; e += kRadThreads) {
+            // active entries: from the compacted list (an even share per thread), else all entries
+            const int ncur = use_list ? s_cnt[chunk_no & 1] : nE;
+            const uint16_t *lcur = lists[chunk_no & 1];
+            uint16_t *lnext = lists[(chunk_no + 1) & 1];
+            for (int k = tid; k < ncur; k += kRadThreads) {
+                const int e = use_list ? lcur[k] : k;
                 uint8_t fl = EF[e];
                 if (!(fl & kEntActive)) continue;
                 int p, l1, l2, N;
@@ -823,6 +841,7 @@ __global__ void __launch_bounds__(kRadThreads, 4) radial_walk_kernel(RadialArgs 
                 Sp[e] = sp;
                 EF[e] = fl;
                 if (fl & kEntActive) {
+                    if (use_list) lnext[atomicAdd(&s_cnt[(chunk_no + 1) & 1], 1)] = (uint16_t)e;
                     my_active = 1;
                     n1 = max(n1, l1);
                     n2 = max(n2, l2);
