@@ -271,9 +271,20 @@ __device__ __forceinline__ bool scr_prim_flat(int l1, int l2, int n, double CA, 
         r0 = sqrt(s * inv2p);
     } while (fabs(r0 - r0p) > 1e-2);
     const double e1 = r0 - CA, e2 = r0 - CB;
-    *val = sqrt(kPi * inv_p) * ipow(r0, n) * bessel_scaled(l1, k1 * r0) * bessel_scaled(l2, k2 * r0) *
-           exp(-eta * r0 * r0 - aA * e1 * e1 - aB * e2 * e2) * 0.5 * (1 + erf(sqrt(p) * r0));
     *iters = -steps - 1;
+    // every factor of the envelope is finite and non-negative: a Gaussian factor that
+    // underflowed to exactly 0 makes the product exactly 0, so the other factors are not
+    // needed; and 1 + erf(z) is exactly 2 once erfc(z) < 2^-54 (z > 5.9), taken here as
+    // p r0^2 > 49 (z > 7). The product keeps libgrpp's order (screening.c:333-338).
+    const double ex = exp(-eta * r0 * r0 - aA * e1 * e1 - aB * e2 * e2);
+    if (ex == 0.0) {
+        *val = 0.0;
+        return false;
+    }
+    const double z2 = p * r0 * r0;
+    const double erf_part = z2 > 49.0 ? 2.0 : 1 + erf(sqrt(p) * r0);
+    *val = sqrt(kPi * inv_p) * ipow(r0, n) * bessel_scaled(l1, k1 * r0) * bessel_scaled(l2, k2 * r0) * ex * 0.5 *
+           erf_part;
     return false;
 }
 
