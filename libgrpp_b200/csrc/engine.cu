@@ -185,6 +185,37 @@ struct Packer {
     }
 };
 
+// Slot schedule of the Cartesian pairs of one (bra, ket) table class for mmd_kernel. Pairs
+// with equal (tx, uy, vz) = (ax+bx, ay+by, az+bz) have the same contraction loops: they are
+// coupled two by two into slots (2h, 2h+1) of one lane (an odd one out takes a slot couple
+// alone), and the couples fill the slot rows in (tx, uy, vz) order, so the 32 lanes of a row
+// run equal or nearly equal loops. Appends 32 x kpl slots to out; returns the rows in use.
+static int mmd_pair_schedule(const int8_t *ca, int nA, const int8_t *cb, int nB, int kpl, std::vector<uint16_t> &out)
+{
+    std::map<int, std::vector<int>> groups;  // key (tx * 32 + uy) * 32 + vz, ascending
+    for (int m = 0; m < nA; m++)
+        for (int n = 0; n < nB; n++) {
+            const int tx = ca[3 * m] + cb[3 * n], uy = ca[3 * m + 1] + cb[3 * n + 1], vz = ca[3 * m + 2] + cb[3 * n + 2];
+            groups[(tx * 32 + uy) * 32 + vz].push_back(m * nB + n);
+        }
+    std::vector<std::pair<int, int>> units;
+    for (auto &g : groups)
+        for (size_t i = 0; i < g.second.size(); i += 2)
+            units.push_back({g.second[i], i + 1 < g.second.size() ? g.second[i + 1] : -1});
+    const size_t base = out.size();
+    out.resize(base + 32 * (size_t)kpl, kMmdNoPair);
+    if ((int)units.size() > 16 * kpl) {  // more units than slot couples: plain order, unequal couples
+        for (int pr = 0; pr < nA * nB; pr++) out[base + pr] = (uint16_t)pr;
+        return (nA * nB + 63) / 64;
+    }
+    for (size_t r = 0; r < units.size(); r++) {
+        const int row = (int)(r / 32), lane = (int)(r % 32);
+        out[base + (2 * row) * 32 + lane] = (uint16_t)units[r].first;
+        if (units[r].second >= 0) out[base + (2 * row + 1) * 32 + lane] = (uint16_t)units[r].second;
+    }
+    return (int)(units.size() + 31) / 32;
+}
+
 template <typename T>
 T *at(void *base, size_t off)
 {
@@ -591,6 +622,33 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     proj_off[projs.size()] = sph_tot;
     const int64_t out_tot = out_off[nt];
 
+    // Cartesian pair schedules of the type 1 items, one per (bra, ket) table class
+    const int mmd_kpl = ncart(mmd_lmax) * ncart(mmd_lmax) <= 256 ? 8 : 32;
+    std::vector<uint16_t> mmd_sched;
+    {
+        std::map<std::vector<int8_t>, int> tab_id;  // a shell's Cartesian table -> class
+        std::vector<int> sh_tab(ns);
+        for (int i = 0; i < ns; i++) {
+            const std::vector<int8_t> tab(cart.begin() + 3 * sh_co[i], cart.begin() + 3 * (sh_co[i] + ncart(sh_L[i])));
+            auto ins = tab_id.insert({tab, (int)tab_id.size()});
+            sh_tab[i] = ins.first->second;
+        }
+        std::map<std::pair<int, int>, std::pair<int, int>> sched_of;  // -> (offset, rows)
+        for (auto &it : items) {
+            const int nA = ncart(sh_L[it.bra]), nB = ncart(sh_L[it.ket]);
+            CHECK_INPUT(nA * nB <= 32 * mmd_kpl, "type 1 block larger than one pass of the pair schedule");
+            auto f = sched_of.find({sh_tab[it.bra], sh_tab[it.ket]});
+            if (f == sched_of.end()) {
+                const int off = (int)mmd_sched.size();
+                const int rows = mmd_pair_schedule(cart.data() + 3 * sh_co[it.bra], nA, cart.data() + 3 * sh_co[it.ket],
+                                                   nB, mmd_kpl, mmd_sched);
+                f = sched_of.insert({{sh_tab[it.bra], sh_tab[it.ket]}, {off, rows}}).first;
+            }
+            it.sched = f->second.first;
+            it.sched_rows = f->second.second;
+        }
+    }
+
     // angular tensors
     for (int L = 0; L <= kMaxL; L++)
         for (int l = 0; l <= kMaxL; l++)
@@ -622,7 +680,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     const size_t o_items = pk.add(items), o_rt = pk.add(rad_task), o_rq = pk.add(rad_qoff), o_ru = pk.add(rad_uoff),
                  o_ucls = pk.add(ucls), o_ulist = pk.add(ulist);
     const size_t o_bs = pk.add(blk_shell), o_bo = pk.add(blk_oc), o_bco = pk.add(blk_cart_off), o_bso = pk.add(blk_sph_off),
-                 o_poffp = pk.add(proj_off);
+                 o_poffp = pk.add(proj_off), o_msch = pk.add(mmd_sched);
     std::vector<int8_t> stop_dummy;
     DevBuf *bin = own_buffers ? &P.in : &st.in, *bscr = own_buffers ? &P.scratch : &st.scratch,
            *bout = own_buffers ? &P.out : &st.out;
@@ -695,8 +753,9 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         m.smax = mmd_smax;
         m.status = statusd;
         m.counters = (unsigned long long *)(statusd + 16);
+        m.sched = at<uint16_t>(ib, o_msch);
         const int wpb = 4;
-        P.mmd_kpl = ncart(mmd_lmax) * ncart(mmd_lmax) <= 256 ? 8 : 32;
+        P.mmd_kpl = mmd_kpl;
         // per warp: the workspace, then 32 x KPL pair descriptors (8 bytes each)
         const size_t smem = (size_t)wpb * (mmd_ws_size(mmd_lmax, mmd_smax) + 32 * P.mmd_kpl) * sizeof(double);
         CHECK_INPUT(smem <= 200 * 1024, "type 1 workspace of this batch's angular momenta exceeds one block's shared memory");

@@ -31,6 +31,8 @@ struct MmdItem {
     int pot;             // potential index, or -1 for an overlap
     int out_kind;        // 0: arep output, 1: outercore U scratch, 2: outercore S scratch
     int64_t out_off;     // offset of the nbra x nket row-major block
+    int sched;           // offset of the item's Cartesian pair schedule (MmdArgs::sched)
+    int sched_rows;      // slot couples (2h, 2h+1) of the schedule in use
 };
 
 struct MmdArgs {
@@ -47,7 +49,14 @@ struct MmdArgs {
     int lmax;            // max l over the items
     int *status;
     unsigned long long *counters;  // kRadCntMmdTriples / kRadCntMmdFlops slots (may be null)
+    // per class of (bra, ket) Cartesian tables, 32 x KPL slots: slot (q, lane) at q * 32 + lane
+    // holds the pair index m * nket + n the lane owns in its q-th register, or kMmdNoPair. Slots
+    // (2h, 2h+1) of a lane hold pairs with equal (ax+bx, ay+by, az+bz), or one pair and an empty
+    // slot; the 32 lanes of a slot row hold pairs of equal or adjacent (ax+bx, ay+by, az+bz)
+    const uint16_t *sched;
 };
+constexpr uint16_t kMmdNoPair = 0xffff;
+
 
 // FP64 operations of one primitive triple, by phase (FMA = 2, exp/div/sqrt/pow = 1):
 // setup (q, 3 mu, 3 Q, 9 exponentials, K) 40; a Hermite coefficient 5; an auxiliary
@@ -81,6 +90,31 @@ __host__ __device__ inline int mmd_ws_size(int lmax, int smax)
 __device__ __forceinline__ int r0_row(int S, int t, int u)
 {
     return mmd_tet(S) - mmd_tet(S - t) + u * (S - t + 1) - u * (u - 1) / 2;
+}
+
+// sum_{t<=tx, u<=uy, v<=vz} E^x_t E^y_u E^z_v R^0_tuv for two pairs with equal (tx, uy, vz),
+// side by side on shared R^0 loads; each sum in the reference's (t, u, v) order
+__device__ __forceinline__ void mmd_contract2(const double *E, const double *R0, int S, int2 d0, int2 d1, double &s0,
+                                              double &s1)
+{
+    const int tx = (d0.y >> 16) & 31, uy = (d0.y >> 21) & 31, vz = (d0.y >> 26) & 31;
+    const int ox0 = d0.x & 0xffff, oy0 = (int)((unsigned)d0.x >> 16);
+    const int ox1 = d1.x & 0xffff, oy1 = (int)((unsigned)d1.x >> 16);
+    const double *ez0 = E + (d0.y & 0xffff), *ez1 = E + (d1.y & 0xffff);
+    s0 = 0.0;
+    s1 = 0.0;
+    for (int t = 0; t <= tx; t++) {
+        const double ex0 = E[ox0 + t], ex1 = E[ox1 + t];
+        for (int u = 0; u <= uy; u++) {
+            const double exy0 = ex0 * E[oy0 + u], exy1 = ex1 * E[oy1 + u];
+            const double *r0 = R0 + r0_row(S, t, u);
+            for (int v = 0; v <= vz; v++) {
+                const double rv = r0[v];
+                s0 += exy0 * ez0[v] * rv;
+                s1 += exy1 * ez1[v] * rv;
+            }
+        }
+    }
 }
 
 constexpr int kMmdMaxPairsPerLane = 32;  // up to 1024 Cartesian pairs per pass (KPL = 32 variant)
@@ -155,7 +189,8 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
         __syncwarp();
 
         const int npairs = nA * nB;
-        for (int pass = 0; pass < npairs; pass += 32 * KPL) {
+        {  // one pass over all pairs: npairs <= 32 x KPL (the host checks it)
+            const int pass = 0;
             // operations of one primitive triple's contraction over this pass's Cartesian pairs (counters)
             const int pend = min(npairs, pass + 32 * KPL);
             unsigned long long contract_fl = 0;
@@ -167,10 +202,16 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                 }
                 for (int o = 16; o > 0; o >>= 1) contract_fl += __shfl_xor_sync(0xffffffffu, contract_fl, o);
             }
+            const uint16_t *sch = a.sched + item.sched;
+            const int nslots = 2 * item.sched_rows;
 #pragma unroll
             for (int qq = 0; qq < KPL; qq++) {
-                const int pr = pass + lane + 32 * qq;
-                if (pr >= npairs) break;
+                if (qq >= nslots) break;
+                const int pr = sch[qq * 32 + lane];
+                if (pr == kMmdNoPair) {
+                    pdesc[qq * 32 + lane] = make_int2(0, -1);  // empty slot
+                    continue;
+                }
                 const int m = pr / nB, n = pr % nB;
                 const int ax = ca[3 * m], ay = ca[3 * m + 1], az = ca[3 * m + 2];
                 const int bx = cb[3 * n], by = cb[3 * n + 1], bz = cb[3 * n + 2];
@@ -318,31 +359,31 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                 }
                                 pref = npow == 1 ? NA * NB * 2.0 * kPi / q : NA * NB * 2.0 * kPi15 / sqrt(q);
                             }
-                            // ---- Cartesian pairs of this lane
+                            // ---- Cartesian pairs of this lane, by slot couples (2h, 2h+1) of equal
+                            // (tx, uy, vz); a lone pair runs with itself as partner, so every lane of a
+                            // row takes the same path
 #pragma unroll
-                            for (int qq = 0; qq < KPL; qq++) {
-                                const int pr = pass + lane + 32 * qq;
-                                if (pr >= npairs) break;
-                                const int2 dsc = pdesc[qq * 32 + lane];
-                                const int offx = dsc.x & 0xffff, offy = (int)((unsigned)dsc.x >> 16), offz = dsc.y & 0xffff;
-                                const int tx = (dsc.y >> 16) & 31, uy = (dsc.y >> 21) & 31, vz = (dsc.y >> 26) & 31;
-                                double buf;
+                            for (int h = 0; h < KPL; h += 2) {
+                                if (h >= nslots) break;
+                                const int2 d0 = pdesc[h * 32 + lane], d1 = pdesc[(h + 1) * 32 + lane];
+                                if (d0.y < 0) continue;
                                 if (npow == 2) {
-                                    buf = NA * NB * E[offx] * E[offy] * E[offz] * p15;
-                                } else {
-                                    double s = 0.0;
-                                    const double *ez = E + offz;
-                                    for (int t = 0; t <= tx; t++) {
-                                        const double ex = E[offx + t];
-                                        for (int u = 0; u <= uy; u++) {
-                                            const double exy = ex * E[offy + u];
-                                            const double *r0 = R0 + r0_row(S, t, u);
-                                            for (int v = 0; v <= vz; v++) s += exy * ez[v] * r0[v];
-                                        }
-                                    }
-                                    buf = s * pref;
+                                    accp[h] += (ci * cj) * (NA * NB * E[d0.x & 0xffff] * E[(int)((unsigned)d0.x >> 16)] *
+                                                            E[d0.y & 0xffff] * p15);
+                                    if (d1.y >= 0)
+                                        accp[h + 1] += (ci * cj) * (NA * NB * E[d1.x & 0xffff] *
+                                                                    E[(int)((unsigned)d1.x >> 16)] * E[d1.y & 0xffff] * p15);
+                                    continue;
                                 }
-                                accp[qq] += (ci * cj) * buf;
+                                const bool same = (d1.y >> 16) == (d0.y >> 16);  // false for an empty d1
+                                double s0, s1;
+                                mmd_contract2(E, R0, S, d0, same ? d1 : d0, s0, s1);
+                                accp[h] += (ci * cj) * (s0 * pref);
+                                if (same) accp[h + 1] += (ci * cj) * (s1 * pref);
+                                else if (d1.y >= 0) {  // unequal couple (not produced by the schedule builder)
+                                    mmd_contract2(E, R0, S, d1, d1, s0, s1);
+                                    accp[h + 1] += (ci * cj) * (s0 * pref);
+                                }
                             }
                         } else {
                             // ---- overlap: 1D Obara-Saika tables per axis (overlap.c:92-120)
@@ -376,9 +417,9 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                             }
 #pragma unroll
                             for (int qq = 0; qq < KPL; qq++) {
-                                const int pr = pass + lane + 32 * qq;
-                                if (pr >= npairs) break;
+                                if (qq >= nslots) break;
                                 const int2 dsc = pdesc[qq * 32 + lane];
+                                if (dsc.y < 0) continue;
                                 const double buf = NA * NB * E[dsc.x & 0xffff] * E[(int)((unsigned)dsc.x >> 16)] *
                                                    E[dsc.y & 0xffff];
                                 accp[qq] += (ci * cj) * buf;
@@ -393,8 +434,9 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
             }
 #pragma unroll
             for (int qq = 0; qq < KPL; qq++) {
-                const int pr = pass + lane + 32 * qq;
-                if (pr < npairs) out[pr] = res[qq];
+                if (qq >= nslots) break;
+                const int pr = sch[qq * 32 + lane];
+                if (pr != kMmdNoPair) out[pr] = res[qq];
             }
         }
         __syncwarp();
