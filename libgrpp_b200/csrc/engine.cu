@@ -216,6 +216,66 @@ static int mmd_pair_schedule(const int8_t *ca, int nA, const int8_t *cb, int nB,
     return (int)(units.size() + 31) / 32;
 }
 
+// Update programs of mmd_kernel's Hermite coefficients for every (la, lb) with la, lb <= lmax,
+// and of its R^n_tuv tables for every S = 1..smax (mmd_e_code / MmdArgs::rtab).
+static void mmd_update_tables(int lmax, int smax, std::vector<int> &etab, std::vector<int> &etab_off,
+                              std::vector<int2> &rtab, std::vector<int> &rtab_off)
+{
+    etab_off.assign((kMaxL + 1) * (kMaxL + 1), 0);
+    for (int la = 0; la <= lmax; la++)
+        for (int lb = 0; lb <= lmax; lb++) {
+            etab_off[la * (kMaxL + 1) + lb] = (int)etab.size();
+            const int S = la + lb, la1 = la + 1, lb1 = lb + 1, S1 = S + 1;
+            for (int w = 0; w <= S; w++) {
+                const int ilo = std::max(0, w - lb), ihi = std::min(la, w), per_axis = (ihi - ilo + 1) * (w + 1);
+                for (int e = 0; e < 3 * per_axis; e++) {
+                    const int ax = e / per_axis, r = e % per_axis, i = ilo + r / (w + 1), t = r % (w + 1), j = w - i;
+                    etab.push_back(mmd_e_code(((ax * la1 + i) * lb1 + j) * S1 + t, ax, i, j, t));
+                }
+            }
+        }
+    rtab_off.assign(2 * kMaxL + 1, 0);
+    for (int S = 1; S <= smax; S++) {
+        rtab_off[S] = (int)rtab.size();
+        std::vector<int> lvl(S + 1);
+        for (int s = 0, o = 0; s <= S; s++) {
+            lvl[s] = o;
+            o += (s + 1) * (s + 2) / 2 * (S - s + 1);
+        }
+        rtab.resize(rtab.size() + mmd_r_size(S), int2{0, 0});
+        int2 *tab = rtab.data() + rtab_off[S];
+        for (int s = 1; s <= S; s++) {
+            const int ne = (s + 1) * (s + 2) / 2, nn = S - s + 1, ne1 = s * (s + 1) / 2, ne2 = (s - 1) * s / 2;
+            const int o1 = lvl[s - 1], o2 = s >= 2 ? lvl[s - 2] : 0;
+            for (int e = 0; e < ne * nn; e++) {
+                const int n = e / ne, idx = e % ne;
+                int kk = 0;
+                while ((kk + 1) * (kk + 2) / 2 <= idx) kk++;
+                const int v = idx - kk * (kk + 1) / 2, u = kk - v, t = s - kk;
+                // step down along z if t = u = 0, else along y if t = 0, else along x
+                int uu = u, vv = v, kq, ax;
+                if (t + u == 0) {
+                    vv = v - 1;
+                    kq = v;
+                    ax = 2;
+                } else if (t == 0) {
+                    uu = u - 1;
+                    kq = u;
+                    ax = 1;
+                } else {
+                    kq = t;
+                    ax = 0;
+                }
+                const int src1 = o1 + n * ne1 + r_in_level(uu, vv);
+                int src2 = 0;
+                if (kq > 1) src2 = o2 + n * ne2 + r_in_level(uu == u ? u : u - 2, vv == v ? v : v - 2);
+                const int r0d = n == 0 ? r0_row(S, t, u) + v : kMmdNoR0;
+                tab[lvl[s] + e] = int2{src1 | (src2 << 16), kq | (ax << 5) | (r0d << 7)};
+            }
+        }
+    }
+}
+
 template <typename T>
 T *at(void *base, size_t off)
 {
@@ -649,6 +709,10 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         }
     }
 
+    std::vector<int> mmd_etab, mmd_etab_off, mmd_rtab_off;
+    std::vector<int2> mmd_rtab;
+    mmd_update_tables(mmd_lmax, mmd_smax, mmd_etab, mmd_etab_off, mmd_rtab, mmd_rtab_off);
+
     // angular tensors
     for (int L = 0; L <= kMaxL; L++)
         for (int l = 0; l <= kMaxL; l++)
@@ -681,6 +745,8 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
                  o_ucls = pk.add(ucls), o_ulist = pk.add(ulist);
     const size_t o_bs = pk.add(blk_shell), o_bo = pk.add(blk_oc), o_bco = pk.add(blk_cart_off), o_bso = pk.add(blk_sph_off),
                  o_poffp = pk.add(proj_off), o_msch = pk.add(mmd_sched);
+    const size_t o_met = pk.add(mmd_etab), o_meto = pk.add(mmd_etab_off), o_mrt = pk.add(mmd_rtab),
+                 o_mrto = pk.add(mmd_rtab_off);
     std::vector<int8_t> stop_dummy;
     DevBuf *bin = own_buffers ? &P.in : &st.in, *bscr = own_buffers ? &P.scratch : &st.scratch,
            *bout = own_buffers ? &P.out : &st.out;
@@ -754,6 +820,10 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         m.status = statusd;
         m.counters = (unsigned long long *)(statusd + 16);
         m.sched = at<uint16_t>(ib, o_msch);
+        m.etab = at<int>(ib, o_met);
+        m.etab_off = at<int>(ib, o_meto);
+        m.rtab = at<int2>(ib, o_mrt);
+        m.rtab_off = at<int>(ib, o_mrto);
         const int wpb = 4;
         P.mmd_kpl = mmd_kpl;
         // per warp: the workspace, then 32 x KPL pair descriptors (8 bytes each)

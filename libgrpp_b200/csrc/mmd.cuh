@@ -54,8 +54,35 @@ struct MmdArgs {
     // (2h, 2h+1) of a lane hold pairs with equal (ax+bx, ay+by, az+bz), or one pair and an empty
     // slot; the 32 lanes of a slot row hold pairs of equal or adjacent (ax+bx, ay+by, az+bz)
     const uint16_t *sched;
+    // update programs of the Hermite coefficients, per (la, lb) at etab_off[la * (kMaxL + 1) + lb]:
+    // one int per coefficient in wavefront order (see mmd_e_code); and of the R^n_tuv table, per
+    // S at rtab_off[S]: one int2 per entry of levels s >= 1, at the entry's own index (see mmd_r_code)
+    const int *etab, *etab_off;
+    const int2 *rtab;
+    const int *rtab_off;
 };
 constexpr uint16_t kMmdNoPair = 0xffff;
+
+// Hermite coefficient E[ax][i][j][t] (row-major over (ax, i, j, t), extents 3, la+1, lb+1, S+1):
+// bits 0-12 its index, 13-14 ax, 15-18 i, 19-22 j, 23-27 t, 28-30 the recurrence form
+// (type1_mcmurchie_davidson.c:569-622):
+//   0: K[ax] (i = j = 0)           1: (Q-A)[ax] E[ax][0][0][0] (i = 1, j = 0)
+//   2: (Q-B)[ax] E[ax][0][0][0] (i = 0, j = 1)
+//   3: (Q-B)[ax] E[ax][0][j-1][0] + E[ax][0][j-1][1] (i = 0, j >= 2)
+//   4: (Q-A)[ax] E[ax][i-1][j][0] + E[ax][i-1][j][1] (other t = 0)
+//   5: (i E[ax][i-1][j][t-1] + j E[ax][i][j-1][t-1]) / (2 q t) (t >= 1), each term as f i E
+__host__ __device__ inline int mmd_e_code(int dst, int ax, int i, int j, int t)
+{
+    int ty;
+    if (t > 0) ty = 5;
+    else if (i == 0 && j == 0) ty = 0;
+    else if (i == 1 && j == 0) ty = 1;
+    else if (i == 0 && j == 1) ty = 2;
+    else if (i == 0) ty = 3;
+    else ty = 4;
+    return dst | (ax << 13) | (i << 15) | (j << 19) | (t << 23) | (ty << 28);
+}
+constexpr int kMmdNoR0 = 4095;  // R^n_tuv entry with n > 0: not an R^0 value
 
 
 // FP64 operations of one primitive triple, by phase (FMA = 2, exp/div/sqrt/pow = 1):
@@ -83,11 +110,12 @@ constexpr double kPi15 = 5.568327996831708;  // pi^(3/2), correctly rounded
 __host__ __device__ inline int mmd_tet(int m) { return (m + 1) * (m + 2) * (m + 3) / 6; }
 __host__ __device__ inline int mmd_ws_size(int lmax, int smax)
 {
-    return mmd_e_size(lmax) + mmd_r_size(smax) + mmd_tet(smax) + 2 * (smax + 2) + 16 + 2 * kMmdMaxPrims;
+    return mmd_e_size(lmax) + mmd_r_size(smax) + mmd_tet(smax) + 2 * (smax + 2) + 16 + 2 * kMmdMaxPrims + 12 +
+           (smax + 1);
 }
 
 // start of row (t, u) in the R^0 layout: rows ordered t-major, then u
-__device__ __forceinline__ int r0_row(int S, int t, int u)
+__host__ __device__ __forceinline__ int r0_row(int S, int t, int u)
 {
     return mmd_tet(S) - mmd_tet(S - t) + u * (S - t + 1) - u * (u - 1) / 2;
 }
@@ -133,7 +161,7 @@ __device__ __forceinline__ int r_level_off(int S, int s)
 }
 
 // index of (u+v = k, v) within level s: tri(k) + v
-__device__ __forceinline__ int r_in_level(int u, int v) { return (u + v) * (u + v + 1) / 2 + v; }
+__host__ __device__ __forceinline__ int r_in_level(int u, int v) { return (u + v) * (u + v + 1) / 2 + v; }
 
 // KPL: Cartesian pairs held per lane per pass (8: up to 256 pairs, 32: up to 1024)
 // COUNT: keep the operation counters (a separate instantiation, so the timed kernel carries none)
@@ -150,6 +178,8 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
     double *aux = R0 + mmd_tet(a.smax);
     int *lvl = (int *)(aux + (a.smax + 2));
     double *normA = aux + 2 * (a.smax + 2) + 16, *normB = normA + kMmdMaxPrims;  // per item
+    // per primitive triple: (Q-A)[3], (Q-B)[3], K[3], (Q-C)[3], then 1/(2 q t) for t = 1..S
+    double *sQA = normB + kMmdMaxPrims, *sQB = sQA + 3, *sK = sQB + 3, *sQC = sK + 3, *finv = sQC + 3;
     // lane-private descriptors of the Cartesian pairs of the current pass (after all warps'
     // workspaces): x = E row of axis x | E row of axis y << 16, y = E row of axis z |
     // (ax+bx) << 16 | (ay+by) << 21 | (az+bz) << 26 — each pair is decoded once per pass,
@@ -277,30 +307,46 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                 else
                                     c_fl += 4ull * (pend - pass);
                             }
-                            for (int w = 0; w <= S; w++) {
+                            // per-triple scalars shared by the coefficient updates (the same
+                            // expressions the updates would evaluate)
+                            if (lane < 3) {
+                                const double Qd = lane == 0 ? Q[0] : (lane == 1 ? Q[1] : Q[2]);
+                                const double Ad = lane == 0 ? A[0] : (lane == 1 ? A[1] : A[2]);
+                                const double Bd = lane == 0 ? B[0] : (lane == 1 ? B[1] : B[2]);
+                                const double Cd = lane == 0 ? C[0] : (lane == 1 ? C[1] : C[2]);
+                                sQA[lane] = Qd - Ad;
+                                sQB[lane] = Qd - Bd;
+                                sQC[lane] = Qd - Cd;
+                                sK[lane] = lane == 0 ? K[0] : (lane == 1 ? K[1] : K[2]);
+                            }
+                            if (lane >= 1 && lane <= S) finv[lane] = 1.0 / (2.0 * q * lane);
+                            __syncwarp();
+                            const int *ecode = a.etab + __ldg(a.etab_off + la * (kMaxL + 1) + lb);
+                            const int sj = S1, si = lb1 * S1;  // index steps of j and i
+                            for (int w = 0, wo = 0; w <= S; w++) {
                                 // entries (axis, i, j=w-i, t<=w)
                                 const int ilo = max(0, w - lb), ihi = min(la, w);
-                                const int ni = ihi - ilo + 1, per_axis = ni * (w + 1), tot = 3 * per_axis;
+                                const int tot = 3 * (ihi - ilo + 1) * (w + 1);
                                 for (int e = lane; e < tot; e += 32) {
-                                    const int ax = e / per_axis, r = e % per_axis;
-                                    const int ii = ilo + r / (w + 1), t = r % (w + 1), jj = w - ii;
+                                    const int c = __ldg(ecode + wo + e);
+                                    const int dst = c & 8191, ax = (c >> 13) & 3, ty = c >> 28;
+                                    const int e000 = ax * la1 * lb1 * S1;
                                     double v;
-                                    if (t == 0) {
-                                        if (ii == 0 && jj == 0) v = K[ax];
-                                        else if (ii == 1 && jj == 0) v = (Q[ax] - A[ax]) * E[eidx(lb1, S1, ax, 0, 0, 0, la1)];
-                                        else if (ii == 0 && jj == 1) v = (Q[ax] - B[ax]) * E[eidx(lb1, S1, ax, 0, 0, 0, la1)];
-                                        else if (ii == 0)
-                                            v = (Q[ax] - B[ax]) * E[eidx(lb1, S1, ax, ii, jj - 1, 0, la1)] + E[eidx(lb1, S1, ax, ii, jj - 1, 1, la1)];
-                                        else
-                                            v = (Q[ax] - A[ax]) * E[eidx(lb1, S1, ax, ii - 1, jj, 0, la1)] + E[eidx(lb1, S1, ax, ii - 1, jj, 1, la1)];
-                                    } else {
-                                        const double f = 1.0 / (2.0 * q * t);
+                                    if (ty == 0) v = sK[ax];
+                                    else if (ty == 1) v = sQA[ax] * E[e000];
+                                    else if (ty == 2) v = sQB[ax] * E[e000];
+                                    else if (ty == 3) v = sQB[ax] * E[dst - sj] + E[dst - sj + 1];
+                                    else if (ty == 4) v = sQA[ax] * E[dst - si] + E[dst - si + 1];
+                                    else {
+                                        const int ii = (c >> 15) & 15, jj = (c >> 19) & 15, t = (c >> 23) & 31;
+                                        const double f = finv[t];
                                         v = 0.0;
-                                        if (ii > 0) v += f * ii * E[eidx(lb1, S1, ax, ii - 1, jj, t - 1, la1)];
-                                        if (jj > 0) v += f * jj * E[eidx(lb1, S1, ax, ii, jj - 1, t - 1, la1)];
+                                        if (ii > 0) v += f * ii * E[dst - si - 1];
+                                        if (jj > 0) v += f * jj * E[dst - sj - 1];
                                     }
-                                    E[eidx(lb1, S1, ax, ii, jj, t, la1)] = v;
+                                    E[dst] = v;
                                 }
+                                wo += tot;
                                 __syncwarp();
                             }
                             const double p15 = npow == 2 ? pow(kPi / q, 1.5) : 0.0;  // once per primitive triple
@@ -308,7 +354,6 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                 pref = 0.0;
                             } else {
                                 // ---- auxiliary functions and R by levels (type1_mcmurchie_davidson.c:457-564)
-                                const double QC[3] = {Q[0] - C[0], Q[1] - C[1], Q[2] - C[2]};
                                 const double dx = Q[0] - C[0], dy = Q[1] - C[1], dz = Q[2] - C[2];
                                 const double x = q * (dx * dx + dy * dy + dz * dz);
                                 if (npow == 1) {
@@ -322,38 +367,28 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                 if (lane <= S) R[lane] = pow(q2, lane) * aux[lane];  // level 0: n = 0..S
                                 if (lane == 0) R0[0] = R[0];
                                 __syncwarp();
+                                const int2 *rcode = a.rtab + __ldg(a.rtab_off + S);
                                 for (int s = 1; s <= S; s++) {
                                     const int ne = (s + 1) * (s + 2) / 2, nn = S - s + 1, tot = ne * nn;
-                                    const int o = lvl[s], o1 = lvl[s - 1], o2 = s >= 2 ? lvl[s - 2] : 0;
-                                    const int ne1 = s * (s + 1) / 2, ne2 = (s - 1) * s / 2;
+                                    const int o = lvl[s], ne1 = s * (s + 1) / 2, ne2 = (s - 1) * s / 2;
                                     for (int e = lane; e < tot; e += 32) {
-                                        const int n = e / ne, idx = e % ne;
-                                        // decode idx -> (u+v = kk, v), t = s - kk
-                                        int kk = (int)((sqrtf((float)(8 * idx + 1)) - 1.0f) * 0.5f);  // corrected below
-                                        while ((kk + 1) * (kk + 2) / 2 <= idx) kk++;
-                                        while (kk * (kk + 1) / 2 > idx) kk--;
-                                        const int v = idx - kk * (kk + 1) / 2, u = kk - v, t = s - kk;
-                                        int tt = t, uu = u, vv = v, kq;
-                                        double X;
-                                        if (t + u == 0) { vv = v - 1; kq = v; X = QC[2]; }
-                                        else if (t == 0) { uu = u - 1; kq = u; X = QC[1]; }
-                                        else { tt = t - 1; kq = t; X = QC[0]; }
-                                        // previous-level element (t-1|u-1|v-1) and (t-2|u-2|v-2)
-                                        const int i1 = r_in_level(uu, vv);
-                                        const double r1n1 = R[o1 + (n + 1) * ne1 + i1], r1n = R[o1 + n * ne1 + i1];
+                                        // entry (t, u, v) of order n from its step down along one axis
+                                        // (the first of z, y, x with t+u, t, ... as in the reference)
+                                        const int2 c = __ldg(rcode + o + e);
+                                        const int src1 = c.x & 0xffff, src2 = (int)((unsigned)c.x >> 16);
+                                        const int kq = c.y & 31, ax = (c.y >> 5) & 3, r0d = (c.y >> 7) & 4095;
+                                        const double X = sQC[ax];
+                                        const double r1n1 = R[src1 + ne1], r1n = R[src1];
                                         double val = 0.0;
                                         if (kq > 1) {
-                                            const int t2 = (tt == t) ? t : t - 2, u2 = (uu == u) ? u : u - 2, v2 = (vv == v) ? v : v - 2;
-                                            const int i2 = r_in_level(u2, v2);
-                                            const double r2n1 = R[o2 + (n + 1) * ne2 + i2], r2n = R[o2 + n * ne2 + i2];
-                                            (void)t2;
+                                            const double r2n1 = R[src2 + ne2], r2n = R[src2];
                                             if (isg) val += (kq - 1) * (r2n1 - 2.0 * q * r2n);
                                             else val += (kq - 1) * r2n1;
                                         }
                                         if (isg) val += X * (r1n1 - 2.0 * q * r1n);
                                         else val += X * r1n1;
-                                        R[o + n * ne + idx] = val;
-                                        if (n == 0) R0[r0_row(S, t, u) + v] = val;
+                                        R[o + e] = val;
+                                        if (r0d != kMmdNoR0) R0[r0d] = val;
                                     }
                                     __syncwarp();
                                 }
