@@ -121,6 +121,7 @@ int init_device_state(DeviceState &st, int device)
     const HostTables &h = g_host;
     DeviceTables d;
     GRPP_CUDA(upload_vec(st, h.bessel, &d.bessel));
+    GRPP_CUDA(upload_vec(st, h.bessel_p, &d.bessel_p));
     GRPP_CUDA(upload_vec(st, h.rfun, &d.rfun));
     GRPP_CUDA(upload_vec(st, h.boys, &d.boys));
     GRPP_CUDA(upload_vec(st, h.dawson, &d.dawson));

@@ -12,7 +12,7 @@ namespace grpp {
 
 // ---- limits ------------------------------------------------------------------
 constexpr int kMaxL = 10;          // basis and projector angular momentum (libgrpp.h:16-21), +1 for gradients
-constexpr int kBesL = 40;          // Bessel table orders 0..kBesL-1
+constexpr int kBesL = 40;          // Bessel table orders 0..kBesL-1 (even: the pair layout)
 constexpr int kBesNX = 1601;       // x = 0.00 .. 16.00 step 0.01 (specfunc_bessel_table.c:14-17)
 constexpr int kRfunL = 40;         // asymptotic R_l coefficients (specfunc_scaled_mod_sph_bessel.c:163-190)
 constexpr int kBoysNX = 301;       // x = 0.0 .. 30.0 step 0.1 (specfunc_boys.c:24)
@@ -28,6 +28,7 @@ constexpr double kZeroThresh = 1e-14;  // LIBGRPP_ZERO_THRESH
 
 struct DeviceTables {
     const double *bessel;     // [kBesNX][kBesL][5]: value + 4 derivatives
+    const double *bessel_p;   // the same values as [kBesNX][kBesL/2][5][2]: orders 2p, 2p+1 side by side
     const double *rfun;       // [kRfunL][kRfunL]
     const double *boys;       // [kBoysNX][kBoysNN]
     const double *dawson;     // [kDawNY]

@@ -64,6 +64,7 @@ constexpr size_t kNaRsh = 320705, kNaComb = 6545 * 3, kNaLmat = 6900;
 
 static __device__ __align__(256) unsigned char g_scratch[kNoAllocScratchBytes];
 static __device__ double g_bessel[kNaBessel];
+static __device__ __align__(16) double g_bessel_p[kNaBessel];
 static __device__ double g_rfun[kRfunL * kRfunL];
 static __device__ double g_boys[kBoysNX * kBoysNN];
 static __device__ double g_dawson[kDawNY];
@@ -122,6 +123,7 @@ int setup(int dev)
     DeviceTables d;
     int rc = 0;
     if ((rc = copy_table(g_bessel, h.bessel, kNaBessel, &d.bessel))) return rc;
+    if ((rc = copy_table(g_bessel_p, h.bessel_p, kNaBessel, &d.bessel_p))) return rc;
     if ((rc = copy_table(g_rfun, h.rfun, (size_t)kRfunL * kRfunL, &d.rfun))) return rc;
     if ((rc = copy_table(g_boys, h.boys, (size_t)kBoysNX * kBoysNN, &d.boys))) return rc;
     if ((rc = copy_table(g_dawson, h.dawson, (size_t)kDawNY, &d.dawson))) return rc;

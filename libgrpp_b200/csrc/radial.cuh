@@ -642,13 +642,18 @@ __device__ __forceinline__ void bessel_row_acc(int lmax, double x, double e, dou
         const int i0 = (int)(round(x * 100) + 1e-5);
         const double dx = x - i0 * 0.01;
         const double dx2 = dx * dx, dx3 = dx2 * dx, dx4 = dx3 * dx;
-        const double *d = c_tab.bessel + (size_t)i0 * kBesL * 5;
+        // orders l, l+1 from one 80-byte block of the pair layout: five 16-byte loads
+        const double2 *d = reinterpret_cast<const double2 *>(c_tab.bessel_p) + (size_t)i0 * kBesL * 5 / 2;
 #pragma unroll 1
-        for (int l = 0; l <= lmax; l++) {
-            const double *q = d + 5 * l;
-            const double m = __ldg(q) + __ldg(q + 1) * dx + __ldg(q + 2) * dx2 * 0.5 + __ldg(q + 3) * dx3 * (1.0 / 6.0) +
-                             __ldg(q + 4) * dx4 * (1.0 / 24.0);
-            dst[l * stride] += e * m;
+        for (int l = 0; l <= lmax; l += 2) {
+            const double2 *q = d + 5 * (l / 2);
+            const double2 c0 = __ldg(q), c1 = __ldg(q + 1), c2 = __ldg(q + 2), c3 = __ldg(q + 3), c4 = __ldg(q + 4);
+            const double m0 = c0.x + c1.x * dx + c2.x * dx2 * 0.5 + c3.x * dx3 * (1.0 / 6.0) + c4.x * dx4 * (1.0 / 24.0);
+            dst[l * stride] += e * m0;
+            if (l < lmax) {
+                const double m1 = c0.y + c1.y * dx + c2.y * dx2 * 0.5 + c3.y * dx3 * (1.0 / 6.0) + c4.y * dx4 * (1.0 / 24.0);
+                dst[(l + 1) * stride] += e * m1;
+            }
         }
     } else {
 #pragma unroll 1

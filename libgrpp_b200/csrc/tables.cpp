@@ -147,12 +147,19 @@ void build_host_tables(HostTables &t)
     t.bessel.assign((size_t)kBesNX * kBesL * 5, 0.0);
     for (int i = 0; i < kBesNX; i++)
         memcpy(&t.bessel[(size_t)i * kBesL * 5], &v[(size_t)i * LV * 5], kBesL * 5 * sizeof(double));
+    // pair layout: per x, per order pair p, coefficient k of orders 2p and 2p+1 side by side
+    static_assert(kBesL % 2 == 0, "the pair layout needs an even number of orders");
+    t.bessel_p.assign(t.bessel.size(), 0.0);
+    for (int i = 0; i < kBesNX; i++)
+        for (int l = 0; l < kBesL; l++)
+            for (int k = 0; k < 5; k++)
+                t.bessel_p[(size_t)i * kBesL * 5 + (l / 2) * 10 + 2 * k + (l % 2)] = t.bessel[((size_t)i * kBesL + l) * 5 + k];
 
     t.rfun.assign(kRfunL * kRfunL, 0.0);
     for (int n = 0; n < kRfunL; n++)
         for (int k = 0; k <= n; k++) {
             long double c = 1.0L;
-            for (int j = n - k + 1; j <= n + k; j++) c *= j;
+            for (int q = 0; q < 2 * k; q++) c *= (long double)(n - k + 1 + q);  // (n+k)! / (n-k)!
             for (int j = 1; j <= k; j++) c /= 2.0L * j;
             t.rfun[n * kRfunL + k] = (double)c;
         }

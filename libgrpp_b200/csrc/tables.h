@@ -7,7 +7,7 @@
 namespace grpp {
 
 struct HostTables {
-    std::vector<double> bessel, rfun, boys, dawson, rsh_coef, lmat, dfact, binom;
+    std::vector<double> bessel, bessel_p, rfun, boys, dawson, rsh_coef, lmat, dfact, binom;
     std::vector<int> rsh_off, rsh_comb_off, lmat_off;
     std::vector<int8_t> rsh_comb;
 };
