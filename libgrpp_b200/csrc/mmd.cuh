@@ -111,7 +111,7 @@ __host__ __device__ inline int mmd_tet(int m) { return (m + 1) * (m + 2) * (m + 
 __host__ __device__ inline int mmd_ws_size(int lmax, int smax)
 {
     return mmd_e_size(lmax) + mmd_r_size(smax) + mmd_tet(smax) + 2 * (smax + 2) + 16 + 2 * kMmdMaxPrims + 12 +
-           (smax + 1);
+           (smax + 1) + 7 * 32;
 }
 
 // start of row (t, u) in the R^0 layout: rows ordered t-major, then u
@@ -180,6 +180,8 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
     double *normA = aux + 2 * (a.smax + 2) + 16, *normB = normA + kMmdMaxPrims;  // per item
     // per primitive triple: (Q-A)[3], (Q-B)[3], K[3], (Q-C)[3], then 1/(2 q t) for t = 1..S
     double *sQA = normB + kMmdMaxPrims, *sQB = sQA + 3, *sK = sQB + 3, *sQC = sK + 3, *finv = sQC + 3;
+    // per chunk of 32 primitive pairs, lane l's pair: q, Q[3], K[3] at spre[v * 32 + l]
+    double *spre = finv + (a.smax + 1);
     // lane-private descriptors of the Cartesian pairs of the current pass (after all warps'
     // workspaces): x = E row of axis x | E row of axis y << 16, y = E row of axis z |
     // (ax+bx) << 16 | (ay+by) << 21 | (az+bz) << 26 — each pair is decoded once per pass,
@@ -260,44 +262,56 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
 #pragma unroll
                 for (int q = 0; q < KPL; q++) accp[q] = 0.0;
 
-                for (int i = 0; i < npA; i++) {
-                    const double ci = cA[i];
-                    if (fabs(ci) < kZeroThresh && !overlap) continue;
-                    for (int j = 0; j < npB; j++) {
-                        const double cj = cB[j];
-                        if (fabs(cj) < kZeroThresh && !overlap) continue;
+                // primitive pairs (i, j) in the reference's order, 32 at a time: first each lane
+                // evaluates the scalars of one pair (q, Q, the Gaussian factors K per axis,
+                // K[d] = e(d,ab) e(d,ac) e(d,bc)); pairs with a zero coefficient (|c| < 1e-14)
+                // or a K[d] that underflowed to exactly 0 add exact zeros and are dropped
+                const int np2 = npA * npB;
+                for (int base = 0; base < np2; base += 32) {
+                    const int rr = base + lane;
+                    bool live = false;
+                    __syncwarp();  // the previous chunk's readers of spre are done
+                    if (rr < np2) {
+                        const int i = rr / npB, j = rr - i * npB;
+                        if (overlap) {
+                            live = true;
+                        } else if (!(fabs(cA[i]) < kZeroThresh) && !(fabs(cB[j]) < kZeroThresh)) {
+                            const double al = xA[i], be = xB[j];
+                            const double q = al + be + zeta;
+                            const double muab = (al * be) / q, muac = (al * zeta) / q, mubc = (be * zeta) / q;
+                            spre[lane] = q;
+#pragma unroll
+                            for (int d = 0; d < 3; d++) {
+                                // each product rounded, as the reference's (a A + b B + c C) / q
+                                // (type1_mcmurchie_davidson.c:198); no contraction into an FMA
+                                spre[(1 + d) * 32 + lane] =
+                                    __dadd_rn(__dadd_rn(__dmul_rn(al, A[d]), __dmul_rn(be, B[d])), __dmul_rn(zeta, C[d])) / q;
+                                const double dab = A[d] - B[d], dac = A[d] - C[d], dbc = B[d] - C[d];
+                                const double Kd = exp(-muab * dab * dab) * exp(-muac * dac * dac) * exp(-mubc * dbc * dbc);
+                                spre[(4 + d) * 32 + lane] = Kd;
+                                live = d == 0 ? Kd != 0.0 : (live && Kd != 0.0);
+                            }
+                        }
+                    }
+                    unsigned live_mask = __ballot_sync(0xffffffffu, live);
+                    __syncwarp();
+                    while (live_mask) {
+                        const int bl = __ffs(live_mask) - 1;
+                        live_mask &= live_mask - 1;
+                        const int i = (base + bl) / npB, j = (base + bl) - i * npB;
+                        const double ci = cA[i], cj = cB[j];
                         const double al = xA[i], be = xB[j];
                         const double NA = normA[i], NB = normB[j];
                         double pref;
                         if (!overlap) {
                             // ---- Hermite E by wavefronts (type1_mcmurchie_davidson.c:569-622)
-                            const double q = al + be + zeta;
-                            // the same scalars as every lane computing them, one per lane:
-                            // lanes 0-2 the three mu, lanes 3-5 Q[x,y,z]; then lanes 0-8 the nine
-                            // exponentials, K[d] = e(d,ab) e(d,ac) e(d,bc) in that order
-                            double sc = 0.0;
-                            if (lane < 3) sc = (lane == 0 ? al * be : (lane == 1 ? al * zeta : be * zeta)) / q;
-                            else if (lane < 6) sc = (al * A[lane - 3] + be * B[lane - 3] + zeta * C[lane - 3]) / q;
-                            const double muab = __shfl_sync(0xffffffffu, sc, 0), muac = __shfl_sync(0xffffffffu, sc, 1),
-                                         mubc = __shfl_sync(0xffffffffu, sc, 2);
+                            const double q = spre[bl];
                             double Q[3], K[3];
-                            Q[0] = __shfl_sync(0xffffffffu, sc, 3);
-                            Q[1] = __shfl_sync(0xffffffffu, sc, 4);
-                            Q[2] = __shfl_sync(0xffffffffu, sc, 5);
-                            double ev = 0.0;
-                            if (lane < 9) {
-                                const int d = lane / 3, m = lane % 3;
-                                const double dd = m == 0 ? A[d] - B[d] : (m == 1 ? A[d] - C[d] : B[d] - C[d]);
-                                const double mu = m == 0 ? muab : (m == 1 ? muac : mubc);
-                                ev = exp(-mu * dd * dd);
-                            }
 #pragma unroll
-                            for (int d = 0; d < 3; d++)
-                                K[d] = __shfl_sync(0xffffffffu, ev, 3 * d) * __shfl_sync(0xffffffffu, ev, 3 * d + 1) *
-                                       __shfl_sync(0xffffffffu, ev, 3 * d + 2);
-                            // K[d] scales every Hermite coefficient of axis d: when one underflowed to
-                            // exactly 0 the triple adds exact zeros (warp-uniform test)
-                            if (K[0] == 0.0 || K[1] == 0.0 || K[2] == 0.0) continue;
+                            for (int d = 0; d < 3; d++) {
+                                Q[d] = spre[(1 + d) * 32 + bl];
+                                K[d] = spre[(4 + d) * 32 + bl];
+                            }
                             if (COUNT && lane == 0) {
                                 c_trip++;
                                 c_fl += 40 + 5 * mmd_e_count(la, lb);
