@@ -77,13 +77,37 @@ struct DevBuf {
     }
 };
 
+// page-locked host staging buffer (uploads that do not wait for the stream)
+struct PinBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n)
+    {
+        if (n <= cap) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        const size_t want = std::max<size_t>(n + n / 4, 1 << 20);
+        cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+};
+
+// Two buffer sets: a batch larger than one chunk alternates between them, so the host
+// prepares and uploads chunk c+1 and downloads chunk c-1 while the GPU runs chunk c.
 struct DeviceState {
     int device = -1;
     bool ready = false;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev[6];
+    cudaStream_t stream = nullptr;       // all kernels and uploads
+    cudaStream_t copy_stream = nullptr;  // downloads of finished chunks
+    cudaEvent_t ev[2][6];                // per buffer set: phase boundaries of one execution
+    cudaEvent_t done[2];                 // per buffer set: execution and its status copy finished
+    cudaEvent_t uploaded[2];             // per buffer set: the staging buffer's last upload finished
     std::vector<void *> table_bufs;
-    DevBuf in, scratch, out;
+    DevBuf in[2], scratch[2], out[2];
+    PinBuf stage[2];                     // upload staging per buffer set
+    int *hstat[2] = {nullptr, nullptr};  // page-locked status words + counters per buffer set
     DevBuf atab;
     size_t atab_used = 0;
     // learned grid-level model (libgrpp_b200_set_level_model): FP32 normalisation, BF16 weights
@@ -91,6 +115,7 @@ struct DeviceState {
     __nv_bfloat16 *lm_w = nullptr;
     bool lm_ready = false;
     std::vector<int64_t> atab_off;
+    bool atab_dirty = true;  // atab_off has entries the device copy lacks
     DevBuf atab_off_dev;
     std::mutex mu;
 };
@@ -135,7 +160,14 @@ int init_device_state(DeviceState &st, int device)
     GRPP_CUDA(upload_vec(st, h.binom, &d.binom));
     GRPP_CUDA(cudaMemcpyToSymbol(c_tab, &d, sizeof(d)));
     GRPP_CUDA(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking));
-    for (auto &e : st.ev) GRPP_CUDA(cudaEventCreate(&e));
+    GRPP_CUDA(cudaStreamCreateWithFlags(&st.copy_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; k++) {
+        for (auto &e : st.ev[k]) GRPP_CUDA(cudaEventCreate(&e));
+        GRPP_CUDA(cudaEventCreateWithFlags(&st.done[k], cudaEventDisableTiming));
+        GRPP_CUDA(cudaEventCreateWithFlags(&st.uploaded[k], cudaEventDisableTiming));
+        GRPP_CUDA(cudaHostAlloc((void **)&st.hstat[k], 16 * sizeof(int) + kRadCntNum * sizeof(unsigned long long),
+                                cudaHostAllocDefault));
+    }
     st.atab_off.assign((kMaxL + 2) * (kMaxL + 2), -1);
     GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -396,6 +428,7 @@ int ensure_atab(DeviceState &st, int L, int l)
     GRPP_CUDA(cudaGetLastError());
     st.atab_off[key] = (int64_t)st.atab_used;
     st.atab_used += sz;
+    st.atab_dirty = true;
     return 0;
 }
 
@@ -403,6 +436,7 @@ int ensure_atab(DeviceState &st, int L, int l)
 
 struct Plan {
     DeviceState *st = nullptr;
+    int set = 0;  // buffer set, events and status words of the device state it uses
     RunOptions opt;
     int64_t n_tasks = 0, out_tot = 0, n_radial = 0, n_mmd = 0, n_entries = 0, h2d_bytes = 0, scratch_bytes = 0;
     DevBuf in, scratch, out;
@@ -445,12 +479,14 @@ int64_t batch_output_size(const libgrpp_b200_batch_t *b)
 // Host preprocessing, upload and kernel arguments of one batch. With own_buffers the
 // plan allocates its device memory (kept until plan_destroy); otherwise it borrows the
 // device state's buffers and is valid until the next batch on that device.
-int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions &opt, bool own_buffers, Plan &P)
+int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions &opt, bool own_buffers, Plan &P,
+               int set = 0)
 {
     int rc = 0;
     cudaStream_t s = st.stream;
     const int64_t nt = b->n_tasks;
     P.st = &st;
+    P.set = set;
     P.n_tasks = nt;
     P.opt = opt;
     if (nt == 0) return 0;
@@ -722,9 +758,13 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         rc = ensure_atab(st, lp.first, lp.second);
         if (rc) return rc;
     }
-    GRPP_CUDA(st.atab_off_dev.ensure(st.atab_off.size() * sizeof(int64_t)));
-    GRPP_CUDA(cudaMemcpyAsync(st.atab_off_dev.p, st.atab_off.data(), st.atab_off.size() * sizeof(int64_t),
-                              cudaMemcpyHostToDevice, s));
+    if (st.atab_dirty) {  // offsets of newly built tables (existing offsets never change)
+        GRPP_CUDA(st.atab_off_dev.ensure(st.atab_off.size() * sizeof(int64_t)));
+        GRPP_CUDA(cudaMemcpyAsync(st.atab_off_dev.p, st.atab_off.data(), st.atab_off.size() * sizeof(int64_t),
+                                  cudaMemcpyHostToDevice, s));
+        GRPP_CUDA(cudaStreamSynchronize(s));
+        st.atab_dirty = false;
+    }
 
     // ---------------------------------------------------------------- upload
     std::vector<int> sh_po_v(sh_po), cart_off_v(sh_co);
@@ -749,10 +789,15 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     const size_t o_met = pk.add(mmd_etab), o_meto = pk.add(mmd_etab_off), o_mrt = pk.add(mmd_rtab),
                  o_mrto = pk.add(mmd_rtab_off);
     std::vector<int8_t> stop_dummy;
-    DevBuf *bin = own_buffers ? &P.in : &st.in, *bscr = own_buffers ? &P.scratch : &st.scratch,
-           *bout = own_buffers ? &P.out : &st.out;
+    DevBuf *bin = own_buffers ? &P.in : &st.in[set], *bscr = own_buffers ? &P.scratch : &st.scratch[set],
+           *bout = own_buffers ? &P.out : &st.out[set];
     GRPP_CUDA(bin->ensure(pk.buf.size()));
-    GRPP_CUDA(cudaMemcpyAsync(bin->p, pk.buf.data(), pk.buf.size(), cudaMemcpyHostToDevice, s));
+    // through the set's page-locked staging buffer, once its previous upload has finished
+    GRPP_CUDA(cudaEventSynchronize(st.uploaded[set]));
+    GRPP_CUDA(st.stage[set].ensure(pk.buf.size()));
+    memcpy(st.stage[set].p, pk.buf.data(), pk.buf.size());
+    GRPP_CUDA(cudaMemcpyAsync(bin->p, st.stage[set].p, pk.buf.size(), cudaMemcpyHostToDevice, s));
+    GRPP_CUDA(cudaEventRecord(st.uploaded[set], s));
     P.h2d_bytes = (int64_t)pk.buf.size();
     void *ib = bin->p;
 
@@ -987,13 +1032,15 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     return 0;
 }
 
-int plan_execute(Plan &P)
+// Enqueue one execution of a plan on the state's stream (no host synchronisation).
+int plan_launch(Plan &P)
 {
     DeviceState &st = *P.st;
     cudaStream_t s = st.stream;
+    cudaEvent_t *ev = st.ev[P.set];
     if (P.n_tasks == 0) return 0;
     GRPP_CUDA(cudaMemsetAsync(P.status, 0, 16 * sizeof(int) + kRadCntNum * sizeof(unsigned long long), s));
-    GRPP_CUDA(cudaEventRecord(st.ev[0], s));
+    GRPP_CUDA(cudaEventRecord(ev[0], s));
     if (P.mmd_blocks > 0) {
         if (P.count_ops) {
             if (P.mmd_kpl == 8) mmd_kernel<8, true><<<P.mmd_blocks, P.mmd_threads, P.mmd_smem, s>>>(P.mmd);
@@ -1004,7 +1051,7 @@ int plan_execute(Plan &P)
         }
         GRPP_CUDA(cudaGetLastError());
     }
-    GRPP_CUDA(cudaEventRecord(st.ev[1], s));
+    GRPP_CUDA(cudaEventRecord(ev[1], s));
     if (P.ocp_blocks > 0) {
         oc_proj_kernel<<<P.ocp_blocks, 64, 0, s>>>(P.ocp);
         GRPP_CUDA(cudaGetLastError());
@@ -1016,7 +1063,7 @@ int plan_execute(Plan &P)
             radial_screen_flat_kernel<<<P.scr_blocks, kRadThreads, 0, s>>>(P.rad);
             GRPP_CUDA(cudaGetLastError());
         }
-        GRPP_CUDA(cudaEventRecord(st.ev[4], s));
+        GRPP_CUDA(cudaEventRecord(ev[4], s));
         RadialArgs ra = P.rad;
         if (P.opt.radial_mode == LIBGRPP_B200_RADIAL_LEARNED) {
             if (!st.lm_ready) {
@@ -1033,29 +1080,40 @@ int plan_execute(Plan &P)
             GRPP_CUDA(cudaGetLastError());
             ra.order = P.order;
             ra.pred_level = P.pred_level;
-            GRPP_CUDA(cudaEventRecord(st.ev[5], s));
+            GRPP_CUDA(cudaEventRecord(ev[5], s));
         }
         radial_walk_kernel<<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(ra);
         GRPP_CUDA(cudaGetLastError());
     }
-    GRPP_CUDA(cudaEventRecord(st.ev[2], s));
+    GRPP_CUDA(cudaEventRecord(ev[2], s));
     final_kernel<<<P.fin_blocks, kFinThreads, P.fin_smem, s>>>(P.fin, P.fin_smem_layout);
     GRPP_CUDA(cudaGetLastError());
-    GRPP_CUDA(cudaEventRecord(st.ev[3], s));
-    int hstatus[16];
-    GRPP_CUDA(cudaMemcpyAsync(hstatus, P.status, sizeof(hstatus), cudaMemcpyDeviceToHost, s));
-    GRPP_CUDA(cudaMemcpyAsync(P.stats.radial_counters, P.counters, kRadCntNum * sizeof(unsigned long long),
-                              cudaMemcpyDeviceToHost, s));
-    GRPP_CUDA(cudaStreamSynchronize(s));
-    cudaEventElapsedTime(&P.stats.ms_mmd, st.ev[0], st.ev[1]);
-    cudaEventElapsedTime(&P.stats.ms_radial, st.ev[1], st.ev[2]);
-    if (P.rad_blocks > 0) cudaEventElapsedTime(&P.stats.ms_screen, st.ev[1], st.ev[4]);
+    GRPP_CUDA(cudaEventRecord(ev[3], s));
+    int *hs = st.hstat[P.set];
+    GRPP_CUDA(cudaMemcpyAsync(hs, P.status, 16 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    GRPP_CUDA(cudaMemcpyAsync(hs + 16, P.counters, kRadCntNum * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    GRPP_CUDA(cudaEventRecord(st.done[P.set], s));
+    return 0;
+}
+
+// Wait for a launched execution; its timings, counters and status.
+int plan_finish(Plan &P)
+{
+    DeviceState &st = *P.st;
+    cudaEvent_t *ev = st.ev[P.set];
+    if (P.n_tasks == 0) return 0;
+    GRPP_CUDA(cudaEventSynchronize(st.done[P.set]));
+    const int *hstatus = st.hstat[P.set];
+    memcpy(P.stats.radial_counters, hstatus + 16, kRadCntNum * sizeof(unsigned long long));
+    cudaEventElapsedTime(&P.stats.ms_mmd, ev[0], ev[1]);
+    cudaEventElapsedTime(&P.stats.ms_radial, ev[1], ev[2]);
+    if (P.rad_blocks > 0) cudaEventElapsedTime(&P.stats.ms_screen, ev[1], ev[4]);
     P.stats.ms_predict = 0.f;
     if (P.rad_blocks > 0 && P.opt.radial_mode == LIBGRPP_B200_RADIAL_LEARNED)
-        cudaEventElapsedTime(&P.stats.ms_predict, st.ev[4], st.ev[5]);
+        cudaEventElapsedTime(&P.stats.ms_predict, ev[4], ev[5]);
     P.stats.fallbacks = hstatus[4];
-    cudaEventElapsedTime(&P.stats.ms_final, st.ev[2], st.ev[3]);
-    cudaEventElapsedTime(&P.stats.ms_total, st.ev[0], st.ev[3]);
+    cudaEventElapsedTime(&P.stats.ms_final, ev[2], ev[3]);
+    cudaEventElapsedTime(&P.stats.ms_total, ev[0], ev[3]);
     P.stats.n_tasks = P.n_tasks;
     P.stats.n_radial = P.n_radial;
     P.stats.n_mmd = P.n_mmd;
@@ -1065,6 +1123,13 @@ int plan_execute(Plan &P)
         return LIBGRPP_B200_ERR_INVALID;
     }
     return 0;
+}
+
+int plan_execute(Plan &P)
+{
+    int rc = plan_launch(P);
+    if (rc == 0) rc = plan_finish(P);
+    return rc;
 }
 
 int plan_download(Plan &P, double *h_arep, double *h_sx, double *h_sy, double *h_sz)
@@ -1080,8 +1145,10 @@ int plan_download(Plan &P, double *h_arep, double *h_sx, double *h_sy, double *h
 
 // Large batches run as consecutive chunks of tasks whose radial tables together stay
 // below kChunkEntries entries (24 bytes of device scratch each) and kChunkTasks tasks;
-// outputs land at each chunk's offset in the caller's arrays.
-constexpr int64_t kChunkEntries = int64_t(1) << 27, kChunkTasks = int64_t(1) << 20;
+// outputs land at each chunk's offset in the caller's arrays. Chunks of 16384 tasks keep
+// every kernel's grid several waves deep while the host work of one chunk hides behind
+// the GPU work of the previous one.
+constexpr int64_t kChunkEntries = int64_t(1) << 27, kChunkTasks = int64_t(1) << 14;
 
 int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double *h_arep, double *h_sx, double *h_sy,
                    double *h_sz, RunStats *stats)
@@ -1107,10 +1174,10 @@ int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double 
             CHECK_INPUT(pot >= 0 && pot < b->n_pots, "GRPP potential index out of range");
         }
     }
-    // radial entries of a task: sum over the centre's semilocal potentials of (L+la+1)(L+lb+1)(la+lb+1)
-    RunStats total;
-    int64_t t0 = 0, out0 = 0;
-    while (t0 < b->n_tasks || (t0 == 0 && b->n_tasks == 0)) {
+    // chunk boundaries; a task's radial entries: sum over the centre's semilocal potentials
+    // of (L+la+1)(L+lb+1)(la+lb+1)
+    std::vector<std::pair<int64_t, int64_t>> chunks;
+    for (int64_t t0 = 0; t0 < b->n_tasks;) {
         int64_t t1 = t0, ent = 0;
         while (t1 < b->n_tasks && t1 - t0 < kChunkTasks) {
             const int la = b->shell_L[b->task_a[t1]], lb = b->shell_L[b->task_b[t1]], g = b->centre_grpp[b->task_c[t1]];
@@ -1125,25 +1192,51 @@ int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double 
             ent += e;
             t1++;
         }
-        libgrpp_b200_batch_t v = *b;
-        v.n_tasks = t1 - t0;
-        v.task_a = b->task_a + t0;
-        v.task_b = b->task_b + t0;
-        v.task_c = b->task_c + t0;
-        Plan P;
-        rc = plan_build(*stp, &v, opt, false, P);
-        if (rc) return rc;
-        rc = plan_execute(P);
-        if (rc) return rc;
-        rc = plan_download(P, h_arep ? h_arep + out0 : nullptr, h_sx ? h_sx + out0 : nullptr,
-                           h_sy ? h_sy + out0 : nullptr, h_sz ? h_sz + out0 : nullptr);
-        if (rc) return rc;
-        out0 += P.out_tot;
-        total.n_tasks += P.stats.n_tasks;
-        total.ms_total += P.stats.ms_total;
-        if (b->n_tasks == 0) break;
+        chunks.push_back({t0, t1});
         t0 = t1;
     }
+    if (chunks.empty()) chunks.push_back({0, 0});
+    // chunk c uses buffer set c % 2: while the GPU runs chunk c, the host downloads chunk
+    // c-1 (on the copy stream) and then prepares chunk c+1
+    RunStats total;
+    Plan P[2];
+    int64_t out_at[2] = {0, 0}, out0 = 0;
+    auto finish_and_download = [&](Plan &Q, int64_t at) -> int {
+        int r = plan_finish(Q);
+        if (r) return r;
+        if (Q.n_tasks > 0) {
+            double *h[4] = {h_arep, h_sx, h_sy, h_sz};
+            GRPP_CUDA(cudaStreamWaitEvent(stp->copy_stream, stp->done[Q.set], 0));
+            for (int k = 0; k < 4; k++)
+                if (h[k])
+                    GRPP_CUDA(cudaMemcpyAsync(h[k] + at, Q.outs[k], Q.out_tot * sizeof(double), cudaMemcpyDeviceToHost,
+                                              stp->copy_stream));
+            GRPP_CUDA(cudaStreamSynchronize(stp->copy_stream));
+        }
+        total.n_tasks += Q.stats.n_tasks;
+        total.ms_total += Q.stats.ms_total;
+        return 0;
+    };
+    for (size_t c = 0; c < chunks.size(); c++) {
+        const int k = (int)(c & 1);
+        libgrpp_b200_batch_t v = *b;
+        v.n_tasks = chunks[c].second - chunks[c].first;
+        v.task_a = b->task_a + chunks[c].first;
+        v.task_b = b->task_b + chunks[c].first;
+        v.task_c = b->task_c + chunks[c].first;
+        P[k] = Plan();
+        rc = plan_build(*stp, &v, opt, false, P[k], k);
+        if (rc) return rc;
+        rc = plan_launch(P[k]);
+        if (rc) return rc;
+        out_at[k] = out0;
+        out0 += P[k].out_tot;
+        if (c >= 1) {
+            rc = finish_and_download(P[1 - k], out_at[1 - k]);
+            if (rc) return rc;
+        }
+    }
+    rc = finish_and_download(P[(chunks.size() - 1) & 1], out_at[(chunks.size() - 1) & 1]);
     if (stats) *stats = total;
     return rc;
 }
@@ -1210,12 +1303,12 @@ int measure_fp64_peak(double *tflops)
     GRPP_CUDA(cudaMalloc(&d, sizeof(double)));
     const int threads = 256, blocks = nsm * 8, iters = 4096;
     fp64_peak_kernel<<<blocks, threads, 0, s>>>(d, 64, 0.999999, 1e-7);
-    GRPP_CUDA(cudaEventRecord(stp->ev[4], s));
+    GRPP_CUDA(cudaEventRecord(stp->ev[0][4], s));
     fp64_peak_kernel<<<blocks, threads, 0, s>>>(d, iters, 0.999999, 1e-7);
-    GRPP_CUDA(cudaEventRecord(stp->ev[5], s));
-    GRPP_CUDA(cudaEventSynchronize(stp->ev[5]));
+    GRPP_CUDA(cudaEventRecord(stp->ev[0][5], s));
+    GRPP_CUDA(cudaEventSynchronize(stp->ev[0][5]));
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, stp->ev[4], stp->ev[5]);
+    cudaEventElapsedTime(&ms, stp->ev[0][4], stp->ev[0][5]);
     cudaFree(d);
     *tflops = 2.0 * 8.0 * iters * (double)threads * blocks / (ms * 1e-3) / 1e12;
     return 0;

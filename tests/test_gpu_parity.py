@@ -120,8 +120,9 @@ def test_h2o_gradients(gpu_lib):
 
 
 def test_large_batch_runs_in_chunks(gpu_lib):
-    """A batch whose radial tables exceed one chunk (2^27 entries) through the batched
-    entry point, which splits it, equals the same tasks run as one plan."""
+    """A batch larger than one chunk (16384 tasks, and here also more than 2^27 radial
+    entries) through the batched entry point, which splits it and overlaps the chunks,
+    equals the same tasks run as one plan."""
     S = synthetic.config1()
     a, b, c = S.all_tasks()
     La = np.array([s.L for s in S.shells])
