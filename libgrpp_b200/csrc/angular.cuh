@@ -36,7 +36,7 @@ __host__ __device__ inline int abc_index(int l, int a, int b, int c)
     idx += b * (l - a + 1) - b * (b - 1) / 2;
     return idx + c;
 }
-__host__ __device__ inline int n_abc(int l) { return (l + 1) * (l + 2) * (l + 3) / 6; }
+__host__ __device__ constexpr int n_abc(int l) { return (l + 1) * (l + 2) * (l + 3) / 6; }
 
 // lambda slots for |abc| = n: lambda = lo, lo+2, ..., L+n
 __host__ __device__ inline int lam_lo(int L, int n) { return L - n >= 0 ? L - n : ((L + n) & 1); }
@@ -251,6 +251,10 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
     extern __shared__ double dsm[];
     __shared__ double powA[3][kMaxL + 2], powB[3][kMaxL + 2];
     __shared__ double sCA[3], sCB[3];
+    // powers u^0..u^lam of the unit vectors along kA, kB: [side][axis][power], each the same
+    // chain of products 1 * u * u ... as the reference's per-term loops
+    __shared__ double upow[2][3][kFinMaxLam + 1];
+    __shared__ int8_t nabcA[n_abc(kMaxL)], nabcB[n_abc(kMaxL)];  // |abc| of each abc index
     const int tid = threadIdx.x;
     double *rshA = dsm, *rshB = rshA + sm.n_rsh, *omA = rshB + sm.n_rsh, *omB = omA + sm.n_omega, *Qs = omB + sm.n_omega,
            *V = Qs + sm.n_q;
@@ -307,22 +311,48 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                     const double inv = 1.0 / lenB;
                     for (int d = 0; d < 3; d++) uB[d] = kB[d] * inv;
                 }
-                for (int e = tid; e < 2 * (lam_max + 1) * rs; e += kFinThreads) {
-                    const int side = e / ((lam_max + 1) * rs), r = e % ((lam_max + 1) * rs);
-                    const int l = r / rs, mu = r % rs - l;
-                    if (mu > l) continue;
-                    const double *u = side ? uB : uA;
+                if (tid < 6) {
+                    const int side = tid / 3, d = tid % 3;
+                    const double ud = side ? (d == 0 ? uB[0] : (d == 1 ? uB[1] : uB[2]))
+                                           : (d == 0 ? uA[0] : (d == 1 ? uA[1] : uA[2]));
+                    double pw = 1.0;
+                    upow[side][d][0] = pw;
+                    for (int i = 1; i <= lam_max; i++) {
+                        pw *= ud;
+                        upow[side][d][i] = pw;
+                    }
+                }
+                for (int e = tid; e < n_abc(la) + n_abc(lb); e += kFinThreads) {
+                    const bool sideB = e >= n_abc(la);
+                    const int l = sideB ? lb : la;
+                    int idx = sideB ? e - n_abc(la) : e, aa, bb;
+                    for (aa = 0; aa <= l; aa++) {
+                        const int cnt = (l - aa + 1) * (l - aa + 2) / 2;
+                        if (idx < cnt) break;
+                        idx -= cnt;
+                    }
+                    for (bb = 0; bb <= l - aa; bb++) {
+                        const int cnt = l - aa - bb + 1;
+                        if (idx < cnt) break;
+                        idx -= cnt;
+                    }
+                    (sideB ? nabcB : nabcA)[sideB ? e - n_abc(la) : e] = (int8_t)(aa + bb + idx);
+                }
+                __syncthreads();
+                // (l, mu) pairs e = l^2 + l + mu of both sides
+                const int nlm = (lam_max + 1) * (lam_max + 1);
+                for (int e = tid; e < 2 * nlm; e += kFinThreads) {
+                    const int side = e >= nlm, r = side ? e - nlm : e;
+                    int l = (int)sqrtf((float)r);
+                    while (l * l > r) l--;
+                    while ((l + 1) * (l + 1) <= r) l++;
+                    const int mu = r - l * l - l;
+                    const double(*up)[kFinMaxLam + 1] = upow[side];
                     const int nc = ncart(l);
                     const int8_t *cc = c_tab.rsh_comb + 3 * c_tab.rsh_comb_off[l];
                     const double *y = c_tab.rsh_coef + c_tab.rsh_off[l] + (mu + l) * nc;
                     double v = 0.0;
-                    for (int q = 0; q < nc; q++) {
-                        double px = 1.0, py = 1.0, pz = 1.0;
-                        for (int i = 0; i < cc[3 * q]; i++) px *= u[0];
-                        for (int i = 0; i < cc[3 * q + 1]; i++) py *= u[1];
-                        for (int i = 0; i < cc[3 * q + 2]; i++) pz *= u[2];
-                        v += y[q] * (px * py * pz);
-                    }
+                    for (int q = 0; q < nc; q++) v += y[q] * (up[0][cc[3 * q]] * up[1][cc[3 * q + 1]] * up[2][cc[3 * q + 2]]);
                     (side ? rshB : rshA)[l * rs + mu + l] = v;
                 }
             }
@@ -362,20 +392,8 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                     const int sl = sideB ? slB : slA, nab = sideB ? nabB : nabA, l = sideB ? lb : la;
                     const int m = r % nm, slot = (r / nm) % sl, abc = r / (nm * sl);
                     (void)nab;
-                    // n of abc: decode from the index
-                    int aa = 0, idx = abc;
-                    for (aa = 0; aa <= l; aa++) {
-                        const int cnt = (l - aa + 1) * (l - aa + 2) / 2;
-                        if (idx < cnt) break;
-                        idx -= cnt;
-                    }
-                    int bb = 0;
-                    for (bb = 0; bb <= l - aa; bb++) {
-                        const int cnt = l - aa - bb + 1;
-                        if (idx < cnt) break;
-                        idx -= cnt;
-                    }
-                    const int n = aa + bb + idx;
+                    (void)l;
+                    const int n = sideB ? nabcB[abc] : nabcA[abc];
                     double w = 0.0;
                     if (slot < lam_count(L, n)) {
                         const int lam = lam_lo(L, n) + 2 * slot;

@@ -372,8 +372,8 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
                                 const double x = q * (dx * dx + dy * dy + dz * dz);
                                 if (npow == 1) {
                                     if (lane <= S) aux[lane] = boys(lane, x);
-                                } else if (lane == 0) {
-                                    gfun_values(x, S, aux);
+                                } else {
+                                    gfun_values_warp(x, S, aux, lane);
                                 }
                                 __syncwarp();
                                 const bool isg = npow == 0;

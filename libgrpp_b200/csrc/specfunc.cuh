@@ -168,6 +168,40 @@ __device__ inline void gfun_values(double x, int nmax, double *g)
     }
 }
 
+// gfun_values by one warp (all 32 lanes call it; g[] is written by lane 0). For x <= 12
+// lane k forms the series term k with the same product chains as the serial loop
+// (x^k and k! by repeated multiplication from 1), and lane 0 adds the terms in order up
+// to the first one below 1e-15, as the serial loop does; the recursions stay on lane 0.
+__device__ inline void gfun_values_warp(double x, int nmax, double *g, int lane)
+{
+    if (x <= 12.0) {
+        const double ex = exp(-x);
+        double sum = 0.0;
+        for (int k0 = 0; k0 < 100; k0 += 32) {
+            const int k = k0 + lane;
+            double xk = 1.0, fk = 1.0;
+            for (int i = 1; i <= k; i++) {
+                xk *= x;
+                fk *= i;
+            }
+            const double c = ex * xk / fk / (2.0 * nmax + 2.0 * k + 1.0);
+            const unsigned stop = __ballot_sync(0xffffffffu, k >= 99 || fabs(c) < 1e-15);
+            const int last = stop ? __ffs(stop) - 1 : 31;  // last term added in this block
+            for (int j = 0; j <= last; j++) {
+                const double cj = __shfl_sync(0xffffffffu, c, j);
+                if (lane == 0) sum += cj;
+            }
+            if (stop) break;
+        }
+        if (lane == 0) {
+            g[nmax] = sum;
+            for (int n = nmax; n > 0; n--) g[n - 1] = (1.0 - 2.0 * x * g[n]) / (2.0 * n - 1.0);
+        }
+    } else if (lane == 0) {
+        gfun_values(x, nmax, g);
+    }
+}
+
 // (2a/pi)^(3/4) (4a)^(L/2)  (libgrpp/norm_gaussian.c:16-23)
 __device__ __forceinline__ double gaussian_norm(int L, double a)
 {
