@@ -29,12 +29,10 @@ namespace grpp {
 // lexicographic index of (a, b, c), a+b+c <= l (a outer, then b, then c)
 __host__ __device__ inline int abc_index(int l, int a, int b, int c)
 {
-    // triples with first component < a
-    int idx = 0;
-    for (int q = 0; q < a; q++) idx += (l - q + 1) * (l - q + 2) / 2;
-    // with first a and second < b
-    idx += b * (l - a + 1) - b * (b - 1) / 2;
-    return idx + c;
+    // triples with first component < a: sum_{q<a} (l-q+1)(l-q+2)/2 = tet(l+1) - tet(l+1-a),
+    // tet(m) = m(m+1)(m+2)/6; then those with first a and second < b
+    const int m = l + 1, r = l + 1 - a;
+    return (m * (m + 1) * (m + 2) - r * (r + 1) * (r + 2)) / 6 + b * (l - a + 1) - b * (b - 1) / 2 + c;
 }
 __host__ __device__ constexpr int n_abc(int l) { return (l + 1) * (l + 2) * (l + 3) / 6; }
 
@@ -424,32 +422,7 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                     // V[abc][def] (type2_integrals.c:174-196, spin_orbit_integrals.c:197-224)
                     for (int e = tid; e < (r1 - r0) * nabB; e += kFinThreads) {
                         const int abc = r0 + e / nabB, def = e % nabB;
-                        int aa = 0, idx = abc;
-                        for (aa = 0; aa <= la; aa++) {
-                            const int cnt = (la - aa + 1) * (la - aa + 2) / 2;
-                            if (idx < cnt) break;
-                            idx -= cnt;
-                        }
-                        int bb;
-                        for (bb = 0; bb <= la - aa; bb++) {
-                            const int cnt = la - aa - bb + 1;
-                            if (idx < cnt) break;
-                            idx -= cnt;
-                        }
-                        const int n1 = aa + bb + idx;
-                        int dd = 0, jdx = def;
-                        for (dd = 0; dd <= lb; dd++) {
-                            const int cnt = (lb - dd + 1) * (lb - dd + 2) / 2;
-                            if (jdx < cnt) break;
-                            jdx -= cnt;
-                        }
-                        int ee;
-                        for (ee = 0; ee <= lb - dd; ee++) {
-                            const int cnt = lb - dd - ee + 1;
-                            if (jdx < cnt) break;
-                            jdx -= cnt;
-                        }
-                        const int n2 = dd + ee + jdx, N = n1 + n2;
+                        const int n1 = nabcA[abc], n2 = nabcB[def], N = n1 + n2;
                         double v0 = 0.0, v1 = 0.0, v2 = 0.0;
                         const int c1 = lam_count(L, n1), c2 = lam_count(L, n2);
                         for (int s1 = 0; s1 < c1; s1++) {
