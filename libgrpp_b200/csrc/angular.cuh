@@ -193,6 +193,10 @@ struct FinalArgs {
     int raw_so;                       // 1: spin-orbit output without the 2/(2L+1) factor
     double *arep, *so_x, *so_y, *so_z;
     int *status;
+    // dynamic schedule: blocks pop positions from *queue (zeroed before the launch) and take
+    // task order[position], largest estimated work first; queue may be null: static round-robin
+    const int *order;
+    int *queue;
 };
 
 // RSH values S_{l mu}(k/|k|) for l = 0..lmax (spherical_harmonics.c:227-280); out[l*(2*kFinMaxLam+1) + mu + l]
@@ -258,7 +262,24 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
            *V = Qs + sm.n_q;
     const int rs = sm.rsh_stride;
 
-    for (int t = blockIdx.x; t < a.n_tasks; t += gridDim.x) {
+    __shared__ int s_next;
+    int t_static = blockIdx.x;
+    for (;;) {
+        int t;
+        if (a.queue) {
+            __syncthreads();  // every thread has read the previous s_next
+            if (tid == 0) {
+                const int k = atomicAdd(a.queue, 1);
+                s_next = k < a.n_tasks ? a.order[k] : -1;
+            }
+            __syncthreads();
+            t = s_next;
+            if (t < 0) break;
+        } else {
+            t = t_static;
+            t_static += gridDim.x;
+            if (t >= a.n_tasks) break;
+        }
         const int sa = a.task_a[t], sb = a.task_b[t], c = a.task_c[t];
         const int la = a.shell_L[sa], lb = a.shell_L[sb], nA = ncart(la), nB = ncart(lb), nel = nA * nB;
         const int8_t *cA = a.cart + 3 * a.shell_cart_off[sa], *cB = a.cart + 3 * a.shell_cart_off[sb];

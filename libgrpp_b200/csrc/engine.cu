@@ -309,6 +309,23 @@ static void mmd_update_tables(int lmax, int smax, std::vector<int> &etab, std::v
     }
 }
 
+// Positions of work items in decreasing order of estimated work (buckets of a quarter
+// octave; items of one bucket keep their order), for the kernels' dynamic queues.
+static std::vector<int> order_by_cost(const std::vector<double> &cost)
+{
+    std::vector<int> key(cost.size());
+    int kmax = 0;
+    for (size_t i = 0; i < cost.size(); i++) {
+        key[i] = cost[i] > 1.0 ? std::min(255, (int)(4.0 * std::log2(cost[i]))) : 0;
+        kmax = std::max(kmax, key[i]);
+    }
+    std::vector<int> start(kmax + 2, 0), out(cost.size());
+    for (int k : key) start[kmax - k + 1]++;
+    for (int b = 1; b <= kmax + 1; b++) start[b] += start[b - 1];
+    for (size_t i = 0; i < cost.size(); i++) out[start[kmax - key[i]]++] = (int)i;
+    return out;
+}
+
 template <typename T>
 T *at(void *base, size_t off)
 {
@@ -745,7 +762,33 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
             it.sched_rows = f->second.second;
         }
     }
+    // estimated work per type 1 item: primitive triples x (Hermite + R entries + contraction terms)
+    std::vector<int> mmd_order;
+    {
+        std::vector<double> cost(items.size());
+        for (size_t q = 0; q < items.size(); q++) {
+            const MmdItem &it = items[q];
+            const int la = sh_L[it.bra], lb = sh_L[it.ket], S = la + lb;
+            const double np2 = (double)sh_np[it.bra] * sh_np[it.ket], pairs = (double)ncart(la) * ncart(lb);
+            if (it.pot < 0) cost[q] = np2 * (pairs + 10.0);
+            else
+                cost[q] = np2 * p_n[it.pot] *
+                          (mmd_e_count(la, lb) + mmd_r_size(S) + pairs * (S + 3.0) * (S + 3.0) * (S + 3.0) / 27.0);
+        }
+        mmd_order = order_by_cost(cost);
+    }
 
+    // estimated work per task in the assembly: per semilocal potential, the V table and the
+    // re-centring sums of its Cartesian pairs
+    std::vector<int> fin_order;
+    {
+        std::vector<double> cost(nt);
+        for (int64_t t = 0; t < nt; t++) {
+            const int la = sh_L[ta[t]], lb = sh_L[tb[t]], g = b->centre_grpp[tc[t]];
+            cost[t] = 1.0 + (double)g_sl_n[g] * ((double)n_abc(la) * n_abc(lb) + 4.0 * ncart(la) * ncart(lb));
+        }
+        fin_order = order_by_cost(cost);
+    }
     std::vector<int> mmd_etab, mmd_etab_off, mmd_rtab_off;
     std::vector<int2> mmd_rtab;
     mmd_update_tables(mmd_lmax, mmd_smax, mmd_etab, mmd_etab_off, mmd_rtab, mmd_rtab_off);
@@ -787,7 +830,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     const size_t o_bs = pk.add(blk_shell), o_bo = pk.add(blk_oc), o_bco = pk.add(blk_cart_off), o_bso = pk.add(blk_sph_off),
                  o_poffp = pk.add(proj_off), o_msch = pk.add(mmd_sched);
     const size_t o_met = pk.add(mmd_etab), o_meto = pk.add(mmd_etab_off), o_mrt = pk.add(mmd_rtab),
-                 o_mrto = pk.add(mmd_rtab_off);
+                 o_mrto = pk.add(mmd_rtab_off), o_mord = pk.add(mmd_order), o_ford = pk.add(fin_order);
     std::vector<int8_t> stop_dummy;
     DevBuf *bin = own_buffers ? &P.in : &st.in[set], *bscr = own_buffers ? &P.scratch : &st.scratch[set],
            *bout = own_buffers ? &P.out : &st.out[set];
@@ -870,13 +913,21 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         m.etab_off = at<int>(ib, o_meto);
         m.rtab = at<int2>(ib, o_mrt);
         m.rtab_off = at<int>(ib, o_mrto);
+        m.order = at<int>(ib, o_mord);
+        m.queue = statusd + 8;
         const int wpb = 4;
         P.mmd_kpl = mmd_kpl;
         // per warp: the workspace, then 32 x KPL pair descriptors (8 bytes each)
         const size_t smem = (size_t)wpb * (mmd_ws_size(mmd_lmax, mmd_smax) + 32 * P.mmd_kpl) * sizeof(double);
         CHECK_INPUT(smem <= 200 * 1024, "type 1 workspace of this batch's angular momenta exceeds one block's shared memory");
         P.mmd = m;
-        P.mmd_blocks = (int)std::min<int64_t>(((int64_t)items.size() + wpb - 1) / wpb, (int64_t)nsm * 16);
+        // persistent grid: the resident blocks pop items until the queue is empty
+        int mmd_occ = 0;
+        if (mmd_kpl == 8)
+            GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mmd_occ, mmd_kernel<8, false>, 32 * wpb, smem));
+        else
+            GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mmd_occ, mmd_kernel<32, false>, 32 * wpb, smem));
+        P.mmd_blocks = (int)std::min<int64_t>(((int64_t)items.size() + wpb - 1) / wpb, (int64_t)nsm * std::max(mmd_occ, 1));
         P.mmd_threads = 32 * wpb;
         P.mmd_smem = smem;
     }
@@ -1005,6 +1056,8 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         f.so_y = o_sy;
         f.so_z = o_sz;
         f.status = statusd;
+        f.order = at<int>(ib, o_ford);
+        f.queue = statusd + 9;
         FinalSmem fs{};
         fs.rsh_stride = 2 * fin_lam + 1;
         fs.n_rsh = (fin_lam + 1) * fs.rsh_stride;
@@ -1026,7 +1079,9 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         const size_t smem = smem_base + (size_t)fs.n_w * sizeof(double);
         P.fin = f;
         P.fin_smem_layout = fs;
-        P.fin_blocks = (int)std::min<int64_t>(nt, (int64_t)nsm * 8);
+        int fin_occ = 0;  // persistent grid over the task queue
+        GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fin_occ, final_kernel, kFinThreads, smem));
+        P.fin_blocks = (int)std::min<int64_t>(nt, (int64_t)nsm * std::max(fin_occ, 1));
         P.fin_smem = smem;
     }
     return 0;
