@@ -695,7 +695,7 @@ __device__ __forceinline__ int level_last_point(int L) { return (1 << (L + 5)) -
 // The walk of a task stops at the first chunk boundary after which no entry is active;
 // points evaluated past that are never added. The orders, powers and potentials
 // evaluated per point shrink with the set of active entries.
-__global__ void __launch_bounds__(kRadThreads, 4) radial_walk_kernel(RadialArgs a)
+__global__ void __launch_bounds__(kRadThreads, 5) radial_walk_kernel(RadialArgs a)
 {
     __shared__ RadialShared sh;
     __shared__ int s_need[2][4];  // per buffer: max l1, max l2, max N of active entries, potential mask
