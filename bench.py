@@ -16,7 +16,8 @@ steps) for the learned batched form (the walk scheduled by the level model);
 "plain" = the same steps with the plain level-by-level schedule, and
 learned_over_plain their ratio (results are bit-identical); e2e = the same
 tasks through the public batched C-ABI call with host inputs and outputs
-(packing, host->device and device->host copies included).
+(packing, host->device and device->host copies included; the outputs go to
+page-locked host arrays allocated once through libgrpp_b200_host_alloc).
 --impl reference times libgrpp itself (oracle/_ref, compiled from its
 sources) on this host's cores over a bounded sample of each step's tasks.
 """
@@ -278,14 +279,17 @@ def run_ours(args, rank, world, local):
     main_mode = args.mode
     R = res[main_mode]
 
-    # end to end through the public batched call (host in, host out)
+    # end to end through the public batched call (host in, host out): outputs land in
+    # page-locked host arrays the caller allocated once (libgrpp_b200_host_alloc)
     e2e_batches = batches[: max(1, min(len(batches), args.e2e_steps))]
-    lib.full_grpp_batch(e2e_batches[0], modes[main_mode])
+    n_out = max(int(b.block_offsets()[-1]) for b in e2e_batches)
+    outs = [lib.pinned_empty(n_out) for _ in range(4)]
+    lib.full_grpp_batch(e2e_batches[0], modes[main_mode], out=outs)
     if dist is not None:
         dist.barrier()
     t0 = time.perf_counter()
     for b in e2e_batches:
-        lib.full_grpp_batch(b, modes[main_mode])
+        lib.full_grpp_batch(b, modes[main_mode], out=outs)
     e2e_s = time.perf_counter() - t0
     e2e_s, e2e_tasks = reduce_time_and_work(dist, e2e_s, float(sum(len(b.task_a) for b in e2e_batches)), "cuda")
     d2h = 4 * 8 * int(batches[0].block_offsets()[-1])

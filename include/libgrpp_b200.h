@@ -100,6 +100,13 @@ int64_t libgrpp_b200_batch_output_size(const libgrpp_b200_batch_t *batch);
 int libgrpp_b200_full_grpp_batch(const libgrpp_b200_batch_t *batch, int radial_mode, double *arep,
                                  double *so_x, double *so_y, double *so_z);
 
+/* Page-locked host memory for input and output arrays of the calls above: device<->host
+ * copies to and from it run at full link speed and need no staging. Returns NULL on
+ * failure (message in libgrpp_b200_last_error_message). Free with libgrpp_b200_host_free.
+ * Not part of libgrpp's interface. */
+void *libgrpp_b200_host_alloc(size_t bytes);
+void libgrpp_b200_host_free(void *p);
+
 /* Select the CUDA device used by the calling thread (this library keeps its own
  * CUDA runtime state; default device 0). Returns a status code. */
 int libgrpp_b200_set_device(int device);

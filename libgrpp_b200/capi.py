@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes as ct
 import os
+import weakref
 
 import numpy as np
 
@@ -78,6 +79,8 @@ class LibGRPP:
         self._opt("libgrpp_b200_last_error_message", ct.c_char_p, [])
         self._opt("libgrpp_b200_full_grpp_batch", ct.c_int, [_V, ct.c_int, _D, _D, _D, _D])
         self._opt("libgrpp_b200_set_device", ct.c_int, [ct.c_int])
+        self._opt("libgrpp_b200_host_alloc", _V, [ct.c_size_t])
+        self._opt("libgrpp_b200_host_free", None, [_V])
         self._opt("libgrpp_b200_fp64_peak", ct.c_int, [_D])
         self._opt("libgrpp_b200_type2_batch_noalloc", ct.c_int, [_V, _D])
         self._opt("libgrpp_b200_plan_create", _V, [_V, ct.c_int])
@@ -195,15 +198,33 @@ class LibGRPP:
         return int(self.lib.grpp_driver_num_threads())
 
     # ------------------------------------------------------------ batched (GPU engine)
-    def full_grpp_batch(self, batch, radial_mode=0):
+    def full_grpp_batch(self, batch, radial_mode=0, out=None):
+        """AREP, SO_x, SO_y, SO_z blocks of every task. out: optional four float64 arrays of at
+        least the batch's output size (e.g. from pinned_empty), written in place and returned."""
         if radial_mode == 1:
             self.ensure_level_model()
         n = int(batch.block_offsets()[-1])
-        outs = [np.empty(max(n, 1)) for _ in range(4)]  # the call writes every element
+        if out is None:
+            outs = [np.empty(max(n, 1)) for _ in range(4)]  # the call writes every element
+        else:
+            outs = list(out)
+            if len(outs) != 4 or any(x.dtype != np.float64 or not x.flags.c_contiguous or x.size < n for x in outs):
+                raise ValueError("out must be four C-contiguous float64 arrays of at least the batch's output size")
         rc = self.lib.libgrpp_b200_full_grpp_batch(ct.byref(batch.struct), radial_mode, *[_dp(x) for x in outs])
         if rc != 0:
             raise RuntimeError(f"libgrpp_b200_full_grpp_batch failed ({rc}): {self.last_error_message()}")
         return [x[:n] for x in outs]
+
+    def pinned_empty(self, n: int) -> np.ndarray:
+        """A float64 array of n elements in page-locked host memory (freed with the array)."""
+        nbytes = max(int(n), 1) * 8
+        p = self.lib.libgrpp_b200_host_alloc(nbytes)
+        if not p:
+            raise MemoryError(f"libgrpp_b200_host_alloc({nbytes}) failed: {self.last_error_message()}")
+        buf = (ct.c_double * max(int(n), 1)).from_address(p)
+        arr = np.frombuffer(buf, dtype=np.float64, count=max(int(n), 1))
+        weakref.finalize(arr, self.lib.libgrpp_b200_host_free, ct.c_void_p(p))
+        return arr[:int(n)] if n > 0 else arr
 
     def type2_batch_noalloc(self, batch):
         """AREP type 2 blocks of every task through the allocation-free entry point."""

@@ -654,6 +654,10 @@ int libgrpp_b200_full_grpp_batch(const libgrpp_b200_batch_t *b, int radial_mode,
 
 int libgrpp_b200_set_device(int device) { return grpp::set_device(device); }
 
+void *libgrpp_b200_host_alloc(size_t bytes) { return grpp::host_alloc(bytes); }
+
+void libgrpp_b200_host_free(void *p) { grpp::host_free(p); }
+
 int libgrpp_b200_fp64_peak(double *tflops) { return grpp::measure_fp64_peak(tflops); }
 
 libgrpp_b200_plan_t *libgrpp_b200_plan_create(const libgrpp_b200_batch_t *b, int radial_mode)

@@ -1689,6 +1689,23 @@ int run_grad_contract(const libgrpp_b200_batch_t *sub, const RunOptions &opt, co
 const RunStats *plan_stats(const Plan *P) { return &P->stats; }
 int64_t plan_h2d_bytes(const Plan *P) { return P->h2d_bytes; }
 
+void *host_alloc(size_t bytes)
+{
+    set_error(0, "");
+    void *p = nullptr;
+    const cudaError_t e = cudaHostAlloc(&p, std::max<size_t>(bytes, 1), cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        set_error(LIBGRPP_B200_ERR_CUDA, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+        return nullptr;
+    }
+    return p;
+}
+
+void host_free(void *p)
+{
+    if (p) cudaFreeHost(p);
+}
+
 int set_device(int device)
 {
     GRPP_CUDA(cudaSetDevice(device));

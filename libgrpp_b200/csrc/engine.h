@@ -42,6 +42,8 @@ void plan_destroy(Plan *P);
 const RunStats *plan_stats(const Plan *P);
 int64_t plan_h2d_bytes(const Plan *P);
 int set_device(int device);
+void *host_alloc(size_t bytes);
+void host_free(void *p);
 int measure_fp64_peak(double *tflops);
 
 // density-contracted gradient (gradient.cuh): one entry per task of the original list

@@ -124,7 +124,7 @@ static void bessel_tables_init(void)
     for (int n = 0; n < 50; n++) {
         for (int k = 0; k <= n; k++) {
             long double v = 1.0L;
-            for (int j = n - k + 1; j <= n + k; j++) v *= j; /* (n+k)!/(n-k)! */
+            for (int q = 0; q < 2 * k; q++) v *= (long double)(n - k + 1 + q); /* (n+k)!/(n-k)! */
             for (int j = 1; j <= k; j++) v /= (2.0L * j);    /* / (k! 2^k) */
             rfun[n][k] = (double)v;
         }
