@@ -110,6 +110,7 @@ struct DeviceState {
     int *hstat[2] = {nullptr, nullptr};  // page-locked status words + counters per buffer set
     DevBuf atab;
     size_t atab_used = 0;
+    DevBuf grad;  // density-contracted gradient: tasks, component table, D, per-task sums
     // learned grid-level model (libgrpp_b200_set_level_model): FP32 normalisation, BF16 weights
     float *lm_norm = nullptr;
     __nv_bfloat16 *lm_w = nullptr;
@@ -1649,9 +1650,8 @@ int run_grad_contract(const libgrpp_b200_batch_t *sub, const RunOptions &opt, co
     const size_t tab_n = (size_t)(kMaxL + 1) * kGradMaxCart * 9;
     const size_t bytes = n_tasks * sizeof(GradTask) + tab_n * sizeof(int) + (size_t)n_bf * n_bf * sizeof(double) +
                          (size_t)n_tasks * 24 * sizeof(double) + 4 * 256;
-    void *buf = nullptr;
-    GRPP_CUDA(cudaMalloc(&buf, bytes));
-    char *q = (char *)buf;
+    GRPP_CUDA(stp->grad.ensure(bytes));  // kept across calls: no allocation per chunk
+    char *q = (char *)stp->grad.p;
     auto take = [&q](size_t n) {
         char *r = q;
         q += (n + 255) & ~(size_t)255;
@@ -1678,7 +1678,6 @@ int run_grad_contract(const libgrpp_b200_batch_t *sub, const RunOptions &opt, co
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(out24, gd, (size_t)n_tasks * 24 * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(buf);
     if (e != cudaSuccess) {
         set_error(LIBGRPP_B200_ERR_CUDA, std::string("gradient contraction: ") + cudaGetErrorString(e));
         return LIBGRPP_B200_ERR_CUDA;
