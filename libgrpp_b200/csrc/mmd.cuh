@@ -61,8 +61,7 @@ struct MmdArgs {
     const int2 *rtab;
     const int *rtab_off;
     // dynamic schedule: warps pop positions from *queue (zeroed before the launch) and take
-    // item order[position]; the host orders items by decreasing estimated work. queue may be
-    // null: static round-robin over the items
+    // item order[position]; the host orders items by decreasing estimated work
     const int *order;
     int *queue;
 };
@@ -194,21 +193,12 @@ __global__ void __launch_bounds__(128) mmd_kernel(MmdArgs a)
     int2 *pdesc = reinterpret_cast<int2 *>(smem + wpb * ws) + warp * 32 * KPL;
 
     unsigned long long c_trip = 0, c_fl = 0;  // operation counters of this lane
-    int it_static = blockIdx.x * wpb + warp;
     for (;;) {
-        int it;
-        if (a.queue) {
-            int k = 0;
-            if (lane == 0) k = atomicAdd(a.queue, 1);
-            k = __shfl_sync(0xffffffffu, k, 0);
-            if (k >= a.n_items) break;
-            it = a.order[k];
-        } else {
-            it = it_static;
-            it_static += gridDim.x * wpb;
-            if (it >= a.n_items) break;
-        }
-        const MmdItem item = a.items[it];
+        int k = 0;
+        if (lane == 0) k = atomicAdd(a.queue, 1);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (k >= a.n_items) break;
+        const MmdItem item = a.items[a.order[k]];
         const int la = a.shell_L[item.bra], lb = a.shell_L[item.ket];
         const int nA = ncart(la), nB = ncart(lb), S = la + lb;
         const int la1 = la + 1, lb1 = lb + 1, S1 = S + 1;
