@@ -140,6 +140,7 @@ __device__ __forceinline__ void mmd_contract2(const double *E, const double *R0,
         for (int u = 0; u <= uy; u++) {
             const double exy0 = ex0 * E[oy0 + u], exy1 = ex1 * E[oy1 + u];
             const double *r0 = R0 + r0_row(S, t, u);
+#pragma unroll 4
             for (int v = 0; v <= vz; v++) {
                 const double rv = r0[v];
                 s0 += exy0 * ez0[v] * rv;
