@@ -135,3 +135,21 @@ def test_large_batch_runs_in_chunks(gpu_lib):
     plan.close()
     for x, y in zip(chunked, whole):
         assert np.array_equal(x, y)
+
+
+def test_batched_call_into_page_locked_outputs(gpu_lib):
+    """The batched call writes into caller arrays in page-locked memory (libgrpp_b200_host_alloc)
+    exactly what it returns in fresh arrays; the arrays are reused across calls."""
+    S = synthetic.config1()
+    a, b, c = S.all_tasks()
+    sel = np.random.default_rng(7).choice(len(a), 3000, replace=False)
+    batch = S.batch(a[sel], b[sel], c[sel])
+    n = int(batch.block_offsets()[-1])
+    fresh = gpu_lib.full_grpp_batch(batch)
+    outs = [gpu_lib.pinned_empty(n + 5) for _ in range(4)]
+    for _ in range(2):
+        got = gpu_lib.full_grpp_batch(batch, out=outs)
+        for x, y in zip(got, fresh):
+            assert np.array_equal(x, y)
+    with pytest.raises(ValueError):
+        gpu_lib.full_grpp_batch(batch, out=[np.empty(n, dtype=np.float32) for _ in range(4)])
