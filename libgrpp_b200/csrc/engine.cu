@@ -1,7 +1,8 @@
 // GRPP engine: the single CUDA translation unit (device tables, kernels, host
 // orchestration of a batch of (shell A, shell B, centre C) tasks).
 //
-// Pipeline of one batch, all on one stream:
+// Pipeline of one batch (kernels and uploads on the state's stream; the batched call's
+// downloads of finished chunks on a second stream):
 //   1. atab_kernel    k-independent angular tensors, cached per device and (L, l)
 //   2. mmd_kernel     type 1 blocks <A|U_L|B> written straight into the arep output,
 //                     and <S|U_oc|oc>, <S|oc> Cartesian blocks for every (shell, centre)
@@ -12,6 +13,8 @@
 //                     predicted level first, then the grid walk
 //   5. final_kernel   per task: T1 + sum type 2 + sum 2/(2L+1) SO + outercore, in
 //                     libgrpp_full_grpp_integrals' accumulation order
+// mmd_kernel and final_kernel run persistent grids that pop work from a queue ordered by
+// estimated work, largest first; the walk does the same in learned mode.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
