@@ -473,6 +473,8 @@ struct Plan {
     int ocp_blocks = 0;
     RadialArgs rad;
     int rad_blocks = 0, scr_blocks = 0;
+    double *wu = nullptr;  // w U_p(r) table (scratch), filled by wu_table_kernel before the walk
+    int wu_grpps = 0, wu_blocks = 0;
     size_t rad_smem = 0;
     FinalArgs fin;
     FinalSmem fin_smem_layout;
@@ -854,7 +856,14 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     const int64_t flag_words = (qn + nrad + 2 * 8) / 8 + 1;  // entry flags + per-task walk flags, in doubles
     // per radial item: stop level, predicted level (int8), order (int); learned-mode control words
     const int64_t lm_words = (2 * nrad + 4 * nrad + 16 * 4) / 8 + 4;
-    const size_t scratch_bytes = (size_t)(3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words + lm_words) * sizeof(double);
+    // table of w U_p(r) per GRPP, semilocal potential slot and grid point (wu_table_kernel),
+    // when the batch walks a grid and the table stays below 256 MiB
+    int wu_npot = 0;
+    for (int g = 0; g < ng; g++) wu_npot = std::max(wu_npot, g_sl_n[g]);
+    int64_t wu_words = rad_task.empty() ? 0 : (int64_t)ng * wu_npot * kRadGridPts;
+    if (wu_words * (int64_t)sizeof(double) > (int64_t(256) << 20)) wu_words = 0;
+    const size_t scratch_bytes =
+        (size_t)(3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words + lm_words + wu_words) * sizeof(double);
     GRPP_CUDA(bscr->ensure(scratch_bytes));
     GRPP_CUDA(bout->ensure((size_t)4 * std::max<int64_t>(out_tot, 1) * sizeof(double)));
     P.scratch_bytes = (int64_t)scratch_bytes;
@@ -867,6 +876,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     int8_t *predd = stopd + nrad;
     int *orderd = (int *)(((uintptr_t)(predd + nrad) + 15) & ~(uintptr_t)15);
     int *lmctld = orderd + nrad;
+    double *wud = wu_words > 0 ? (double *)bscr->p + (3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words + lm_words) : nullptr;
     P.stop_level = stopd;
     P.pred_level = predd;
     P.order = orderd;
@@ -1009,6 +1019,11 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         CHECK_INPUT(smem <= 160 * 1024, "radial grid chunk of this batch exceeds one block's shared memory");
         r.list_max = (int)rad_list_max;
         r.chunk_doubles = chunk_doubles;
+        r.wu = wud;
+        r.wu_npot = wu_npot;
+        P.wu = wud;
+        P.wu_grpps = ng;
+        P.wu_blocks = (int)std::min<int64_t>((wu_words + 255) / 256, (int64_t)nsm * 16);
         P.rad = r;
         P.rad_blocks = (int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 16);
         int scr_occ = 0;
@@ -1140,6 +1155,10 @@ int plan_launch(Plan &P)
             ra.order = P.order;
             ra.pred_level = P.pred_level;
             GRPP_CUDA(cudaEventRecord(ev[5], s));
+        }
+        if (P.wu) {
+            wu_table_kernel<<<P.wu_blocks, 256, 0, s>>>(P.rad, P.wu_grpps, P.wu);
+            GRPP_CUDA(cudaGetLastError());
         }
         radial_walk_kernel<<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(ra);
         GRPP_CUDA(cudaGetLastError());

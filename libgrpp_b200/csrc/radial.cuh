@@ -70,6 +70,11 @@ struct RadialArgs {
     // walk: two lists of active entry indices (uint16) of up to list_max entries each, after
     // chunk_doubles doubles of point arrays in dynamic shared memory; list_max = 0: no lists
     int list_max, chunk_doubles;
+    // w U_p(r) at every grid point per GRPP and semilocal potential slot, at
+    // wu[(grpp * wu_npot + slot) * kRadGridPts + point] (wu_table_kernel); null: the walk
+    // evaluates the potential terms itself
+    const double *wu;
+    int wu_npot;
     // entries the angular sums read, per item: u_off[item] = first used index; per class
     // (L, la, lb) ucls = {offset into ulist, count}; ulist = entry offsets within a potential's block
     const int64_t *u_off;
@@ -117,6 +122,7 @@ struct RadialShared {
     int la, lb, np_a, np_b, npot, nterm_tot, d_n;
     int l1max_all, l2max_all;
     int one_centre;
+    int grpp;
     int n_entries;
     int any_active;
     double ca[kRadMaxPrims], xa[kRadMaxPrims], ka[kRadMaxPrims];
@@ -475,6 +481,7 @@ __device__ void load_task(const RadialArgs &a, int item, RadialShared &sh, int t
         sh.lb = a.shell_L[sb];
         sh.d_n = sh.la + sh.lb + 1;
         const int g = a.centre_grpp[c];
+        sh.grpp = g;
         sh.npot = a.grpp_sl_n[g];
         int e = 0, nt = 0, l1m = 0, l2m = 0;
         for (int p = 0; p < sh.npot; p++) {
@@ -695,6 +702,40 @@ __device__ __forceinline__ int level_last_point(int L) { return (1 << (L + 5)) -
 // The walk of a task stops at the first chunk boundary after which no entry is active;
 // points evaluated past that are never added. The orders, powers and potentials
 // evaluated per point shrink with the set of active entries.
+// w U_p(r) = w sum_k c_k r^(n_k-2) exp(-zeta_k r^2) at every point of the nested grid, for
+// every semilocal potential slot of every GRPP: the grid does not depend on the task, so
+// the walk reads these values instead of evaluating the terms for each task. Same point,
+// weight, terms, order and exact-zero skips as the walk's own evaluation.
+__global__ void wu_table_kernel(RadialArgs a, int n_grpps, double *wu)
+{
+    const int64_t total = (int64_t)n_grpps * a.wu_npot * kRadGridPts;
+    for (int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id < total; id += (int64_t)gridDim.x * blockDim.x) {
+        const int f = (int)(id % kRadGridPts);
+        const int64_t gp = id / kRadGridPts;
+        const int pp = (int)(gp % a.wu_npot), g = (int)(gp / a.wu_npot);
+        if (pp >= a.grpp_sl_n[g]) {
+            wu[id] = 0.0;
+            continue;
+        }
+        const int pot = a.sl_pot[a.grpp_sl_off[g] + pp];
+        int lev, i, nr;
+        walk_point(f, lev, i, nr);
+        double r, w;
+        log3_point(i, nr, r, w);
+        const double r2 = r * r, ir = 1.0 / r, ir2 = 1.0 / r2;
+        double u = 0.0;
+        for (int k = 0; k < a.pot_nprim[pot]; k++) {
+            const int o = a.pot_prim_off[pot] + k;
+            const double ex = exp(-a.pot_alpha[o] * r2);
+            if (ex == 0.0) continue;  // the term adds an exact zero
+            const int pw = a.pot_powers[o];
+            const double rp = pw == 2 ? 1.0 : (pw == 1 ? ir : ir2);  // r^(n-2)
+            u += a.pot_coef[o] * rp * ex;
+        }
+        wu[id] = w * u;
+    }
+}
+
 __global__ void __launch_bounds__(kRadThreads, 5) radial_walk_kernel(RadialArgs a)
 {
     __shared__ RadialShared sh;
@@ -780,8 +821,13 @@ __global__ void __launch_bounds__(kRadThreads, 5) radial_walk_kernel(RadialArgs 
                 double r, w;
                 log3_point(i, nr, r, w);
                 const double r2 = r * r, ir = 1.0 / r, ir2 = 1.0 / r2;
+                const double *wug = a.wu ? a.wu + (int64_t)sh.grpp * a.wu_npot * kRadGridPts + f0 + tid : nullptr;
                 for (int pp = 0; pp < npot; pp++) {
                     if (!((umask >> pp) & 1)) continue;
+                    if (wug) {
+                        cwu[pp * kRadRow + tid] = __ldg(wug + (int64_t)pp * kRadGridPts);
+                        continue;
+                    }
                     double u = 0.0;
                     for (int k = 0; k < sh.pn[pp]; k++) {
                         const int tk = sh.poff[pp] + k;
