@@ -475,6 +475,9 @@ struct Plan {
     int rad_blocks = 0, scr_blocks = 0;
     double *wu = nullptr;  // w U_p(r) table (scratch), filled by wu_table_kernel before the walk
     int wu_grpps = 0, wu_blocks = 0;
+    double *ftab = nullptr;  // F_l(r) tables per (shell, centre) pair (scratch), ftab_kernel
+    int ft_blocks = 0;
+    size_t ft_smem = 0;
     size_t rad_smem = 0;
     FinalArgs fin;
     FinalSmem fin_smem_layout;
@@ -643,6 +646,21 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     std::vector<MmdItem> items;
     std::vector<int> rad_task;
     std::vector<int64_t> rad_qoff, rad_uoff;
+    // (shell, centre) pairs of the radial items, for the F_l(r) tables (ftab_kernel)
+    std::map<int64_t, int> fpair_of;
+    std::vector<int> fp_shell, fp_centre, fp_lmax, item_fa, item_fb;
+    auto fpair = [&](int shell, int centre, int lmax) {
+        const int64_t key = (int64_t)shell * b->n_centres + centre;
+        auto ins = fpair_of.insert({key, (int)fp_shell.size()});
+        if (ins.second) {
+            fp_shell.push_back(shell);
+            fp_centre.push_back(centre);
+            fp_lmax.push_back(lmax);
+        } else {
+            fp_lmax[ins.first->second] = std::max(fp_lmax[ins.first->second], lmax);
+        }
+        return ins.first->second;
+    };
     int64_t qtot = 0, utot = 0, rad_list_max = 0;
     std::vector<int2> ucls((kMaxL + 1) * (kMaxL + 1) * (kMaxL + 1), int2{0, 0});
     std::vector<uint8_t> ucls_set(ucls.size(), 0);
@@ -673,10 +691,11 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
             rad_task.push_back((int)t);
             rad_qoff.push_back(qtot);
             rad_uoff.push_back(utot);
-            int e = 0;
+            int e = 0, Lmx = 0;
             int64_t item_used = 0;
             for (int i = 0; i < g_sl_n[g]; i++) {
                 const int L = p_L[sl_pot[g_sl_off[g] + i]];
+                Lmx = std::max(Lmx, L);
                 e += (L + la + 1) * (L + lb + 1) * (la + lb + 1);
                 const int key = (L * (kMaxL + 1) + la) * (kMaxL + 1) + lb;
                 if (!ucls_set[key]) {
@@ -695,6 +714,8 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
                 atab_flag[L * (kMaxL + 1) + lb] = 1;
             }
             CHECK_INPUT(e <= kRadMaxEntries, "radial table larger than 16384 entries for one task");
+            item_fa.push_back(fpair(A, C, Lmx + la));
+            item_fb.push_back(fpair(B, C, Lmx + lb));
             CHECK_INPUT(std::max(rad_l1, rad_l2) <= kRadMaxLam && la + lb + 1 <= kRadMaxN, "angular momentum too high for the radial path");
             qtot += e;
             rad_list_max = std::max(rad_list_max, item_used);
@@ -799,6 +820,13 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     std::vector<int2> mmd_rtab;
     mmd_update_tables(mmd_lmax, mmd_smax, mmd_etab, mmd_etab_off, mmd_rtab, mmd_rtab_off);
 
+    // F_l(r) tables per (shell, centre) pair: (lmax + 1) rows of grid points each, when they
+    // stay below 8 GiB
+    std::vector<int64_t> fp_off(fp_shell.size() + 1, 0);
+    for (size_t k = 0; k < fp_shell.size(); k++) fp_off[k + 1] = fp_off[k] + (int64_t)(fp_lmax[k] + 1) * kRadGridPts;
+    int64_t f_words = rad_task.empty() ? 0 : fp_off.back();
+    if (f_words * (int64_t)sizeof(double) > (int64_t(8) << 30)) f_words = 0;
+
     // angular tensors
     for (int L = 0; L <= kMaxL; L++)
         for (int l = 0; l <= kMaxL; l++)
@@ -835,6 +863,8 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
                  o_ucls = pk.add(ucls), o_ulist = pk.add(ulist);
     const size_t o_bs = pk.add(blk_shell), o_bo = pk.add(blk_oc), o_bco = pk.add(blk_cart_off), o_bso = pk.add(blk_sph_off),
                  o_poffp = pk.add(proj_off), o_msch = pk.add(mmd_sched);
+    const size_t o_fps = pk.add(fp_shell), o_fpc = pk.add(fp_centre), o_fpl = pk.add(fp_lmax), o_fpo = pk.add(fp_off),
+                 o_ifa = pk.add(item_fa), o_ifb = pk.add(item_fb);
     const size_t o_met = pk.add(mmd_etab), o_meto = pk.add(mmd_etab_off), o_mrt = pk.add(mmd_rtab),
                  o_mrto = pk.add(mmd_rtab_off), o_mord = pk.add(mmd_order), o_ford = pk.add(fin_order);
     std::vector<int8_t> stop_dummy;
@@ -863,7 +893,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     int64_t wu_words = rad_task.empty() ? 0 : (int64_t)ng * wu_npot * kRadGridPts;
     if (wu_words * (int64_t)sizeof(double) > (int64_t(256) << 20)) wu_words = 0;
     const size_t scratch_bytes =
-        (size_t)(3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words + lm_words + wu_words) * sizeof(double);
+        (size_t)(3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words + lm_words + wu_words + f_words) * sizeof(double);
     GRPP_CUDA(bscr->ensure(scratch_bytes));
     GRPP_CUDA(bout->ensure((size_t)4 * std::max<int64_t>(out_tot, 1) * sizeof(double)));
     P.scratch_bytes = (int64_t)scratch_bytes;
@@ -877,6 +907,8 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     int *orderd = (int *)(((uintptr_t)(predd + nrad) + 15) & ~(uintptr_t)15);
     int *lmctld = orderd + nrad;
     double *wud = wu_words > 0 ? (double *)bscr->p + (3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words + lm_words) : nullptr;
+    double *ftd = f_words > 0 ? (double *)bscr->p + (3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words + lm_words + wu_words)
+                              : nullptr;
     P.stop_level = stopd;
     P.pred_level = predd;
     P.order = orderd;
@@ -1021,6 +1053,22 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         r.chunk_doubles = chunk_doubles;
         r.wu = wud;
         r.wu_npot = wu_npot;
+        r.ftab = ftd;
+        r.fp_off = at<int64_t>(ib, o_fpo);
+        r.fp_shell = at<int>(ib, o_fps);
+        r.fp_centre = at<int>(ib, o_fpc);
+        r.fp_lmax = at<int>(ib, o_fpl);
+        r.item_fa = at<int>(ib, o_ifa);
+        r.item_fb = at<int>(ib, o_ifb);
+        r.n_fpairs = (int)fp_shell.size();
+        P.ftab = ftd;
+        {
+            int fl = 0;
+            for (int v : fp_lmax) fl = std::max(fl, v);
+            P.ft_smem = (size_t)(fl + 1) * kRadRow * sizeof(double);
+            const int64_t nblk = (int64_t)fp_shell.size() * ((kRadGridPts + kRadThreads - 1) / kRadThreads);
+            P.ft_blocks = (int)std::min<int64_t>(nblk, (int64_t)nsm * 16);
+        }
         P.wu = wud;
         P.wu_grpps = ng;
         P.wu_blocks = (int)std::min<int64_t>((wu_words + 255) / 256, (int64_t)nsm * 16);
@@ -1158,6 +1206,10 @@ int plan_launch(Plan &P)
         }
         if (P.wu) {
             wu_table_kernel<<<P.wu_blocks, 256, 0, s>>>(P.rad, P.wu_grpps, P.wu);
+            GRPP_CUDA(cudaGetLastError());
+        }
+        if (P.ftab) {
+            ftab_kernel<<<P.ft_blocks, kRadThreads, P.ft_smem, s>>>(P.rad, P.ftab);
             GRPP_CUDA(cudaGetLastError());
         }
         radial_walk_kernel<<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(ra);

@@ -75,6 +75,14 @@ struct RadialArgs {
     // evaluates the potential terms itself
     const double *wu;
     int wu_npot;
+    // F_l(r) = sum_i c_i N_i exp(-a_i (r-CS)^2) M_l(2 a_i CS r), l = 0..fp_lmax[k], at every grid
+    // point for each (shell, centre) pair k of the batch (ftab_kernel), at
+    // ftab[fp_off[k] + l * kRadGridPts + point]; item_fa / item_fb: the pairs (A, C) and (B, C)
+    // of an item. ftab null: the walk evaluates F itself
+    const double *ftab;
+    const int64_t *fp_off;
+    const int *fp_shell, *fp_centre, *fp_lmax, *item_fa, *item_fb;
+    int n_fpairs;
     // entries the angular sums read, per item: u_off[item] = first used index; per class
     // (L, la, lb) ucls = {offset into ulist, count}; ulist = entry offsets within a potential's block
     const int64_t *u_off;
@@ -123,6 +131,7 @@ struct RadialShared {
     int l1max_all, l2max_all;
     int one_centre;
     int grpp;
+    int64_t fa_off, fb_off;  // F tables of (A, C) and (B, C), when tabulated
     int n_entries;
     int any_active;
     double ca[kRadMaxPrims], xa[kRadMaxPrims], ka[kRadMaxPrims];
@@ -508,6 +517,10 @@ __device__ void load_task(const RadialArgs &a, int item, RadialShared &sh, int t
         sh.l2max_all = l2m;
         sh.np_a = a.rp_n[sa];
         sh.np_b = a.rp_n[sb];
+        if (a.ftab) {
+            sh.fa_off = a.fp_off[a.item_fa[item]];
+            sh.fb_off = a.fp_off[a.item_fb[item]];
+        }
     }
     __syncthreads();
     for (int i = tid; i < sh.np_a; i += nthr) {
@@ -702,6 +715,42 @@ __device__ __forceinline__ int level_last_point(int L) { return (1 << (L + 5)) -
 // The walk of a task stops at the first chunk boundary after which no entry is active;
 // points evaluated past that are never added. The orders, powers and potentials
 // evaluated per point shrink with the set of active entries.
+// F_l(r) of every (shell, centre) pair of the batch at every point of the nested grid, one
+// CTA per pair and chunk of 128 points: the same point, distance CS (as load_task forms it),
+// primitives, exact-zero skips and Bessel rows as the walk's own evaluation, so every order
+// l holds the walk's value. Dynamic shared memory: (max fp_lmax + 1) x kRadRow doubles.
+__global__ void __launch_bounds__(kRadThreads) ftab_kernel(RadialArgs a, double *ftab)
+{
+    extern __shared__ double cf[];
+    const int tid = threadIdx.x;
+    const int nchunk = (kRadGridPts + kRadThreads - 1) / kRadThreads;
+    for (int64_t blk = blockIdx.x; blk < (int64_t)a.n_fpairs * nchunk; blk += gridDim.x) {
+        const int pr = (int)(blk / nchunk), f = (int)(blk % nchunk) * kRadThreads + tid;
+        if (f >= kRadGridPts) continue;
+        const int s = a.fp_shell[pr], c = a.fp_centre[pr], lmax = a.fp_lmax[pr];
+        const double *So = a.shell_origin + 3 * s, *Co = a.centre_origin + 3 * c;
+        double CSv[3];
+        for (int d = 0; d < 3; d++) CSv[d] = Co[d] - So[d];
+        const double CS2 = CSv[0] * CSv[0] + CSv[1] * CSv[1] + CSv[2] * CSv[2];
+        const double CS = sqrt(CS2);
+        int lev, i, nr;
+        walk_point(f, lev, i, nr);
+        double r, w;
+        log3_point(i, nr, r, w);
+        for (int l = 0; l <= lmax; l++) cf[l * kRadRow + tid] = 0.0;
+        const double d2 = (r - CS) * (r - CS);
+        const int np = a.rp_n[s], off = a.rp_off[s];
+#pragma unroll 1
+        for (int q = 0; q < np; q++) {
+            const double x = a.rp_alpha[off + q];
+            const double e = a.rp_coef[off + q] * exp(-x * d2);
+            if (e != 0.0) bessel_row_acc(lmax, (2.0 * x * CS) * r, e, cf + tid, kRadRow);
+        }
+        double *dst = ftab + a.fp_off[pr] + f;
+        for (int l = 0; l <= lmax; l++) dst[(int64_t)l * kRadGridPts] = cf[l * kRadRow + tid];
+    }
+}
+
 // w U_p(r) = w sum_k c_k r^(n_k-2) exp(-zeta_k r^2) at every point of the nested grid, for
 // every semilocal potential slot of every GRPP: the grid does not depend on the task, so
 // the walk reads these values instead of evaluating the terms for each task. Same point,
@@ -839,17 +888,24 @@ __global__ void __launch_bounds__(kRadThreads, 5) radial_walk_kernel(RadialArgs 
                     }
                     cwu[pp * kRadRow + tid] = w * u;
                 }
-                for (int l = 0; l <= u1; l++) cf1[l * kRadRow + tid] = 0.0;
-                for (int l = 0; l <= u2; l++) cf2[l * kRadRow + tid] = 0.0;
+                if (a.ftab) {
+                    // F^A_l, F^B_l of this point from the (shell, centre) tables
+                    const double *FA = a.ftab + sh.fa_off + f0 + tid, *FB = a.ftab + sh.fb_off + f0 + tid;
+                    for (int l = 0; l <= u1; l++) cf1[l * kRadRow + tid] = __ldg(FA + (int64_t)l * kRadGridPts);
+                    for (int l = 0; l <= u2; l++) cf2[l * kRadRow + tid] = __ldg(FB + (int64_t)l * kRadGridPts);
+                } else {
+                    for (int l = 0; l <= u1; l++) cf1[l * kRadRow + tid] = 0.0;
+                    for (int l = 0; l <= u2; l++) cf2[l * kRadRow + tid] = 0.0;
+                }
                 const double dA2 = (r - sh.CA) * (r - sh.CA), dB2 = (r - sh.CB) * (r - sh.CB);
-                if (u1 >= 0) {
+                if (!a.ftab && u1 >= 0) {
 #pragma unroll 1
                     for (int q = 0; q < np_a; q++) {
                         const double e = sh.ca[q] * exp(-sh.xa[q] * dA2);
                         if (e != 0.0) bessel_row_acc(u1, sh.ka[q] * r, e, cf1 + tid, kRadRow);
                     }
                 }
-                if (u2 >= 0) {
+                if (!a.ftab && u2 >= 0) {
 #pragma unroll 1
                     for (int q = 0; q < np_b; q++) {
                         const double e = sh.cb[q] * exp(-sh.xb[q] * dB2);
