@@ -1275,10 +1275,10 @@ int plan_download(Plan &P, double *h_arep, double *h_sx, double *h_sy, double *h
 
 // Large batches run as consecutive chunks of tasks whose radial tables together stay
 // below kChunkEntries entries (24 bytes of device scratch each) and kChunkTasks tasks;
-// outputs land at each chunk's offset in the caller's arrays. Chunks of 16384 tasks keep
+// outputs land at each chunk's offset in the caller's arrays. Chunks of 32768 tasks keep
 // every kernel's grid several waves deep while the host work of one chunk hides behind
 // the GPU work of the previous one.
-constexpr int64_t kChunkEntries = int64_t(1) << 27, kChunkTasks = int64_t(1) << 14;
+constexpr int64_t kChunkEntries = int64_t(1) << 27, kChunkTasks = int64_t(1) << 15;
 
 int run_full_batch(const libgrpp_b200_batch_t *b, const RunOptions &opt, double *h_arep, double *h_sx, double *h_sy,
                    double *h_sz, RunStats *stats)

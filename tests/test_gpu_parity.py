@@ -120,7 +120,7 @@ def test_h2o_gradients(gpu_lib):
 
 
 def test_large_batch_runs_in_chunks(gpu_lib):
-    """A batch larger than one chunk (16384 tasks, and here also more than 2^27 radial
+    """A batch larger than one chunk (32768 tasks, and here also more than 2^27 radial
     entries) through the batched entry point, which splits it and overlaps the chunks,
     equals the same tasks run as one plan."""
     S = synthetic.config1()
