@@ -197,6 +197,12 @@ struct FinalArgs {
     // task order[position], largest estimated work first; queue may be null: static round-robin
     const int *order;
     int *queue;
+    // omega tables per (shell, centre) pair (omega_tab_kernel): for each semilocal potential
+    // of the centre's GRPP in order, omega[abc][slot][m] of that side, from om_off[pair];
+    // task_fpa / task_fpb: the pairs (A, C) and (B, C) of a task. omtab null: computed here
+    const double *omtab;
+    const int64_t *om_off;
+    const int *task_fpa, *task_fpb;
 };
 
 // RSH values S_{l mu}(k/|k|) for l = 0..lmax (spherical_harmonics.c:227-280); out[l*(2*kFinMaxLam+1) + mu + l]
@@ -246,6 +252,98 @@ __device__ __forceinline__ double lmat_val(int L, int comp, int m1, int m2)
 {
     const int d = 2 * L + 1;
     return c_tab.lmat[c_tab.lmat_off[L] + comp * d * d + (m1 + L) * d + (m2 + L)];
+}
+
+// Omega tables of one side for every (shell, centre) pair: a CTA per pair computes the
+// real spherical harmonics of the unit vector along k = -2 a (C - S) (a the shell's first
+// exponent) and, for each semilocal potential of the centre's GRPP in order,
+// omega[abc][slot][m] = sum_mu S_{lam mu} Atab[abc][slot][mu][m] with the skips of
+// angular_integrals.c:78-108 — the same expressions as final_kernel's own evaluation.
+// Dynamic shared memory: (lam_max + 1) x sm.rsh_stride doubles.
+__global__ void __launch_bounds__(kFinThreads) omega_tab_kernel(FinalArgs a, FinalSmem sm, const int *op_shell,
+                                                                const int *op_centre, int n_pairs, double *omtab)
+{
+    extern __shared__ double rsh[];
+    __shared__ double upow[3][kFinMaxLam + 1];
+    __shared__ int8_t nabc[n_abc(kMaxL)];
+    const int tid = threadIdx.x, rs = sm.rsh_stride;
+    for (int pr = blockIdx.x; pr < n_pairs; pr += gridDim.x) {
+        const int sx = op_shell[pr], c = op_centre[pr], l = a.shell_L[sx], g = a.centre_grpp[c];
+        const int nsl = a.grpp_sl_n[g];
+        int lam_max = 0;
+        for (int p = 0; p < nsl; p++) lam_max = max(lam_max, a.pot_L[a.sl_pot[a.grpp_sl_off[g] + p]] + l);
+        double k[3];
+        const double al = a.prim_alpha[a.shell_prim_off[sx]];
+        for (int d = 0; d < 3; d++) k[d] = -2.0 * (al * (a.centre_origin[3 * c + d] - a.shell_origin[3 * sx + d]));
+        const double len = sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
+        double u[3] = {0, 0, 0};
+        if (len > kZeroThresh) {
+            const double inv = 1.0 / len;
+            for (int d = 0; d < 3; d++) u[d] = k[d] * inv;
+        }
+        __syncthreads();  // the previous pair's readers of upow, nabc and rsh are done
+        if (tid < 3) {
+            const double ud = tid == 0 ? u[0] : (tid == 1 ? u[1] : u[2]);
+            double pw = 1.0;
+            upow[tid][0] = pw;
+            for (int i = 1; i <= lam_max; i++) {
+                pw *= ud;
+                upow[tid][i] = pw;
+            }
+        }
+        for (int e = tid; e < n_abc(l); e += kFinThreads) {
+            int idx = e, aa, bb;
+            for (aa = 0; aa <= l; aa++) {
+                const int cnt = (l - aa + 1) * (l - aa + 2) / 2;
+                if (idx < cnt) break;
+                idx -= cnt;
+            }
+            for (bb = 0; bb <= l - aa; bb++) {
+                const int cnt = l - aa - bb + 1;
+                if (idx < cnt) break;
+                idx -= cnt;
+            }
+            nabc[e] = (int8_t)(aa + bb + idx);
+        }
+        __syncthreads();
+        const int nlm = (lam_max + 1) * (lam_max + 1);
+        for (int e = tid; e < nlm; e += kFinThreads) {
+            int ll = (int)sqrtf((float)e);
+            while (ll * ll > e) ll--;
+            while ((ll + 1) * (ll + 1) <= e) ll++;
+            const int mu = e - ll * ll - ll;
+            const int nc = ncart(ll);
+            const int8_t *cc = c_tab.rsh_comb + 3 * c_tab.rsh_comb_off[ll];
+            const double *y = c_tab.rsh_coef + c_tab.rsh_off[ll] + (mu + ll) * nc;
+            double v = 0.0;
+            for (int q = 0; q < nc; q++) v += y[q] * (upow[0][cc[3 * q]] * upow[1][cc[3 * q + 1]] * upow[2][cc[3 * q + 2]]);
+            rsh[ll * rs + mu + ll] = v;
+        }
+        __syncthreads();
+        int64_t off = a.om_off[pr];
+        for (int p = 0; p < nsl; p++) {
+            const int L = a.pot_L[a.sl_pot[a.grpp_sl_off[g] + p]];
+            const int sl = lam_slots(L, l), nab = n_abc(l), nm = 2 * L + 1, nmu = 2 * (L + l) + 1;
+            const double *At = a.atab + a.atab_off[L * (kMaxL + 2) + l];
+            for (int e = tid; e < nab * sl * nm; e += kFinThreads) {
+                const int m = e % nm, slot = (e / nm) % sl, abc = e / (nm * sl);
+                const int n = nabc[abc];
+                double w = 0.0;
+                if (slot < lam_count(L, n)) {
+                    const int lam = lam_lo(L, n) + 2 * slot;
+                    const double *S = rsh + lam * rs;
+                    const double *Ap = At + ((int64_t)(abc * sl + slot) * nmu) * nm + m;
+                    for (int mu = -lam; mu <= lam; mu++) {
+                        const double rv = S[mu + lam];
+                        if (fabs(rv) < kZeroThresh) continue;
+                        w += Ap[(int64_t)(mu + lam) * nm] * rv;
+                    }
+                }
+                omtab[off + e] = w;
+            }
+            off += (int64_t)nab * sl * nm;
+        }
+    }
 }
 
 __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSmem sm)
@@ -318,7 +416,25 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
             }
             __syncthreads();
             // RSH values with stride rs (rsh_values uses 2*kFinMaxLam+1; use a local variant)
-            {
+            const bool omt = a.omtab != nullptr;
+            if (omt) {  // only the |abc| tables are needed: omega comes from the pair tables
+                for (int e = tid; e < n_abc(la) + n_abc(lb); e += kFinThreads) {
+                    const bool sideB = e >= n_abc(la);
+                    const int l = sideB ? lb : la;
+                    int idx = sideB ? e - n_abc(la) : e, aa, bb;
+                    for (aa = 0; aa <= l; aa++) {
+                        const int cnt = (l - aa + 1) * (l - aa + 2) / 2;
+                        if (idx < cnt) break;
+                        idx -= cnt;
+                    }
+                    for (bb = 0; bb <= l - aa; bb++) {
+                        const int cnt = l - aa - bb + 1;
+                        if (idx < cnt) break;
+                        idx -= cnt;
+                    }
+                    (sideB ? nabcB : nabcA)[sideB ? e - n_abc(la) : e] = (int8_t)(aa + bb + idx);
+                }
+            } else {
                 const double lenA = sqrt(kA[0] * kA[0] + kA[1] * kA[1] + kA[2] * kA[2]);
                 const double lenB = sqrt(kB[0] * kB[0] + kB[1] * kB[1] + kB[2] * kB[2]);
                 double uA[3] = {0, 0, 0}, uB[3] = {0, 0, 0};
@@ -393,6 +509,7 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
             }
             const int64_t qbase = a.task_q_off[t];
             int64_t qoff = 0;
+            int64_t omoA = omt ? a.om_off[a.task_fpa[t]] : 0, omoB = omt ? a.om_off[a.task_fpb[t]] : 0;
             const int n_arep = a.grpp_n_arep[g];
             for (int p = 0; p < nsl; p++) {
                 const int L = a.pot_L[a.sl_pot[a.grpp_sl_off[g] + p]];
@@ -405,7 +522,13 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                 const double *AtB = a.atab + a.atab_off[L * (kMaxL + 2) + lb];
                 __syncthreads();
                 // omega tables: omega[abc][slot][m] = sum_mu S_{lam mu} Atab (angular_integrals.c:78-108)
-                for (int e = tid; e < nabA * slA * nm + nabB * slB * nm; e += kFinThreads) {
+                if (omt) {
+                    for (int e = tid; e < nabA * slA * nm; e += kFinThreads) omA[e] = a.omtab[omoA + e];
+                    for (int e = tid; e < nabB * slB * nm; e += kFinThreads) omB[e] = a.omtab[omoB + e];
+                    omoA += nabA * slA * nm;
+                    omoB += nabB * slB * nm;
+                }
+                for (int e = tid; !omt && e < nabA * slA * nm + nabB * slB * nm; e += kFinThreads) {
                     const bool sideB = e >= nabA * slA * nm;
                     const int r = sideB ? e - nabA * slA * nm : e;
                     const int sl = sideB ? slB : slA, nab = sideB ? nabB : nabA, l = sideB ? lb : la;

@@ -478,6 +478,10 @@ struct Plan {
     double *ftab = nullptr;  // F_l(r) tables per (shell, centre) pair (scratch), ftab_kernel
     int ft_blocks = 0;
     size_t ft_smem = 0;
+    double *omtab = nullptr;  // omega tables per (shell, centre) pair (scratch), omega_tab_kernel
+    const int *om_shell = nullptr, *om_centre = nullptr;
+    int om_pairs = 0, om_blocks = 0;
+    size_t om_smem = 0;
     size_t rad_smem = 0;
     FinalArgs fin;
     FinalSmem fin_smem_layout;
@@ -649,6 +653,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     // (shell, centre) pairs of the radial items, for the F_l(r) tables (ftab_kernel)
     std::map<int64_t, int> fpair_of;
     std::vector<int> fp_shell, fp_centre, fp_lmax, item_fa, item_fb;
+    std::vector<int> task_fpa(nt, -1), task_fpb(nt, -1);
     auto fpair = [&](int shell, int centre, int lmax) {
         const int64_t key = (int64_t)shell * b->n_centres + centre;
         auto ins = fpair_of.insert({key, (int)fp_shell.size()});
@@ -716,6 +721,8 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
             CHECK_INPUT(e <= kRadMaxEntries, "radial table larger than 16384 entries for one task");
             item_fa.push_back(fpair(A, C, Lmx + la));
             item_fb.push_back(fpair(B, C, Lmx + lb));
+            task_fpa[t] = item_fa.back();
+            task_fpb[t] = item_fb.back();
             CHECK_INPUT(std::max(rad_l1, rad_l2) <= kRadMaxLam && la + lb + 1 <= kRadMaxN, "angular momentum too high for the radial path");
             qtot += e;
             rad_list_max = std::max(rad_list_max, item_used);
@@ -826,6 +833,20 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     for (size_t k = 0; k < fp_shell.size(); k++) fp_off[k + 1] = fp_off[k] + (int64_t)(fp_lmax[k] + 1) * kRadGridPts;
     int64_t f_words = rad_task.empty() ? 0 : fp_off.back();
     if (f_words * (int64_t)sizeof(double) > (int64_t(8) << 30)) f_words = 0;
+    // omega tables per (shell, centre) pair (omega_tab_kernel): per semilocal potential of the
+    // centre's GRPP, n_abc(l) x slots x (2L+1) values; below 2 GiB
+    std::vector<int64_t> om_off(fp_shell.size() + 1, 0);
+    for (size_t k = 0; k < fp_shell.size(); k++) {
+        const int l = sh_L[fp_shell[k]], g = b->centre_grpp[fp_centre[k]];
+        int64_t w = 0;
+        for (int i = 0; i < g_sl_n[g]; i++) {
+            const int L = p_L[sl_pot[g_sl_off[g] + i]];
+            w += (int64_t)n_abc(l) * lam_slots(L, l) * (2 * L + 1);
+        }
+        om_off[k + 1] = om_off[k] + w;
+    }
+    int64_t om_words = rad_task.empty() ? 0 : om_off.back();
+    if (om_words * (int64_t)sizeof(double) > (int64_t(2) << 30)) om_words = 0;
 
     // angular tensors
     for (int L = 0; L <= kMaxL; L++)
@@ -864,7 +885,8 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     const size_t o_bs = pk.add(blk_shell), o_bo = pk.add(blk_oc), o_bco = pk.add(blk_cart_off), o_bso = pk.add(blk_sph_off),
                  o_poffp = pk.add(proj_off), o_msch = pk.add(mmd_sched);
     const size_t o_fps = pk.add(fp_shell), o_fpc = pk.add(fp_centre), o_fpl = pk.add(fp_lmax), o_fpo = pk.add(fp_off),
-                 o_ifa = pk.add(item_fa), o_ifb = pk.add(item_fb);
+                 o_ifa = pk.add(item_fa), o_ifb = pk.add(item_fb), o_omo = pk.add(om_off), o_tfa = pk.add(task_fpa),
+                 o_tfb = pk.add(task_fpb);
     const size_t o_met = pk.add(mmd_etab), o_meto = pk.add(mmd_etab_off), o_mrt = pk.add(mmd_rtab),
                  o_mrto = pk.add(mmd_rtab_off), o_mord = pk.add(mmd_order), o_ford = pk.add(fin_order);
     std::vector<int8_t> stop_dummy;
@@ -893,7 +915,8 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     int64_t wu_words = rad_task.empty() ? 0 : (int64_t)ng * wu_npot * kRadGridPts;
     if (wu_words * (int64_t)sizeof(double) > (int64_t(256) << 20)) wu_words = 0;
     const size_t scratch_bytes =
-        (size_t)(3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words + lm_words + wu_words + f_words) * sizeof(double);
+        (size_t)(3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words + lm_words + wu_words + f_words + om_words) *
+        sizeof(double);
     GRPP_CUDA(bscr->ensure(scratch_bytes));
     GRPP_CUDA(bout->ensure((size_t)4 * std::max<int64_t>(out_tot, 1) * sizeof(double)));
     P.scratch_bytes = (int64_t)scratch_bytes;
@@ -909,6 +932,9 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     double *wud = wu_words > 0 ? (double *)bscr->p + (3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words + lm_words) : nullptr;
     double *ftd = f_words > 0 ? (double *)bscr->p + (3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words + lm_words + wu_words)
                               : nullptr;
+    double *omd = om_words > 0 ? (double *)bscr->p + (3 * qn + 2 * cn + 2 * sn + 16 + 16 + flag_words + lm_words + wu_words +
+                                                      f_words)
+                               : nullptr;
     P.stop_level = stopd;
     P.pred_level = predd;
     P.order = orderd;
@@ -1125,6 +1151,10 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         f.status = statusd;
         f.order = at<int>(ib, o_ford);
         f.queue = statusd + 9;
+        f.omtab = omd;
+        f.om_off = at<int64_t>(ib, o_omo);
+        f.task_fpa = at<int>(ib, o_tfa);
+        f.task_fpb = at<int>(ib, o_tfb);
         FinalSmem fs{};
         fs.rsh_stride = 2 * fin_lam + 1;
         fs.n_rsh = (fin_lam + 1) * fs.rsh_stride;
@@ -1146,6 +1176,12 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         const size_t smem = smem_base + (size_t)fs.n_w * sizeof(double);
         P.fin = f;
         P.fin_smem_layout = fs;
+        P.omtab = omd;
+        P.om_pairs = (int)fp_shell.size();
+        P.om_shell = at<int>(ib, o_fps);
+        P.om_centre = at<int>(ib, o_fpc);
+        P.om_smem = (size_t)fs.n_rsh * sizeof(double);
+        P.om_blocks = (int)std::min<int64_t>((int64_t)fp_shell.size(), (int64_t)nsm * 8);
         int fin_occ = 0;  // persistent grid over the task queue
         GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fin_occ, final_kernel, kFinThreads, smem));
         P.fin_blocks = (int)std::min<int64_t>(nt, (int64_t)nsm * std::max(fin_occ, 1));
@@ -1216,6 +1252,11 @@ int plan_launch(Plan &P)
         GRPP_CUDA(cudaGetLastError());
     }
     GRPP_CUDA(cudaEventRecord(ev[2], s));
+    if (P.omtab) {
+        omega_tab_kernel<<<P.om_blocks, kFinThreads, P.om_smem, s>>>(P.fin, P.fin_smem_layout, P.om_shell, P.om_centre,
+                                                                    P.om_pairs, P.omtab);
+        GRPP_CUDA(cudaGetLastError());
+    }
     final_kernel<<<P.fin_blocks, kFinThreads, P.fin_smem, s>>>(P.fin, P.fin_smem_layout);
     GRPP_CUDA(cudaGetLastError());
     GRPP_CUDA(cudaEventRecord(ev[3], s));
