@@ -651,20 +651,32 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     std::vector<int> rad_task;
     std::vector<int64_t> rad_qoff, rad_uoff;
     // (shell, centre) pairs of the radial items, for the F_l(r) tables (ftab_kernel)
+    // pair index per (shell, centre): a flat array when it is small, else a map
+    const int64_t n_sc = (int64_t)b->n_shells * b->n_centres;
+    std::vector<int> fpair_flat(n_sc <= (int64_t(1) << 24) ? n_sc : 0, -1);
     std::map<int64_t, int> fpair_of;
     std::vector<int> fp_shell, fp_centre, fp_lmax, item_fa, item_fb;
     std::vector<int> task_fpa(nt, -1), task_fpb(nt, -1);
     auto fpair = [&](int shell, int centre, int lmax) {
         const int64_t key = (int64_t)shell * b->n_centres + centre;
-        auto ins = fpair_of.insert({key, (int)fp_shell.size()});
-        if (ins.second) {
+        int idx = -1;
+        if (!fpair_flat.empty()) {
+            idx = fpair_flat[key];
+        } else {
+            const auto f = fpair_of.find(key);
+            if (f != fpair_of.end()) idx = f->second;
+        }
+        if (idx < 0) {
+            idx = (int)fp_shell.size();
+            if (!fpair_flat.empty()) fpair_flat[key] = idx;
+            else fpair_of[key] = idx;
             fp_shell.push_back(shell);
             fp_centre.push_back(centre);
             fp_lmax.push_back(lmax);
         } else {
-            fp_lmax[ins.first->second] = std::max(fp_lmax[ins.first->second], lmax);
+            fp_lmax[idx] = std::max(fp_lmax[idx], lmax);
         }
-        return ins.first->second;
+        return idx;
     };
     int64_t qtot = 0, utot = 0, rad_list_max = 0;
     std::vector<int2> ucls((kMaxL + 1) * (kMaxL + 1) * (kMaxL + 1), int2{0, 0});
@@ -781,19 +793,20 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
             auto ins = tab_id.insert({tab, (int)tab_id.size()});
             sh_tab[i] = ins.first->second;
         }
-        std::map<std::pair<int, int>, std::pair<int, int>> sched_of;  // -> (offset, rows)
+        const int ntab = (int)tab_id.size();
+        std::vector<std::pair<int, int>> sched_of((size_t)ntab * ntab, {-1, 0});  // (bra, ket) class -> (offset, rows)
         for (auto &it : items) {
             const int nA = ncart(sh_L[it.bra]), nB = ncart(sh_L[it.ket]);
             CHECK_INPUT(nA * nB <= 32 * mmd_kpl, "type 1 block larger than one pass of the pair schedule");
-            auto f = sched_of.find({sh_tab[it.bra], sh_tab[it.ket]});
-            if (f == sched_of.end()) {
+            std::pair<int, int> &f = sched_of[(size_t)sh_tab[it.bra] * ntab + sh_tab[it.ket]];
+            if (f.first < 0) {
                 const int off = (int)mmd_sched.size();
                 const int rows = mmd_pair_schedule(cart.data() + 3 * sh_co[it.bra], nA, cart.data() + 3 * sh_co[it.ket],
                                                    nB, mmd_kpl, mmd_sched);
-                f = sched_of.insert({{sh_tab[it.bra], sh_tab[it.ket]}, {off, rows}}).first;
+                f = {off, rows};
             }
-            it.sched = f->second.first;
-            it.sched_rows = f->second.second;
+            it.sched = f.first;
+            it.sched_rows = f.second;
         }
     }
     // estimated work per type 1 item: primitive triples x (Hermite + R entries + contraction terms)
