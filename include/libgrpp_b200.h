@@ -201,22 +201,23 @@ int libgrpp_b200_plan_learned_stats(const libgrpp_b200_plan_t *plan, double *ms_
 
 /* Allocation-free type 2 integrals (no counterpart in libgrpp).
  *
- * For callers that must not trigger device allocations: code running during CUDA
- * graph capture, processes whose device memory is owned by a pool or framework
- * allocator, services that must keep a fixed device footprint. For every task of
- * the batch, arep receives the sum over the centre GRPP's averaged (AREP)
- * semilocal potentials of the type 2 integrals (libgrpp_type2_integrals summed as
- * libgrpp_full_grpp_integrals does); U_L, spin-orbit and outercore parts are not
- * evaluated. Host arrays in and out, blocks laid out as in
- * libgrpp_b200_full_grpp_batch.
+ * For callers that must not trigger device allocations: processes whose device
+ * memory is owned by a pool or framework allocator, and services that must keep a
+ * fixed device footprint. For every task of the batch, arep receives the sum over
+ * the centre GRPP's averaged (AREP) semilocal potentials of the type 2 integrals
+ * (libgrpp_type2_integrals summed as libgrpp_full_grpp_integrals does); U_L,
+ * spin-orbit and outercore parts are not evaluated. Host arrays in and out, blocks
+ * laid out as in libgrpp_b200_full_grpp_batch.
  *
  * The call allocates no device memory: all device data live in static device
  * arrays loaded with the library, including one 32 MiB scratch array that holds
  * the call's inputs, working state and outputs. Batches needing more are
- * rejected with LIBGRPP_B200_ERR_INVALID (split them). The first call on a
- * device sets that device up (tables copied, scratch address taken); make it
- * before any stream capture. All calls share the scratch array: host calls are
- * serialised, and calls overlapping on the GPU would race. */
+ * rejected with LIBGRPP_B200_ERR_INVALID (split them); so are malformed batches,
+ * checked on the host before any CUDA call. The first call on a device sets that
+ * device up (tables copied, scratch address taken); make it before any stream
+ * capture. The call is synchronous (cudaMemcpy, legacy default stream) and
+ * returns when the results are on the host. All calls share the scratch array:
+ * host calls are serialised, and calls overlapping on the GPU would race. */
 int libgrpp_b200_type2_batch_noalloc(const libgrpp_b200_batch_t *batch, double *arep);
 
 #ifdef __cplusplus

@@ -1,11 +1,12 @@
 // Allocation-free entry point: libgrpp_b200_type2_batch_noalloc.
 //
-// Some callers cannot let a library call cudaMalloc: code that runs while a
-// CUDA graph is being captured, applications whose device memory is owned by a
-// pool or a framework allocator, and long-running services that must not grow
-// their device footprint after start-up. This translation unit serves them:
-// every device buffer it uses is file-scope static device memory, created when
-// the library is loaded and held until the process exits:
+// Some callers cannot let a library call cudaMalloc: applications whose device
+// memory is owned by a pool or framework allocator (a cudaMalloc behind the
+// allocator's back can fail once the pool holds the memory, and fragments what
+// it does not), and long-running services that must keep the device footprint
+// they had at start-up. This translation unit serves them: every device buffer
+// it uses is file-scope static device memory, created when the library is
+// loaded and held until the process exits:
 //   * the constant tables the kernels read (Bessel, RSH, factorials, ...),
 //   * one scratch array of kNoAllocScratchBytes (32 MiB) that holds a call's
 //     packed inputs, the angular tensors, the radial tables and their per-entry
@@ -16,9 +17,13 @@
 // tables; no file of the regular path is changed.
 //
 // Behaviour:
+//  * The batch is checked on the host before any CUDA call (indices, powers,
+//    Cartesian lists); a malformed batch returns LIBGRPP_B200_ERR_INVALID.
 //  * Set-up (tables copied with cudaMemcpyToSymbol, the scratch address taken
 //    with cudaGetSymbolAddress) happens on the first call on each device, with
 //    that device current; make that first call before any stream capture.
+//  * The call is synchronous: it copies with cudaMemcpy and launches on the
+//    legacy default stream, and returns when the results are on the host.
 //  * A batch whose packed size exceeds the scratch array is rejected with
 //    LIBGRPP_B200_ERR_INVALID and a message naming both sizes; nothing runs.
 //  * All calls share the scratch array, which keeps the last call's contents.
@@ -158,8 +163,52 @@ struct Arena {
 
 double host_gaussian_norm(int L, double a) { return std::pow(2 * a / kPi, 0.75) * std::pow(4 * a, 0.5 * L); }
 
+// Checks of every index and value the packing below reads, on the host and before any
+// CUDA call: a malformed batch is rejected with LIBGRPP_B200_ERR_INVALID whether or not
+// a device is present, and nothing is read outside the caller's arrays.
+int validate(const libgrpp_b200_batch_t *b)
+{
+    NA_CHECK(b != nullptr && b->n_tasks >= 0, "null batch or negative task count");
+    if (b->n_tasks == 0) return 0;
+    NA_CHECK(b->n_shells > 0 && b->n_centres > 0 && b->n_grpps > 0 && b->n_pots >= 0, "empty batch description");
+    for (int i = 0; i < b->n_shells; i++) {
+        const int L = b->shell_L[i];
+        NA_CHECK(L >= 0 && L <= kMaxL && b->shell_nprim[i] >= 1 && b->shell_nprim[i] <= kRadMaxPrims,
+                 "shell outside the supported limits (L <= 10, 1..64 primitives)");
+        NA_CHECK(b->shell_prim_off[i] >= 0 && b->shell_cart_off[i] >= 0, "negative shell offset");
+        for (int q = 0; q < ncart(L); q++) {
+            const int *c = b->cart_list + 3 * (b->shell_cart_off[i] + q);
+            NA_CHECK(c[0] >= 0 && c[1] >= 0 && c[2] >= 0 && c[0] + c[1] + c[2] == L, "invalid Cartesian component list");
+        }
+    }
+    for (int p = 0; p < b->n_pots; p++) {
+        NA_CHECK(b->pot_L[p] >= 0 && b->pot_L[p] <= kMaxL, "potential angular momentum outside 0..10");
+        NA_CHECK(b->pot_nprim[p] >= 0 && b->pot_prim_off[p] >= 0, "negative potential size or offset");
+        for (int k = 0; k < b->pot_nprim[p]; k++) {
+            const int n = b->pot_powers[b->pot_prim_off[p] + k];
+            NA_CHECK(n >= 0 && n <= 2, "potential power n must be 0, 1 or 2");
+        }
+    }
+    for (int g = 0; g < b->n_grpps; g++) {
+        NA_CHECK(b->grpp_n_arep[g] >= 0 && b->grpp_arep_off[g] >= 0, "negative potential count or offset in a GRPP");
+        for (int i = 0; i < b->grpp_n_arep[g]; i++) {
+            const int pot = b->grpp_pot_list[b->grpp_arep_off[g] + i];
+            NA_CHECK(pot >= 0 && pot < b->n_pots, "GRPP potential index out of range");
+        }
+    }
+    for (int c = 0; c < b->n_centres; c++)
+        NA_CHECK(b->centre_grpp[c] >= 0 && b->centre_grpp[c] < b->n_grpps, "centre GRPP index out of range");
+    for (int64_t t = 0; t < b->n_tasks; t++)
+        NA_CHECK(b->task_a[t] >= 0 && b->task_a[t] < b->n_shells && b->task_b[t] >= 0 && b->task_b[t] < b->n_shells &&
+                     b->task_c[t] >= 0 && b->task_c[t] < b->n_centres,
+                 "task index out of range");
+    return 0;
+}
+
 int run(const libgrpp_b200_batch_t *b, double *h_arep)
 {
+    if (int rc = validate(b)) return rc;
+    if (b->n_tasks == 0) return 0;
     int dev = 0;
     NA_CUDA(cudaGetDevice(&dev));
     NA_CHECK(dev >= 0 && dev < kMaxDevices, "device index out of range");
@@ -167,9 +216,7 @@ int run(const libgrpp_b200_batch_t *b, double *h_arep)
     int rc = setup(dev);
     if (rc) return rc;
     const int64_t nt = b->n_tasks;
-    if (nt == 0) return 0;
     const int ns = b->n_shells;
-    NA_CHECK(ns > 0 && b->n_centres > 0 && b->n_grpps > 0, "empty batch description");
 
     // ---- shells, radial primitives (shrunk and normalised), Cartesian lists
     std::vector<int> sh_L(b->shell_L, b->shell_L + ns), sh_np(b->shell_nprim, b->shell_nprim + ns),

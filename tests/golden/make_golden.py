@@ -3,7 +3,7 @@
 Run here, where the reference tree and its compiled library exist:
 
     make -C oracle ref
-    python tests/golden/make_golden.py [--ref-root /root/reference]
+    python tests/golden/make_golden.py [--ref-root <libgrpp source tree>]   (default: $LIBGRPP_REFERENCE)
 
 For each of libgrpp's GRPP test directories (test/H2O, Cs, ThO, UO2, KCs) the
 molecule, basis and GRPP inputs are read with libgrpp_b200.formats, the
@@ -150,7 +150,7 @@ def make_gradient_fixture(n_tasks=160, seed=13):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--ref-root", default=os.environ.get("LIBGRPP_REFERENCE", "/root/reference"))
     ap.add_argument("--only", nargs="*")
     ap.add_argument("--pairs", type=int, default=48)
     args = ap.parse_args()

@@ -116,3 +116,35 @@ def test_batch_arrays_block_offsets():
     off = b.block_offsets()
     assert off[-1] == 40 * 40
     assert b.struct.n_tasks == 64
+
+
+def test_noalloc_rejects_malformed_batch_on_the_host():
+    """The allocation-free entry point checks the batch on the host before any CUDA call:
+    a potential power of 3, a GRPP potential index past n_pots or a centre GRPP index past
+    n_grpps returns LIBGRPP_B200_ERR_INVALID with no device present."""
+    from libgrpp_b200.capi import LibGRPP
+    from libgrpp_b200.system import BatchArrays
+    lib = LibGRPP(PRODUCT_LIB)
+    base = synthetic.config0().batch()
+    d0 = {k: v for k, v in base.__dict__.items() if not k.startswith("_")}
+
+    def bad(**changes):
+        d = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d0.items()}
+        for k, f in changes.items():
+            f(d[k])
+        return BatchArrays(**d)
+
+    def set0(v):
+        v[0] = 3
+
+    def set_idx(n):
+        def f(v):
+            v[0] = n
+        return f
+
+    for batch, what in ((bad(pot_powers=set0), "power"),
+                        (bad(grpp_pot_list=set_idx(len(base.pot_L))), "GRPP potential index"),
+                        (bad(centre_grpp=set_idx(len(base.grpp_UL))), "centre GRPP index")):
+        with pytest.raises(RuntimeError, match=what):
+            lib.type2_batch_noalloc(batch)
+        assert lib.last_error() == 1  # LIBGRPP_B200_ERR_INVALID
