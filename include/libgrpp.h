@@ -15,6 +15,10 @@
  *   libgrpp_grpp_t + builders ............. libgrpp/libgrpp.h:94-113, grpp.c:15-109
  *   integrators ........................... libgrpp/libgrpp.h:120-171
  *   gradients ............................. libgrpp/libgrpp.h:178-231
+ *   overlap, kinetic, momentum ............ libgrpp/overlap.h, kinetic.h, momentum.h,
+ *                                           overlap_gradient.h (libgrpp.h:237-241)
+ *   nuclear attraction .................... libgrpp/libgrpp.h:243-310, nuclear_attraction.c:31-236
+ *   nuclear charge models ................. libgrpp/nuclear_models.h:14-48
  *   parameters ............................ libgrpp/parameters.h:11-35
  *
  * All integrators return void, zero their outputs first, and write
@@ -171,6 +175,74 @@ void libgrpp_full_grpp_integrals_gradient(libgrpp_shell_t *shell_A, libgrpp_shel
                                           double *point_3d, double **grad_arep,
                                           double **grad_so_x, double **grad_so_y,
                                           double **grad_so_z);
+
+/* ---- other integrals (libgrpp.h:237-241) ------------------------------- */
+/* <A|B> (overlap.h:13, overlap.c:39-62) */
+void libgrpp_overlap_integrals(libgrpp_shell_t *shell_A, libgrpp_shell_t *shell_B, double *overlap_matrix);
+
+/* d<A|B>/d point_3d, grad is double*[3] (overlap_gradient.h:13-18, overlap_gradient.c:27-82) */
+void libgrpp_overlap_integrals_gradient(libgrpp_shell_t *shell_A, libgrpp_shell_t *shell_B, double *point_3d,
+                                        double **grad);
+
+/* <A| -1/2 nabla^2 |B> (kinetic.h:13, kinetic.c:34-57) */
+void libgrpp_kinetic_energy_integrals(libgrpp_shell_t *shell_A, libgrpp_shell_t *shell_B, double *kinetic_matrix);
+
+/* <A| d/dx |B>, <A| d/dy |B>, <A| d/dz |B> (momentum.h:13-19, momentum.c:34-68) */
+void libgrpp_momentum_integrals(libgrpp_shell_t *shell_A, libgrpp_shell_t *shell_B, double *momentum_x_matrix,
+                                double *momentum_y_matrix, double *momentum_z_matrix);
+
+/* ---- nuclear attraction (libgrpp.h:243-310) ------------------------------ */
+enum {
+    LIBGRPP_NUCLEAR_MODEL_POINT_CHARGE = 0,
+    LIBGRPP_NUCLEAR_MODEL_CHARGED_BALL,
+    LIBGRPP_NUCLEAR_MODEL_GAUSSIAN,
+    LIBGRPP_NUCLEAR_MODEL_FERMI,
+    LIBGRPP_NUCLEAR_MODEL_FERMI_BUBBLE,
+    LIBGRPP_NUCLEAR_MODEL_POINT_CHARGE_NUMERICAL
+};
+
+/* <A| V_nuc(|r - C|) |B> of a nucleus of charge Z at charge_origin; model_params: ball and
+ * Gaussian {R_rms}, Fermi {c, a}, Fermi bubble {c, a, k}, NULL for point charges
+ * (nuclear_attraction.c:31-119) */
+void libgrpp_nuclear_attraction_integrals(libgrpp_shell_t *shell_A, libgrpp_shell_t *shell_B, double *charge_origin,
+                                          int charge, int nuclear_model, double *model_params, double *coulomb_matrix);
+
+void libgrpp_nuclear_attraction_integrals_point_charge(libgrpp_shell_t *shell_A, libgrpp_shell_t *shell_B,
+                                                       double *charge_origin, int charge, double *coulomb_matrix);
+
+void libgrpp_nuclear_attraction_integrals_charged_ball(libgrpp_shell_t *shell_A, libgrpp_shell_t *shell_B,
+                                                       double *charge_origin, int charge, double r_rms,
+                                                       double *coulomb_matrix);
+
+void libgrpp_nuclear_attraction_integrals_gaussian_model(libgrpp_shell_t *shell_A, libgrpp_shell_t *shell_B,
+                                                         double *charge_origin, int charge, double r_rms,
+                                                         double *coulomb_matrix);
+
+void libgrpp_nuclear_attraction_integrals_fermi_model(libgrpp_shell_t *shell_A, libgrpp_shell_t *shell_B,
+                                                      double *charge_origin, int charge, double fermi_param_c,
+                                                      double fermi_param_a, double *coulomb_matrix);
+
+void libgrpp_nuclear_attraction_integrals_fermi_bubble_model(libgrpp_shell_t *shell_A, libgrpp_shell_t *shell_B,
+                                                             double *charge_origin, int charge, double param_c,
+                                                             double param_a, double param_k, double *coulomb_matrix);
+
+/* ---- nuclear charge models (nuclear_models.h:14-48) ------------------------ */
+#define FERMI_UNITS_TO_ATOMIC (1.0 / 52917.7210903)
+
+double libgrpp_estimate_nuclear_rms_radius_johnson_1985(int A);
+double libgrpp_estimate_nuclear_rms_radius_golovko_2008(int A);
+int libgrpp_estimate_fermi_model_parameters(double R_rms, double *c, double *a);
+double libgrpp_charge_density_ball(double r, double Z, double R_rms);
+double libgrpp_charge_density_gaussian(double r, double Z, double R_rms);
+double libgrpp_charge_density_fermi(double r, double Z, double c, double a);
+double libgrpp_charge_density_fermi_bubble(double r, double Z, double c, double a, double k);
+double libgrpp_rms_radius_fermi(int Z, double c, double a);
+double libgrpp_rms_radius_fermi_bubble(int Z, double c, double a, double k);
+double libgrpp_coulomb_potential_point(double r, double Z);
+double libgrpp_coulomb_potential_ball(double r, double Z, double R_rms);
+double libgrpp_coulomb_potential_gaussian(double r, double Z, double R_rms);
+double libgrpp_coulomb_potential_fermi(double r, double Z, double c, double a);
+double libgrpp_coulomb_potential_fermi_bubble(double r, double Z, double c, double a, double k);
 
 #ifdef __cplusplus
 }

@@ -151,6 +151,33 @@ int libgrpp_b200_grpp_gradient_contract(const libgrpp_b200_batch_t *batch, int r
                                         const int *centre_atom, const double *atom_xyz, int n_atoms, const int *bf_off,
                                         int n_bf, const double *D, double *g);
 
+/* One-electron integrals over the batch's shell pairs (task_a, task_b; task_c is not read
+ * and the batch may have no centres), blocks laid out as in libgrpp_b200_full_grpp_batch.
+ * Per pair the values of libgrpp_overlap_integrals (overlap.c:39-62),
+ * libgrpp_kinetic_energy_integrals (kinetic.c:34-57) and libgrpp_momentum_integrals
+ * (momentum.c:34-68; out0..out2 = x, y, z), computed on the GPU. */
+enum {
+    LIBGRPP_B200_ONEE_OVERLAP = 0,
+    LIBGRPP_B200_ONEE_KINETIC = 1,
+    LIBGRPP_B200_ONEE_MOMENTUM = 2
+};
+int libgrpp_b200_onee_batch(const libgrpp_b200_batch_t *batch, int kind, double *out0, double *out1, double *out2);
+
+/* Nuclear attraction over every task (A, B, C): the nucleus of charge centre_charge[C] at
+ * centre C, libgrpp_nuclear_attraction_integrals per task (nuclear_attraction.c:31-119).
+ * nuclear_model is a LIBGRPP_NUCLEAR_MODEL_* value; centre_params[3*C..] holds the model's
+ * parameters (ball, Gaussian: R_rms; Fermi: c, a; Fermi bubble: c, a, k; ignored for point
+ * charges). Point charges run through the type 1 McMurchie-Davidson kernel with a zero
+ * exponent, the other models through the numeric type 1 kernel. centre_grpp is not read. */
+int libgrpp_b200_nuclear_attraction_batch(const libgrpp_b200_batch_t *batch, int nuclear_model,
+                                          const double *centre_charge, const double *centre_params, double *out);
+
+/* <A| U_L |B> of the centre GRPP's local part by numeric radial quadrature instead of
+ * McMurchie-Davidson: libgrpp's evaluate_type1_integral_primitive_gaussians scheme
+ * (type1_integrals.c:109-270, radial_type1_integral.c:73-325) per primitive pair; the
+ * independent evaluation of the same integrals libgrpp_type1_integrals gives. L_A + L_B <= 12. */
+int libgrpp_b200_type1_numeric_batch(const libgrpp_b200_batch_t *batch, double *arep);
+
 /* Learned grid-level model (no counterpart in libgrpp).
  *
  * libgrpp's type 2 radial quadrature (radial_type2_integral.c:242-318) doubles a

@@ -20,7 +20,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 
 SOURCES = ["engine.cu", "tables.cpp", "capi.cpp", "noalloc.cu"]
 HEADERS = ["grpp_common.cuh", "specfunc.cuh", "mmd.cuh", "radial.cuh", "angular.cuh", "level_model.cuh", "gradient.cuh", "tables.h",
-           "engine.h"]
+           "engine.h", "onee.cuh", "nucmodel.h"]
 
 
 def _newer(target, deps):

@@ -66,6 +66,9 @@ class LibGRPP:
             "libgrpp_type1_integrals_gradient": (None, [_V, _V, _D, _V, _D, ct.POINTER(_D)]),
             "libgrpp_type2_integrals_gradient": (None, [_V, _V, _D, _V, _D, ct.POINTER(_D)]),
             "libgrpp_spin_orbit_integrals_gradient": (None, [_V, _V, _D, _V, _D, ct.POINTER(_D), ct.POINTER(_D), ct.POINTER(_D)]),
+            "libgrpp_outercore_potential_integrals_gradient": (None, [_V, _V, _D, ct.c_int, ct.POINTER(_V), ct.POINTER(_V), _D,
+                                                                      ct.POINTER(_D), ct.POINTER(_D), ct.POINTER(_D),
+                                                                      ct.POINTER(_D)]),
         }
         for name, (res, args) in proto.items():
             f = getattr(L, name)
@@ -97,6 +100,16 @@ class LibGRPP:
                   [_V, ct.c_int, _I, _I, _D, ct.c_int, _I, ct.c_int, _D, _D])
         self._opt("libgrpp_b200_set_level_model", ct.c_int, [_F])
         self._opt("libgrpp_b200_level_samples", ct.c_int, [_V, _F, _B, ct.POINTER(ct.c_int64)])
+        self._opt("libgrpp_overlap_integrals", None, [_V, _V, _D])
+        self._opt("libgrpp_kinetic_energy_integrals", None, [_V, _V, _D])
+        self._opt("libgrpp_momentum_integrals", None, [_V, _V, _D, _D, _D])
+        self._opt("libgrpp_overlap_integrals_gradient", None, [_V, _V, _D, ct.POINTER(_D)])
+        self._opt("libgrpp_nuclear_attraction_integrals", None, [_V, _V, _D, ct.c_int, ct.c_int, _D, _D])
+        self._opt("libgrpp_estimate_nuclear_rms_radius_johnson_1985", ct.c_double, [ct.c_int])
+        self._opt("libgrpp_estimate_fermi_model_parameters", ct.c_int, [ct.c_double, _D, _D])
+        self._opt("libgrpp_b200_onee_batch", ct.c_int, [_V, ct.c_int, _D, _D, _D])
+        self._opt("libgrpp_b200_nuclear_attraction_batch", ct.c_int, [_V, ct.c_int, _D, _D, _D])
+        self._opt("libgrpp_b200_type1_numeric_batch", ct.c_int, [_V, _D])
         self._opt("libgrpp_b200_mlp_grad", ct.c_int, [_F, _F, _B, ct.c_int, _F, _F])
         self._opt("libgrpp_b200_mlp_train", ct.c_int, [_F, _B, ct.c_int64, ct.c_int, ct.c_int, ct.c_float, ct.c_uint32, _F, _F])
         self._opt("libgrpp_b200_mlp_predict", ct.c_int, [_F, _F, ct.c_int64, _B])
@@ -169,6 +182,98 @@ class LibGRPP:
             hA, hB, hg, _dp(np.ascontiguousarray(C, dtype=np.float64)), _dp(np.ascontiguousarray(D, dtype=np.float64)),
             *ptrs)
         return g.reshape(4, 3, nA, nB)
+
+    def _grad_ptrs(self, g):
+        return [(_D * 3)(*[g[m, k].ctypes.data_as(_D) for k in range(3)]) for m in range(g.shape[0])]
+
+    def type1_gradient(self, hA, hB, C, hpot, D, nA, nB):
+        """libgrpp_type1_integrals_gradient: d<A|U|B>/dD, [3, nA, nB]."""
+        g = np.zeros((1, 3, nA * nB))
+        self.lib.libgrpp_type1_integrals_gradient(hA, hB, _dp(np.ascontiguousarray(C, dtype=np.float64)), hpot,
+                                                  _dp(np.ascontiguousarray(D, dtype=np.float64)), self._grad_ptrs(g)[0])
+        return g.reshape(3, nA, nB)
+
+    def type2_gradient(self, hA, hB, C, hpot, D, nA, nB):
+        """libgrpp_type2_integrals_gradient: [3, nA, nB]."""
+        g = np.zeros((1, 3, nA * nB))
+        self.lib.libgrpp_type2_integrals_gradient(hA, hB, _dp(np.ascontiguousarray(C, dtype=np.float64)), hpot,
+                                                  _dp(np.ascontiguousarray(D, dtype=np.float64)), self._grad_ptrs(g)[0])
+        return g.reshape(3, nA, nB)
+
+    def spin_orbit_gradient(self, hA, hB, C, hpot, D, nA, nB):
+        """libgrpp_spin_orbit_integrals_gradient: [3 (so_x, so_y, so_z), 3, nA, nB]."""
+        g = np.zeros((3, 3, nA * nB))
+        p = self._grad_ptrs(g)
+        self.lib.libgrpp_spin_orbit_integrals_gradient(hA, hB, _dp(np.ascontiguousarray(C, dtype=np.float64)), hpot,
+                                                       _dp(np.ascontiguousarray(D, dtype=np.float64)), p[0], p[1], p[2])
+        return g.reshape(3, 3, nA, nB)
+
+    def outercore_gradient(self, hA, hB, C, hpots, hocs, D, nA, nB):
+        """libgrpp_outercore_potential_integrals_gradient: [4 (arep, so_x, so_y, so_z), 3, nA, nB]."""
+        g = np.zeros((4, 3, nA * nB))
+        p = self._grad_ptrs(g)
+        n = len(hpots)
+        pots = (_V * max(n, 1))(*hpots)
+        ocs = (_V * max(n, 1))(*hocs)
+        self.lib.libgrpp_outercore_potential_integrals_gradient(
+            hA, hB, _dp(np.ascontiguousarray(C, dtype=np.float64)), n, pots, ocs,
+            _dp(np.ascontiguousarray(D, dtype=np.float64)), *p)
+        return g.reshape(4, 3, nA, nB)
+
+    # ------------------------------------------------------------ one-electron integrals
+    def overlap(self, hA, hB, nA, nB):
+        out = np.zeros(nA * nB)
+        self.lib.libgrpp_overlap_integrals(hA, hB, _dp(out))
+        return out.reshape(nA, nB)
+
+    def kinetic(self, hA, hB, nA, nB):
+        out = np.zeros(nA * nB)
+        self.lib.libgrpp_kinetic_energy_integrals(hA, hB, _dp(out))
+        return out.reshape(nA, nB)
+
+    def momentum(self, hA, hB, nA, nB):
+        o = [np.zeros(nA * nB) for _ in range(3)]
+        self.lib.libgrpp_momentum_integrals(hA, hB, *[_dp(x) for x in o])
+        return [x.reshape(nA, nB) for x in o]
+
+    def overlap_gradient(self, hA, hB, D, nA, nB):
+        g = np.zeros((1, 3, nA * nB))
+        self.lib.libgrpp_overlap_integrals_gradient(hA, hB, _dp(np.ascontiguousarray(D, dtype=np.float64)),
+                                                    self._grad_ptrs(g)[0])
+        return g.reshape(3, nA, nB)
+
+    def nuclear_attraction(self, hA, hB, C, Z, model, params, nA, nB):
+        out = np.zeros(nA * nB)
+        p = np.zeros(4) if params is None else np.ascontiguousarray(params, dtype=np.float64)
+        self.lib.libgrpp_nuclear_attraction_integrals(hA, hB, _dp(np.ascontiguousarray(C, dtype=np.float64)), int(Z),
+                                                      int(model), _dp(p), _dp(out))
+        return out.reshape(nA, nB)
+
+    def onee_batch(self, batch, kind):
+        """Overlap (kind 0), kinetic (1) or momentum (2: three arrays) blocks of every task's shell pair."""
+        n = int(batch.block_offsets()[-1])
+        o = [np.zeros(max(n, 1)) for _ in range(3)]
+        self._check(self.lib.libgrpp_b200_onee_batch(ct.byref(batch.struct), kind, *[_dp(x) for x in o]),
+                    "libgrpp_b200_onee_batch")
+        return [x[:n] for x in o[:3 if kind == 2 else 1]]
+
+    def nuclear_attraction_batch(self, batch, model, charges, params=None):
+        """Nuclear attraction blocks of every task (nucleus at the task's centre)."""
+        n = int(batch.block_offsets()[-1])
+        out = np.zeros(max(n, 1))
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        p = np.zeros(3 * len(q)) if params is None else np.ascontiguousarray(params, dtype=np.float64).ravel()
+        self._check(self.lib.libgrpp_b200_nuclear_attraction_batch(ct.byref(batch.struct), int(model), _dp(q), _dp(p),
+                                                                   _dp(out)), "libgrpp_b200_nuclear_attraction_batch")
+        return out[:n]
+
+    def type1_numeric_batch(self, batch):
+        """<A|U_L|B> of every task by numeric radial quadrature."""
+        n = int(batch.block_offsets()[-1])
+        out = np.zeros(max(n, 1))
+        self._check(self.lib.libgrpp_b200_type1_numeric_batch(ct.byref(batch.struct), _dp(out)),
+                    "libgrpp_b200_type1_numeric_batch")
+        return out[:n]
 
     # ------------------------------------------------------------ batched (CPU drivers)
     def driver_full_batch(self, batch, t0=0, t1=None, nthreads=1):

@@ -19,6 +19,8 @@
 #include "../../include/libgrpp.h"
 #include "../../include/libgrpp_b200.h"
 #include "engine.h"
+#include "nucmodel.h"
+#include "tables.h"
 
 namespace {
 
@@ -178,6 +180,25 @@ bool check_init()
         return false;
     }
     return true;
+}
+
+// one shell pair through the one-electron batch (kind 0 overlap, 1 kinetic, 2 momentum)
+void onee_single(libgrpp_shell_t *A, libgrpp_shell_t *B, int kind, double *o0, double *o1, double *o2)
+{
+    const int n = A->cart_size * B->cart_size;
+    double *outs[3] = {o0, o1, o2};
+    for (double *o : outs)
+        if (o) memset(o, 0, n * sizeof(double));
+    if (!check_init()) return;
+    Builder bd;
+    const int ia = bd.add_shell(A), ib = bd.add_shell(B);
+    bd.add_task(ia, ib, 0);
+    libgrpp_b200_batch_t v = bd.view();
+    std::vector<double> tmp[3];
+    for (auto &x : tmp) x.assign(n, 0.0);
+    if (grpp::run_onee_batch(&v, kind, tmp[0].data(), tmp[1].data(), tmp[2].data()) == 0)
+        for (int k = 0; k < 3; k++)
+            if (outs[k]) memcpy(outs[k], tmp[k].data(), n * sizeof(double));
 }
 
 // run a one-centre batch; out[k] receive consecutive task blocks
@@ -923,4 +944,279 @@ int libgrpp_b200_mlp_predict(const float *params, const float *features, int64_t
 }
 
 }  // extern "C"
+// ============================================================ one-electron integrals
+// libgrpp/overlap.c, kinetic.c, momentum.c, overlap_gradient.c, nuclear_attraction.c,
+// nuclear_models.c: the same entry points, evaluated on the GPU (batches of one).
+
+void libgrpp_overlap_integrals(libgrpp_shell_t *A, libgrpp_shell_t *B, double *matrix)
+{
+    onee_single(A, B, 0, matrix, nullptr, nullptr);
+}
+
+void libgrpp_kinetic_energy_integrals(libgrpp_shell_t *A, libgrpp_shell_t *B, double *matrix)
+{
+    onee_single(A, B, 1, matrix, nullptr, nullptr);
+}
+
+void libgrpp_momentum_integrals(libgrpp_shell_t *A, libgrpp_shell_t *B, double *mx, double *my, double *mz)
+{
+    onee_single(A, B, 2, mx, my, mz);
+}
+
+// overlap_gradient.c:27-141: d<A|B>/dA = +<dA|B>, d<A|B>/dB = -<dA|B>, zero for A = B
+void libgrpp_overlap_integrals_gradient(libgrpp_shell_t *A, libgrpp_shell_t *B, double *D, double **grad)
+{
+    const int nA = A->cart_size, nB = B->cart_size, n = nA * nB;
+    for (int k = 0; k < 3; k++) memset(grad[k], 0, n * sizeof(double));
+    if (!check_init() || points_equal(A->origin, B->origin)) return;
+    double factors[2];
+    int nf = 0;
+    if (points_equal(A->origin, D)) factors[nf++] = +1.0;
+    if (points_equal(B->origin, D)) factors[nf++] = -1.0;
+    if (nf == 0) return;
+    libgrpp_shell_t *Ad = shell_down(A), *Au = shell_up(A);
+    std::vector<double> down(Ad ? Ad->cart_size * nB : 1), up(Au->cart_size * nB);
+    if (Ad) onee_single(Ad, B, 0, down.data(), nullptr, nullptr);
+    onee_single(Au, B, 0, up.data(), nullptr, nullptr);
+    for (int f = 0; f < nf; f++)
+        for (int k = 0; k < 3; k++)
+            for (int i = 0; i < nA; i++)
+                for (int j = 0; j < nB; j++) {
+                    int bra[3] = {A->cart_list[3 * i], A->cart_list[3 * i + 1], A->cart_list[3 * i + 2]};
+                    const int *ket = B->cart_list + 3 * j;
+                    const int idx = i * nB + j;
+                    // the L-1 term only where the exponent is positive: libgrpp also forms it for a zero
+                    // exponent, reading past its L-1 block and multiplying by 0
+                    if (Ad && bra[k] > 0) {
+                        bra[k] -= 1;
+                        const int bi = nlm_to_linear(bra), ki = nlm_to_linear(ket);
+                        bra[k] += 1;
+                        grad[k][idx] -= factors[f] * bra[k] * down[nB * bi + ki];
+                    }
+                    bra[k] += 1;
+                    const int bi = nlm_to_linear(bra), ki = nlm_to_linear(ket);
+                    bra[k] -= 1;
+                    grad[k][idx] += factors[f] * up[nB * bi + ki];
+                }
+    if (Ad) libgrpp_delete_shell(Ad);
+    libgrpp_delete_shell(Au);
+}
+
+void libgrpp_nuclear_attraction_integrals(libgrpp_shell_t *A, libgrpp_shell_t *B, double *charge_origin, int charge,
+                                          int nuclear_model, double *model_params, double *coulomb_matrix)
+{
+    const int n = A->cart_size * B->cart_size;
+    memset(coulomb_matrix, 0, n * sizeof(double));
+    if (!check_init()) return;
+    Builder bd;
+    const int ia = bd.add_shell(A), ib = bd.add_shell(B);
+    bd.add_centre(charge_origin, 0);
+    bd.add_task(ia, ib, 0);
+    bd.grpp_UL.push_back(-1);  // one empty GRPP: the centre needs an operator index only
+    bd.grpp_arep_off.push_back(0);
+    bd.grpp_n_arep.push_back(0);
+    bd.grpp_so_off.push_back(0);
+    bd.grpp_n_so.push_back(0);
+    bd.grpp_oc_off.push_back(0);
+    bd.grpp_n_oc.push_back(0);
+    libgrpp_b200_batch_t v = bd.view();
+    const double z = charge;
+    double prm[3] = {0, 0, 0};
+    const int np = nuclear_model == LIBGRPP_NUCLEAR_MODEL_FERMI ? 2 : (nuclear_model == LIBGRPP_NUCLEAR_MODEL_FERMI_BUBBLE ? 3 : 1);
+    if (nuclear_model != LIBGRPP_NUCLEAR_MODEL_POINT_CHARGE && nuclear_model != LIBGRPP_NUCLEAR_MODEL_POINT_CHARGE_NUMERICAL) {
+        if (!model_params) {
+            grpp::set_error(LIBGRPP_B200_ERR_INVALID, "nuclear model parameters missing");
+            return;
+        }
+        for (int q = 0; q < np; q++) prm[q] = model_params[q];
+    }
+    libgrpp_b200_nuclear_attraction_batch(&v, nuclear_model, &z, prm, coulomb_matrix);
+}
+
+void libgrpp_nuclear_attraction_integrals_point_charge(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, int charge,
+                                                       double *m)
+{
+    libgrpp_nuclear_attraction_integrals(A, B, C, charge, LIBGRPP_NUCLEAR_MODEL_POINT_CHARGE, nullptr, m);
+}
+void libgrpp_nuclear_attraction_integrals_charged_ball(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, int charge,
+                                                       double r_rms, double *m)
+{
+    libgrpp_nuclear_attraction_integrals(A, B, C, charge, LIBGRPP_NUCLEAR_MODEL_CHARGED_BALL, &r_rms, m);
+}
+void libgrpp_nuclear_attraction_integrals_gaussian_model(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, int charge,
+                                                         double r_rms, double *m)
+{
+    libgrpp_nuclear_attraction_integrals(A, B, C, charge, LIBGRPP_NUCLEAR_MODEL_GAUSSIAN, &r_rms, m);
+}
+void libgrpp_nuclear_attraction_integrals_fermi_model(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, int charge,
+                                                      double fermi_param_c, double fermi_param_a, double *m)
+{
+    double p[2] = {fermi_param_c, fermi_param_a};
+    libgrpp_nuclear_attraction_integrals(A, B, C, charge, LIBGRPP_NUCLEAR_MODEL_FERMI, p, m);
+}
+void libgrpp_nuclear_attraction_integrals_fermi_bubble_model(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, int charge,
+                                                             double param_c, double param_a, double param_k, double *m)
+{
+    double p[3] = {param_c, param_a, param_k};
+    libgrpp_nuclear_attraction_integrals(A, B, C, charge, LIBGRPP_NUCLEAR_MODEL_FERMI_BUBBLE, p, m);
+}
+
+// ---- nuclear charge models (nuclear_models.c): host functions
+double libgrpp_estimate_nuclear_rms_radius_johnson_1985(int A) { return 0.836 * pow(A, 1.0 / 3.0) + 0.570; }
+double libgrpp_estimate_nuclear_rms_radius_golovko_2008(int A) { return 0.77 * pow(A, 1.0 / 3.0) + 0.98; }
+int libgrpp_estimate_fermi_model_parameters(double R_rms, double *c, double *a)
+{
+    const double t = 2.3;
+    *a = t / (4 * log(3));
+    const double c2 = 5.0 / 3.0 * R_rms * R_rms - 7.0 / 3.0 * M_PI * M_PI * (*a) * (*a);
+    if (c2 < 0) return -1;
+    *c = sqrt(c2);
+    return 1;
+}
+double libgrpp_charge_density_ball(double r, double Z, double R_rms)
+{
+    const double R0 = sqrt(5.0 / 3.0) * R_rms;
+    return r <= R0 ? 3.0 * Z / (4.0 * M_PI * R0 * R0 * R0) : 0.0;
+}
+double libgrpp_charge_density_gaussian(double r, double Z, double R_rms)
+{
+    const double xi = 3.0 / (2.0 * R_rms * R_rms);
+    return Z * pow(xi / M_PI, 1.5) * exp(-xi * r * r);
+}
+double libgrpp_charge_density_fermi(double r, double Z, double c, double a)
+{
+    const double N = grpp::fermi_norm(c, a, grpp::fermi_table());
+    return 3.0 * Z / (4 * M_PI * c * c * c * N) / (1.0 + exp((r - c) / a));
+}
+double libgrpp_charge_density_fermi_bubble(double r, double Z, double c, double a, double k)
+{
+    const double Nk = grpp::fermi_bubble_norm(c, a, k, grpp::fermi_table());
+    return 3.0 * Z / (4 * M_PI * c * c * c * Nk) * (1 + k * pow(r / c, 2)) / (1.0 + exp((r - c) / a));
+}
+double libgrpp_rms_radius_fermi(int Z, double c, double a)
+{
+    const double *tab = grpp::fermi_table();
+    const double N = grpp::fermi_norm(c, a, tab), rho0 = 3.0 * Z / (4 * M_PI * c * c * c * N);
+    const double r2 = 4 * M_PI * rho0 / Z * pow(c, 5) / 5.0 *
+                      (1.0 + 10.0 / 3.0 * a * a * M_PI * M_PI / (c * c) + 7.0 / 3.0 * pow(M_PI, 4) * pow(a, 4) / pow(c, 4) -
+                       120.0 * pow(a, 5) / pow(c, 5) * grpp::fermi_sk(5, -c / a, tab));
+    return sqrt(r2);
+}
+double libgrpp_rms_radius_fermi_bubble(int Z, double c, double a, double k)
+{
+    const double *tab = grpp::fermi_table();
+    const double Nk = grpp::fermi_bubble_norm(c, a, k, tab), rho0 = 3.0 * Z / (4 * M_PI * c * c * c * Nk);
+    const double part_r4 = pow(c, 5) / 5.0 *
+                           (1.0 + 10.0 / 3.0 * a * a * M_PI * M_PI / (c * c) + 7.0 / 3.0 * pow(M_PI, 4) * pow(a, 4) / pow(c, 4) -
+                            120.0 * pow(a, 5) / pow(c, 5) * grpp::fermi_sk(5, -c / a, tab));
+    const double part_r6 = pow(c, 7) / 7.0 *
+                           (1.0 + 7.0 * a * a * M_PI * M_PI / (c * c) + 49.0 / 3.0 * pow(M_PI, 4) * pow(a, 4) / pow(c, 4) +
+                            31.0 / 3.0 * pow(M_PI, 6) * pow(a, 6) / pow(c, 6) -
+                            5040.0 * pow(a, 7) / pow(c, 7) * grpp::fermi_sk(7, -c / a, tab));
+    return sqrt(4 * M_PI * rho0 / Z * (part_r4 + k / (c * c) * part_r6));
+}
+double libgrpp_coulomb_potential_point(double r, double Z) { return -Z / r; }
+double libgrpp_coulomb_potential_ball(double r, double Z, double R_rms) { return grpp::coulomb_ball(r, Z, R_rms); }
+double libgrpp_coulomb_potential_gaussian(double r, double Z, double R_rms) { return grpp::coulomb_gauss(r, Z, R_rms); }
+double libgrpp_coulomb_potential_fermi(double r, double Z, double c, double a)
+{
+    return grpp::coulomb_fermi(r, Z, c, a, grpp::fermi_table());
+}
+double libgrpp_coulomb_potential_fermi_bubble(double r, double Z, double c, double a, double k)
+{
+    return grpp::coulomb_fermi_bubble(r, Z, c, a, k, grpp::fermi_table());
+}
+
+// ---- batched forms (no counterpart in libgrpp)
+int libgrpp_b200_onee_batch(const libgrpp_b200_batch_t *batch, int kind, double *out0, double *out1, double *out2)
+{
+    if (!check_init()) return LIBGRPP_B200_ERR_NOT_INIT;
+    if (!batch || !out0 || (kind == LIBGRPP_B200_ONEE_MOMENTUM && (!out1 || !out2))) {
+        grpp::set_error(LIBGRPP_B200_ERR_INVALID, "one-electron batch: null argument");
+        return LIBGRPP_B200_ERR_INVALID;
+    }
+    return grpp::run_onee_batch(batch, kind, out0, out1, out2);
+}
+
+int libgrpp_b200_nuclear_attraction_batch(const libgrpp_b200_batch_t *batch, int nuclear_model, const double *centre_charge,
+                                          const double *centre_params, double *out)
+{
+    if (!check_init()) return LIBGRPP_B200_ERR_NOT_INIT;
+    auto invalid = [](const char *m) {
+        grpp::set_error(LIBGRPP_B200_ERR_INVALID, m);
+        return LIBGRPP_B200_ERR_INVALID;
+    };
+    if (!batch || !centre_charge || !out) return invalid("nuclear attraction batch: null argument");
+    if (batch->n_tasks == 0) return 0;
+    const int nc = batch->n_centres;
+    if (nc <= 0) return invalid("nuclear attraction batch: no centres");
+    if (nuclear_model == LIBGRPP_NUCLEAR_MODEL_POINT_CHARGE) {
+        // libgrpp evaluates the point charge through its type 1 McMurchie-Davidson code with a zero
+        // exponent (nuclear_attraction.c:106-117): here every centre gets a GRPP whose U_L is
+        // -Z r^(1-2) exp(0 r^2), and the batch runs through the GRPP engine
+        std::vector<int> pL(nc, 0), pJ(nc, 0), pn(nc, 1), po(nc), pw(nc, 1), g(nc), z0(nc, 0), cg(nc);
+        std::vector<double> pc(nc), pa(nc, 0.0);
+        for (int c = 0; c < nc; c++) {
+            po[c] = c;
+            pc[c] = -centre_charge[c];
+            g[c] = c;
+            cg[c] = c;
+        }
+        libgrpp_b200_batch_t v = *batch;
+        v.n_pots = nc;
+        v.pot_L = pL.data();
+        v.pot_J = pJ.data();
+        v.pot_nprim = pn.data();
+        v.pot_prim_off = po.data();
+        v.pot_powers = pw.data();
+        v.pot_coef = pc.data();
+        v.pot_alpha = pa.data();
+        v.n_grpps = nc;
+        v.grpp_UL = g.data();
+        v.grpp_arep_off = z0.data();
+        v.grpp_n_arep = z0.data();
+        v.grpp_so_off = z0.data();
+        v.grpp_n_so = z0.data();
+        v.grpp_oc_off = z0.data();
+        v.grpp_n_oc = z0.data();
+        v.grpp_pot_list = z0.data();
+        v.grpp_oc_pot = z0.data();
+        v.grpp_oc_shell = z0.data();
+        v.centre_grpp = cg.data();
+        const int64_t n = grpp::batch_output_size(&v);
+        std::vector<double> so[3];
+        for (auto &x : so) x.assign(std::max<int64_t>(n, 1), 0.0);
+        grpp::RunOptions opt;
+        return grpp::run_full_batch(&v, opt, out, so[0].data(), so[1].data(), so[2].data());
+    }
+    int model;
+    switch (nuclear_model) {
+    case LIBGRPP_NUCLEAR_MODEL_POINT_CHARGE_NUMERICAL: model = grpp::kPotPointNum; break;
+    case LIBGRPP_NUCLEAR_MODEL_CHARGED_BALL: model = grpp::kPotBall; break;
+    case LIBGRPP_NUCLEAR_MODEL_GAUSSIAN: model = grpp::kPotGauss; break;
+    case LIBGRPP_NUCLEAR_MODEL_FERMI: model = grpp::kPotFermi; break;
+    case LIBGRPP_NUCLEAR_MODEL_FERMI_BUBBLE: model = grpp::kPotFermiBubble; break;
+    default: return invalid("unknown nuclear charge distribution model");
+    }
+    if (model != grpp::kPotPointNum && !centre_params) return invalid("nuclear model parameters missing");
+    std::vector<double> prm((size_t)4 * nc, 0.0);
+    for (int c = 0; c < nc; c++) {
+        prm[4 * c] = centre_charge[c];
+        if (model != grpp::kPotPointNum)
+            for (int q = 0; q < 3; q++) prm[4 * c + 1 + q] = centre_params[3 * c + q];
+    }
+    // nuclear_attraction.c:50-54: primitive pairs with |c_i c_j| < 1e-13 are skipped
+    return grpp::run_type1_numeric_batch(batch, model, prm.data(), libgrpp_params.radial_tolerance, 1e-13, out);
+}
+
+int libgrpp_b200_type1_numeric_batch(const libgrpp_b200_batch_t *batch, double *arep)
+{
+    if (!check_init()) return LIBGRPP_B200_ERR_NOT_INIT;
+    if (!batch || !arep) {
+        grpp::set_error(LIBGRPP_B200_ERR_INVALID, "numeric type 1 batch: null argument");
+        return LIBGRPP_B200_ERR_INVALID;
+    }
+    return grpp::run_type1_numeric_batch(batch, grpp::kPotGrpp, nullptr, libgrpp_params.radial_tolerance, 0.0, arep);
+}
+
 #pragma GCC visibility pop

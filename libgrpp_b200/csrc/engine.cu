@@ -30,6 +30,7 @@
 #include "angular.cuh"
 #include "level_model.cuh"
 #include "gradient.cuh"
+#include "onee.cuh"
 #include "tables.h"
 #include "engine.h"
 
@@ -114,6 +115,8 @@ struct DeviceState {
     DevBuf atab;
     size_t atab_used = 0;
     DevBuf grad;  // density-contracted gradient: tasks, component table, D, per-task sums
+    DevBuf onee;  // one-electron batches: inputs, angular factors, outputs
+    const double *fermi = nullptr;  // S_j table of the Fermi nuclear models
     // learned grid-level model (libgrpp_b200_set_level_model): FP32 normalisation, BF16 weights
     float *lm_norm = nullptr;
     __nv_bfloat16 *lm_w = nullptr;
@@ -162,6 +165,7 @@ int init_device_state(DeviceState &st, int device)
     GRPP_CUDA(upload_vec(st, h.lmat_off, &d.lmat_off));
     GRPP_CUDA(upload_vec(st, h.dfact, &d.dfact));
     GRPP_CUDA(upload_vec(st, h.binom, &d.binom));
+    GRPP_CUDA(upload_vec(st, h.fermi, &st.fermi));
     GRPP_CUDA(cudaMemcpyToSymbol(c_tab, &d, sizeof(d)));
     GRPP_CUDA(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking));
     GRPP_CUDA(cudaStreamCreateWithFlags(&st.copy_stream, cudaStreamNonBlocking));
@@ -179,6 +183,8 @@ int init_device_state(DeviceState &st, int device)
     GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(radial_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFinSmemMax));
+    GRPP_CUDA(cudaFuncSetAttribute(type1_num_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(t1_smem_doubles(kT1MaxLam) * sizeof(double))));
     GRPP_CUDA(cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_train_smem_bytes()));
     st.device = device;
     st.ready = true;
@@ -1808,6 +1814,246 @@ int run_grad_contract(const libgrpp_b200_batch_t *sub, const RunOptions &opt, co
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         set_error(LIBGRPP_B200_ERR_CUDA, std::string("gradient contraction: ") + cudaGetErrorString(e));
+        return LIBGRPP_B200_ERR_CUDA;
+    }
+    return 0;
+}
+
+// ------------------------------------------------------------------ one-electron batches
+namespace {
+
+// shells and tasks of a batch packed for the one-electron kernels (Cartesian lists as int8,
+// task blocks laid out as in run_full_batch)
+struct OneePack {
+    std::vector<int> sL, snp, spo, sco, ta, tb, tc;
+    std::vector<double> pc, pa, so;
+    std::vector<int8_t> cart;
+    std::vector<int64_t> off;
+    int lmax_pair = 0;
+};
+
+int onee_pack(const libgrpp_b200_batch_t *b, bool need_centres, int lmax_shell, OneePack &k)
+{
+    const int64_t nt = b->n_tasks;
+    auto bad = [](const char *m) {
+        set_error(LIBGRPP_B200_ERR_INVALID, m);
+        return LIBGRPP_B200_ERR_INVALID;
+    };
+    if (nt < 0) return bad("negative task count");
+    if (nt > ((int64_t)1 << 31) - 1) return bad("more than 2^31 - 1 tasks in one call");
+    if (nt == 0) return 0;
+    if (b->n_shells <= 0 || (need_centres && b->n_centres <= 0)) return bad("empty batch description");
+    const int ns = b->n_shells;
+    k.sL.assign(b->shell_L, b->shell_L + ns);
+    k.snp.assign(b->shell_nprim, b->shell_nprim + ns);
+    k.spo.assign(b->shell_prim_off, b->shell_prim_off + ns);
+    k.sco.resize(ns);
+    k.so.assign(b->shell_origin, b->shell_origin + 3 * ns);
+    int tot = 0;
+    for (int i = 0; i < ns; i++) {
+        if (k.sL[i] < 0 || k.sL[i] > lmax_shell) return bad("shell angular momentum outside the supported range");
+        if (k.snp[i] < 0 || k.snp[i] > kRadMaxPrims || k.spo[i] < 0) return bad("shell primitive count or offset out of range");
+        tot = std::max(tot, k.spo[i] + k.snp[i]);
+        k.sco[i] = (int)(k.cart.size() / 3);
+        for (int q = 0; q < 3 * ncart(k.sL[i]); q++) {
+            const int v = b->cart_list[3 * b->shell_cart_off[i] + q];
+            if (v < 0 || v > k.sL[i]) return bad("invalid Cartesian component list");
+            k.cart.push_back((int8_t)v);
+        }
+    }
+    k.pc.assign(b->prim_coef, b->prim_coef + tot);
+    k.pa.assign(b->prim_alpha, b->prim_alpha + tot);
+    k.ta.assign(b->task_a, b->task_a + nt);
+    k.tb.assign(b->task_b, b->task_b + nt);
+    k.off.assign(nt + 1, 0);
+    if (need_centres) k.tc.assign(b->task_c, b->task_c + nt);
+    for (int64_t t = 0; t < nt; t++) {
+        if (k.ta[t] < 0 || k.ta[t] >= ns || k.tb[t] < 0 || k.tb[t] >= ns) return bad("task index out of range");
+        if (need_centres && (k.tc[t] < 0 || k.tc[t] >= b->n_centres)) return bad("task centre index out of range");
+        k.off[t + 1] = k.off[t] + (int64_t)ncart(k.sL[k.ta[t]]) * ncart(k.sL[k.tb[t]]);
+        k.lmax_pair = std::max(k.lmax_pair, k.sL[k.ta[t]] + k.sL[k.tb[t]]);
+    }
+    return 0;
+}
+
+struct OneeUpload {
+    char *dev = nullptr;
+    std::vector<char> host;
+    size_t used = 0;
+    template <typename T>
+    size_t add(const std::vector<T> &v)
+    {
+        const size_t o = (used + 255) & ~size_t(255);
+        used = o + std::max<size_t>(v.size(), 1) * sizeof(T);
+        host.resize(used);
+        if (!v.empty()) memcpy(host.data() + o, v.data(), v.size() * sizeof(T));
+        return o;
+    }
+    size_t reserve(size_t bytes)
+    {
+        const size_t o = (used + 255) & ~size_t(255);
+        used = o + std::max<size_t>(bytes, 8);
+        return o;
+    }
+    template <typename T>
+    T *at(size_t o) const
+    {
+        return (T *)(dev + o);
+    }
+};
+
+}  // namespace
+
+int run_onee_batch(const libgrpp_b200_batch_t *b, int kind, double *h0, double *h1, double *h2)
+{
+    set_error(0, "");
+    if (kind < kOneeOverlap || kind > kOneeMomentum) {
+        set_error(LIBGRPP_B200_ERR_INVALID, "unknown one-electron integral kind");
+        return LIBGRPP_B200_ERR_INVALID;
+    }
+    OneePack k;
+    int rc = onee_pack(b, false, kMaxL, k);
+    if (rc || b->n_tasks == 0) return rc;
+    DeviceState *stp = get_state(rc);
+    if (!stp) return rc;
+    std::lock_guard<std::mutex> lk(stp->mu);
+    cudaStream_t s = stp->stream;
+    const int64_t nt = b->n_tasks, nout = k.off[nt];
+    const int nouts = kind == kOneeMomentum ? 3 : 1;
+    OneeUpload u;
+    const size_t oL = u.add(k.sL), onp = u.add(k.snp), opo = u.add(k.spo), oco = u.add(k.sco), opc = u.add(k.pc),
+                 opa = u.add(k.pa), oso = u.add(k.so), ocart = u.add(k.cart), ota = u.add(k.ta), otb = u.add(k.tb),
+                 ooff = u.add(k.off);
+    const size_t in_bytes = u.used;
+    const size_t oout = u.reserve((size_t)nouts * nout * sizeof(double));
+    GRPP_CUDA(stp->onee.ensure(u.used));
+    u.dev = (char *)stp->onee.p;
+    GRPP_CUDA(cudaMemcpyAsync(u.dev, u.host.data(), in_bytes, cudaMemcpyHostToDevice, s));
+    OneeArgs a{};
+    a.n_tasks = (int)nt;
+    a.kind = kind;
+    a.task_a = u.at<int>(ota);
+    a.task_b = u.at<int>(otb);
+    a.out_off = u.at<int64_t>(ooff);
+    a.shell_L = u.at<int>(oL);
+    a.shell_nprim = u.at<int>(onp);
+    a.shell_prim_off = u.at<int>(opo);
+    a.shell_cart_off = u.at<int>(oco);
+    a.prim_coef = u.at<double>(opc);
+    a.prim_alpha = u.at<double>(opa);
+    a.shell_origin = u.at<double>(oso);
+    a.cart = u.at<int8_t>(ocart);
+    a.out0 = u.at<double>(oout);
+    a.out1 = a.out0 + nout;
+    a.out2 = a.out1 + nout;
+    const int blocks = (int)std::min<int64_t>((nt + kOneeWarps - 1) / kOneeWarps, 148 * 16);
+    onee_os_kernel<<<blocks, 32 * kOneeWarps, 0, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    double *hs[3] = {h0, h1, h2};
+    for (int m = 0; m < nouts && e == cudaSuccess; m++)
+        e = cudaMemcpyAsync(hs[m], a.out0 + m * nout, nout * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_error(LIBGRPP_B200_ERR_CUDA, std::string("one-electron integrals: ") + cudaGetErrorString(e));
+        return LIBGRPP_B200_ERR_CUDA;
+    }
+    return 0;
+}
+
+int run_type1_numeric_batch(const libgrpp_b200_batch_t *b, int model, const double *centre_param, double tol,
+                            double pair_skip, double *h_out)
+{
+    set_error(0, "");
+    auto bad = [](const char *m) {
+        set_error(LIBGRPP_B200_ERR_INVALID, m);
+        return LIBGRPP_B200_ERR_INVALID;
+    };
+    if (model < kPotGrpp || model > kPotFermiBubble) return bad("unknown radially local potential model");
+    OneePack k;
+    int rc = onee_pack(b, true, kMaxL, k);
+    if (rc || b->n_tasks == 0) return rc;
+    if (k.lmax_pair > kT1MaxLam) return bad("numeric type 1 integrals need L_A + L_B <= 12");
+    if (model != kPotGrpp && !centre_param) return bad("nuclear model parameters missing");
+    // the centres' radially local potentials: U_L of each centre's GRPP (terms with |c| > 1e-14,
+    // as libgrpp_shrink_potential keeps them), or the model parameters
+    const int nc = b->n_centres;
+    std::vector<double> cor(b->centre_origin, b->centre_origin + 3 * nc), cpar((size_t)4 * nc, 0.0);
+    std::vector<int> cpo(nc, 0), cpn(nc, 0), ppw;
+    std::vector<double> pco, pal;
+    for (int c = 0; c < nc; c++) {
+        if (model != kPotGrpp) {
+            for (int q = 0; q < 4; q++) cpar[4 * c + q] = centre_param[4 * c + q];
+            continue;
+        }
+        const int g = b->centre_grpp[c];
+        if (g < 0 || g >= b->n_grpps) return bad("centre GRPP index out of range");
+        cpo[c] = (int)pco.size();
+        const int p = b->grpp_UL[g];
+        if (p < 0) continue;
+        if (p >= b->n_pots) return bad("GRPP potential index out of range");
+        for (int q = 0; q < b->pot_nprim[p]; q++) {
+            const int o = b->pot_prim_off[p] + q;
+            if (b->pot_powers[o] < 0 || b->pot_powers[o] > 2) return bad("potential power n must be 0, 1 or 2");
+            if (std::fabs(b->pot_coef[o]) <= kZeroThresh) continue;
+            ppw.push_back(b->pot_powers[o]);
+            pco.push_back(b->pot_coef[o]);
+            pal.push_back(b->pot_alpha[o]);
+        }
+        cpn[c] = (int)pco.size() - cpo[c];
+    }
+    DeviceState *stp = get_state(rc);
+    if (!stp) return rc;
+    std::lock_guard<std::mutex> lk(stp->mu);
+    cudaStream_t s = stp->stream;
+    const int64_t nt = b->n_tasks, nout = k.off[nt];
+    const int Lt = k.lmax_pair;
+    const int64_t n_ang = (int64_t)(Lt + 1) * (2 * Lt + 1) * n_abc(Lt);
+    OneeUpload u;
+    const size_t oL = u.add(k.sL), onp = u.add(k.snp), opo = u.add(k.spo), oco = u.add(k.sco), opc = u.add(k.pc),
+                 opa = u.add(k.pa), oso = u.add(k.so), ocart = u.add(k.cart), ota = u.add(k.ta), otb = u.add(k.tb),
+                 otc = u.add(k.tc), ooff = u.add(k.off), ocor = u.add(cor), ocpar = u.add(cpar), ocpo = u.add(cpo),
+                 ocpn = u.add(cpn), oppw = u.add(ppw), opco = u.add(pco), opal = u.add(pal);
+    const size_t in_bytes = u.used;
+    const size_t oang = u.reserve(n_ang * sizeof(double)), oout = u.reserve(nout * sizeof(double));
+    GRPP_CUDA(stp->onee.ensure(u.used));
+    u.dev = (char *)stp->onee.p;
+    GRPP_CUDA(cudaMemcpyAsync(u.dev, u.host.data(), in_bytes, cudaMemcpyHostToDevice, s));
+    type1_ang_kernel<<<(int)std::min<int64_t>((n_ang + 255) / 256, 4096), 256, 0, s>>>(Lt, u.at<double>(oang));
+    Type1NumArgs a{};
+    a.n_tasks = (int)nt;
+    a.model = model;
+    a.task_a = u.at<int>(ota);
+    a.task_b = u.at<int>(otb);
+    a.task_c = u.at<int>(otc);
+    a.out_off = u.at<int64_t>(ooff);
+    a.shell_L = u.at<int>(oL);
+    a.shell_nprim = u.at<int>(onp);
+    a.shell_prim_off = u.at<int>(opo);
+    a.shell_cart_off = u.at<int>(oco);
+    a.prim_coef = u.at<double>(opc);
+    a.prim_alpha = u.at<double>(opa);
+    a.shell_origin = u.at<double>(oso);
+    a.cart = u.at<int8_t>(ocart);
+    a.centre_origin = u.at<double>(ocor);
+    a.centre_param = u.at<double>(ocpar);
+    a.centre_pot_off = u.at<int>(ocpo);
+    a.centre_pot_n = u.at<int>(ocpn);
+    a.pot_pow = u.at<int>(oppw);
+    a.pot_coef = u.at<double>(opco);
+    a.pot_alpha = u.at<double>(opal);
+    a.fermi = stp->fermi;
+    a.ang1 = u.at<double>(oang);
+    a.lmax_tab = Lt;
+    a.tol = tol;
+    a.pair_skip = pair_skip;
+    a.out = u.at<double>(oout);
+    const size_t smem = (size_t)t1_smem_doubles(Lt) * sizeof(double);
+    type1_num_kernel<<<(int)std::min<int64_t>(nt, 148 * 8), kT1Threads, smem, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_out, a.out, nout * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_error(LIBGRPP_B200_ERR_CUDA, std::string("numeric type 1 integrals: ") + cudaGetErrorString(e));
         return LIBGRPP_B200_ERR_CUDA;
     }
     return 0;

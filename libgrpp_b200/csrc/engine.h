@@ -57,6 +57,13 @@ constexpr int kGradTabCart = 66;   // components of L = 10
 int run_grad_contract(const libgrpp_b200_batch_t *sub, const RunOptions &opt, const GradTaskHost *tasks,
                       int64_t n_tasks, const int *cart_tab, const double *D, int64_t n_bf, double *out24);
 
+// one-electron integrals (onee.cuh): kind 0 overlap, 1 kinetic (out0), 2 momentum (out0..2)
+int run_onee_batch(const libgrpp_b200_batch_t *b, int kind, double *out0, double *out1, double *out2);
+// numeric type 1 integrals of a radially local potential per centre: model 0 the centre GRPP's U_L,
+// 1..5 nuclear charge models with centre_param[4 * c] = {Z, parameters} (nucmodel.h)
+int run_type1_numeric_batch(const libgrpp_b200_batch_t *b, int model, const double *centre_param, double tol,
+                            double pair_skip, double *out);
+
 // learned grid-level model (level_model.cuh)
 int set_level_model(const float *params);
 int level_samples(const libgrpp_b200_batch_t *b, float *features, int8_t *levels, int64_t *n_items);

@@ -12,12 +12,18 @@
 // Real spherical harmonic coefficients follow Flores-Moreno et al.,
 // J. Comput. Chem. 27, 1009 (2006), eq. 32 (libgrpp/spherical_harmonics.c:115-166),
 // L matrices the complex-to-real transform of libgrpp/lmatrix.c:28-141.
+// The Fermi-model function S_j(x) = sum_{i>=1} (-1)^i e^{ix} / i^j (x <= 0), which libgrpp
+// ships as data (specfunc_fermi_sk.c), is generated from its closed forms for j <= 1 and,
+// for j >= 2, from its alternating series summed by the acceleration of Cohen,
+// Rodriguez Villegas and Zagier (Exp. Math. 9, 3 (2000), algorithm 1), in long double.
 #include <cmath>
+#include <mutex>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
 
 #include "grpp_common.cuh"
+#include "nucmodel.h"
 #include "tables.h"
 
 namespace grpp {
@@ -126,8 +132,44 @@ void csh_to_rsh(int m, Cplx &a, Cplx &b)
 
 }  // namespace
 
+// S_j(x), j = -2..7, on x = -10 + 0.005 i, i = 0..2000: row i holds S_{-2} .. S_7
+static void build_fermi_table(std::vector<double> &tab)
+{
+    tab.assign((size_t)kFermiNX * kFermiNK, 0.0);
+    const int n = 48;  // CRVZ terms: error below (3 + sqrt 8)^-48 of the first term
+    for (int i = 0; i < kFermiNX; i++) {
+        const long double x = -10.0L + 0.005L * i, e = expl(x), z = -e;
+        double *row = &tab[(size_t)i * kFermiNK];
+        row[0] = (double)(z * (1 + z) / ((1 - z) * (1 - z) * (1 - z)));  // Li_{-2}(z), z = -e^x
+        row[1] = (double)(z / ((1 - z) * (1 - z)));                    // Li_{-1}
+        row[2] = (double)(z / (1 - z));                                // Li_0
+        row[3] = (double)(-log1pl(e));                                 // Li_1
+        for (int j = 2; j <= 7; j++) {
+            // sum_{k>=0} (-1)^k a_k with a_k = e^{(k+1)x} / (k+1)^j, a moment sequence: S_j = -that sum
+            long double d = powl(3.0L + sqrtl(8.0L), n);
+            d = (d + 1.0L / d) / 2.0L;
+            long double b = -1.0L, c = -d, s = 0.0L;
+            for (int k = 0; k < n; k++) {
+                c = b - c;
+                s += c * (expl((k + 1) * x) / powl((long double)(k + 1), j));
+                b = (long double)(k + n) * (long double)(k - n) * b / ((k + 0.5L) * (k + 1.0L));
+            }
+            row[j + 2] = (double)(-s / d);
+        }
+    }
+}
+
+const double *fermi_table()
+{
+    static std::vector<double> tab;
+    static std::once_flag once;
+    std::call_once(once, [] { build_fermi_table(tab); });
+    return tab.data();
+}
+
 void build_host_tables(HostTables &t)
 {
+    t.fermi.assign(fermi_table(), fermi_table() + (size_t)kFermiNX * kFermiNK);
     // Bessel values for orders 0..kBesL+4 so that all 4 derivative orders of 0..kBesL-1 are exact
     const int LV = kBesL + 5;
     std::vector<double> v((size_t)kBesNX * LV * 5, 0.0);

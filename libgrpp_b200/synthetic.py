@@ -68,10 +68,11 @@ def config0(seed: int = 0) -> System:
                   np.array([0], np.int32), np.stack([A, B]))
 
 
-def config1(seed: int = 1, n_atoms: int = 64) -> System:
+def config1(seed: int = 1, n_atoms: int = 64, amin: float = 0.02, amax: float = 5e3) -> System:
     """64 atoms uniform in a 40-bohr cube (min separation 3 bohr); every atom has
     U_L (4 terms) + projectors l=0..4 (3 terms each) and s..g shells of 8
-    primitives, exponents log-uniform [0.02, 5e3]."""
+    primitives, exponents log-uniform [amin, amax] ([0.02, 5e3] for the workload;
+    config1_moderate() narrows them)."""
     rng = np.random.default_rng(seed)
     xyz = _place(rng, n_atoms, 40.0, 3.0)
     grpps, shells, shell_atom, centres = [], [], [], []
@@ -79,10 +80,17 @@ def config1(seed: int = 1, n_atoms: int = 64) -> System:
         grpps.append(_scalar_grpp(rng, 4, 4))
         centres.append((xyz[i].copy(), i))
         for L in range(5):
-            shells.append(_shell(rng, xyz[i], L, 8))
+            shells.append(_shell(rng, xyz[i], L, 8, amin=amin, amax=amax))
             shell_atom.append(i)
     return System(shells, grpps, centres, CART_ORDER_TURBOMOLE, np.array(shell_atom, np.int32),
                   np.arange(n_atoms, dtype=np.int32), xyz)
+
+
+def config1_moderate(seed: int = 1) -> System:
+    """Config 1 with exponents log-uniform [0.1, 50]: the same atoms, potentials and
+    shell shapes, on which libgrpp keeps its digits (its results move by less than
+    the 1e-10 / 1e-9 tolerance under last-bit input changes)."""
+    return config1(seed, amin=0.1, amax=50.0)
 
 
 def _heavy_grpp(rng, l_proj=4, l_so=4, l_oc=3):
@@ -119,6 +127,23 @@ def config2(seed: int = 2, n_heavy: int = 16, n_h: int = 32, lmax: int = 5, box:
             shell_atom.append(i)
     return System(shells, grpps, centres, CART_ORDER_TURBOMOLE, np.array(shell_atom, np.int32),
                   np.array(centre_atom, np.int32), xyz)
+
+
+def moderate_heavy_system(seed: int = 7) -> System:
+    """Two heavy atoms (U_L, projectors l <= 4, SO l <= 4, outercore s..d shells) and one H;
+    basis shells s..f (H: s, p) of 6 primitives with exponents log-uniform [0.1, 30]. On
+    such blocks libgrpp keeps its digits, so two implementations can be held to the strict
+    1e-10 / 1e-9 tolerance element by element."""
+    rng = np.random.default_rng(seed)
+    xyz = np.array([[0.0, 0.0, 0.0], [1.1, -0.6, 2.3], [-1.4, 1.2, 0.7]])
+    grpps = [_heavy_grpp(rng, l_proj=4, l_so=4, l_oc=2) for _ in range(2)]
+    shells, shell_atom = [], []
+    for i in range(3):
+        for L in range(4 if i < 2 else 2):
+            shells.append(_shell(rng, xyz[i], L, 6, amin=0.1, amax=30.0))
+            shell_atom.append(i)
+    return System(shells, grpps, [(xyz[0].copy(), 0), (xyz[1].copy(), 1)], CART_ORDER_TURBOMOLE,
+                  np.array(shell_atom, np.int32), np.array([0, 1], np.int32), xyz)
 
 
 def config3_density(system: System, seed: int = 3) -> np.ndarray:

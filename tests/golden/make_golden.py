@@ -93,7 +93,8 @@ def sample_tasks(system, n_pairs, seed):
 
 
 # synthetic fixture -> (generator, number of seeded tasks, sampling seed)
-SYNTHETIC = {"config1": (synthetic.config1, 512, 11), "config2": (synthetic.config2, 384, 12)}
+SYNTHETIC = {"config1": (synthetic.config1, 512, 11), "config2": (synthetic.config2, 384, 12),
+             "config1_moderate": (synthetic.config1_moderate, 512, 11)}
 
 
 def write_fixture(name, system, a, b, c, outs, env, extra=None):

@@ -1,0 +1,266 @@
+"""Extended-precision truth for the ill-conditioned elements of the synthetic fixtures.
+
+Run here, after make_golden.py (needs oracle/_ref, libgrpp compiled from its sources):
+
+    make -C oracle oracle ref
+    python tests/golden/make_truth.py [--only config1 config1_moderate config2 config3]
+
+On the synthetic workloads (exponents up to 5e3 on f..h shells, potential centres
+up to tens of bohr away) libgrpp keeps few or no significant digits on some blocks:
+its own result moves by up to the size of the values when its inputs move by a few
+units in the last place. No double-precision evaluation of its formulas can be
+checked against it element by element there. This script computes, for those
+blocks, the value libgrpp's formulas converge to, with oracle/truth_quad.c
+(binary128 arithmetic, converged radial integrals, no screening or skip
+thresholds), and records how far libgrpp itself is from it.
+
+Per fixture, written to tests/golden/truth_<name>.npz:
+  tasks              fixture task indices evaluated (config1, config2): every task
+                     with an element whose reference spread env exceeds 1/8 of the
+                     strict tolerance max(1e-10, 1e-9 |ref|)
+  truth_<comp>       binary128 blocks of those tasks, rounded to double
+  refdev_<comp>      max over the reference run and its ten perturbed re-runs
+                     (tests/util.py ENV_MODES) of |ref_p - truth|: how far libgrpp
+                     itself lands from the exact value
+  truthdev_<comp>    max over two perturbed inputs (modes 3, 4) of
+                     |truth_p - truth|: the exact value's own sensitivity to the
+                     same input changes (small: the loss of digits is in the
+                     formulas' double-precision evaluation, not in the integral)
+  level, resid       deepest radial grid level and final relative change of the
+                     radial integrals per task
+config3 (density-contracted gradient, all tasks): truth_grad [4, n_atoms, 3] from
+the binary128 blocks of the differentiated shell pairs (L+1 with 2a N_L/N_{L+1},
+L-1 with N_L/N_{L-1}, libgrpp/diff_gaussian.c:35-63) contracted with D under
+libgrpp's atom and sign rule (libgrpp/grpp_integrals_gradient.c:280-393), and
+refdev_grad, the oracle's own distance from it over the same eleven runs (the
+config3 reference values are the oracle's: the compiled libgrpp gradient reads
+outside its L-1 block and can return NaN).
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from libgrpp_b200.system import BatchArrays, cartesian_list, ncart  # noqa: E402
+from tests.util import (COMPS, ENV_MODES, fixture_subset, load_fixture, load_oracle, load_ref,  # noqa: E402
+                        perturbed, strict_tol, system_from_fixture, truth_full_batch)
+
+U = 2.0 ** -53
+
+
+def flagged_tasks(batch, z):
+    off = batch.block_offsets()
+    flag = set()
+    for c in COMPS:
+        bad = np.where(z["env_" + c] > strict_tol(z["ref_" + c]) / 8)[0]
+        flag |= set(int(t) for t in np.searchsorted(off, bad, side="right") - 1)
+    return sorted(flag)
+
+
+def make_blocks(name, ref_lib, nthreads):
+    batch, z = load_fixture(name)
+    idx = flagged_tasks(batch, z)
+    sub, _, _ = fixture_subset(batch, z, idx)
+    t = time.time()
+    truth, level, resid = truth_full_batch(sub, nthreads=nthreads)
+    print(f"{name}: {len(idx)} tasks, truth in {time.time() - t:.0f} s, deepest level {level.max()}, "
+          f"worst residual {resid.max():.1e}")
+    base = ref_lib.driver_full_batch(sub, nthreads=nthreads)
+    refdev = [np.abs(base[m] - truth[m]) for m in range(4)]
+    for mode in ENV_MODES:
+        p = ref_lib.driver_full_batch(perturbed(sub, mode), nthreads=nthreads)
+        for m in range(4):
+            refdev[m] = np.maximum(refdev[m], np.abs(p[m] - truth[m]))
+    truthdev = [np.zeros_like(x) for x in truth]
+    for mode in (3, 4):
+        tp, _, _ = truth_full_batch(perturbed(sub, mode), nthreads=nthreads)
+        for m in range(4):
+            truthdev[m] = np.maximum(truthdev[m], np.abs(tp[m] - truth[m]))
+    data = dict(tasks=np.array(idx, dtype=np.int32), level=level, resid=resid)
+    for m, c in enumerate(COMPS):
+        data["truth_" + c] = truth[m]
+        data["refdev_" + c] = refdev[m]
+        data["truthdev_" + c] = truthdev[m]
+        e = np.abs(base[m] - truth[m])
+        print(f"  {c}: max |ref - truth| {e.max():.2e} ({int(np.sum(e > strict_tol(truth[m])))} elements beyond "
+              f"1e-10/1e-9), max refdev {refdev[m].max():.2e}, max truthdev {truthdev[m].max():.2e}")
+    out = os.path.join(HERE, f"truth_{name}.npz")
+    np.savez_compressed(out, **data)
+    print(f"  -> {os.path.relpath(out, ROOT)} ({os.path.getsize(out) / 1e3:.0f} kB)")
+
+
+# ---------------------------------------------------------------- gradient
+
+def _points_equal(a, b):
+    return bool(np.all(np.abs(np.asarray(a) - np.asarray(b)) < 1e-12))
+
+
+def gradient_terms(A, B, C, D):
+    """(differentiate bra?, sign) pairs of libgrpp_full_grpp_integrals_gradient for point D
+    (libgrpp/grpp_integrals_gradient.c:280-393)."""
+    pe = _points_equal
+    out = []
+    if pe(A, C) and pe(B, C):
+        return out
+    if not pe(A, D) and not pe(B, D) and not pe(C, D):
+        return out
+    if not pe(A, C) and not pe(C, B) and not pe(A, B):
+        if pe(A, D):
+            out.append((True, 1.0))
+        if pe(B, D):
+            out.append((False, 1.0))
+        if pe(C, D):
+            out += [(True, -1.0), (False, -1.0)]
+    if pe(A, B) and not pe(A, C):
+        f = 1.0 if pe(A, D) else -1.0
+        out += [(True, f), (False, f)]
+    if not pe(A, C) and pe(C, B):
+        out.append((True, 1.0 if pe(A, D) else -1.0))
+    if pe(A, C) and not pe(C, B):
+        out.append((False, 1.0 if pe(B, D) else -1.0))
+    return out
+
+
+def _gnorm(L, a):
+    return (2 * a / np.pi) ** 0.75 * (4 * a) ** (0.5 * L)
+
+
+def derivative_batch(batch, cart_order):
+    """The batch's shells plus, for each shell, its L+1 and L-1 differentiated shells, and the
+    task list (A-1,B) (A+1,B) (A,B-1) (A,B+1) per task (-1 where L = 0)."""
+    d = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in batch.__dict__.items() if not k.startswith("_")}
+    sL, snp, spo, sco = (list(d[k]) for k in ("shell_L", "shell_nprim", "shell_prim_off", "shell_cart_off"))
+    pc, pa, so, cart = list(d["prim_coef"]), list(d["prim_alpha"]), list(d["shell_origin"]), list(d["cart_list"])
+    ns = len(sL)
+
+    def add(s, L, raise_):
+        idx = len(sL)
+        sL.append(L)
+        snp.append(snp[s])
+        spo.append(len(pc))
+        sco.append(len(cart) // 3)
+        cart.extend(cartesian_list(L, cart_order).ravel().tolist())
+        for i in range(snp[s]):
+            al = pa[spo[s] + i]
+            f = 2.0 * al * _gnorm(sL[s], al) / _gnorm(L, al) if raise_ else _gnorm(sL[s], al) / _gnorm(L, al)
+            pc.append(pc[spo[s] + i] * f)
+            pa.append(al)
+        so.extend(so[3 * s:3 * s + 3])
+        return idx
+
+    up = [add(s, sL[s] + 1, True) for s in range(ns)]
+    dn = [add(s, sL[s] - 1, False) if sL[s] > 0 else -1 for s in range(ns)]
+    ta, tb, tc, sub = [], [], [], []
+    for t in range(len(d["task_a"])):
+        a, b, c = int(d["task_a"][t]), int(d["task_b"][t]), int(d["task_c"][t])
+        ids = []
+        for x, y in ((dn[a], b), (up[a], b), (a, dn[b]), (a, up[b])):
+            if x < 0 or y < 0:
+                ids.append(-1)
+                continue
+            ta.append(x)
+            tb.append(y)
+            tc.append(c)
+            ids.append(len(ta) - 1)
+        sub.append(ids)
+    d.update(shell_L=np.array(sL, np.int32), shell_nprim=np.array(snp, np.int32), shell_prim_off=np.array(spo, np.int32),
+             shell_cart_off=np.array(sco, np.int32), prim_coef=np.array(pc), prim_alpha=np.array(pa),
+             shell_origin=np.array(so), cart_list=np.array(cart, np.int32), task_a=np.array(ta, np.int32),
+             task_b=np.array(tb, np.int32), task_c=np.array(tc, np.int32))
+    return BatchArrays(**d), sub
+
+
+def truth_gradient(system, batch, D, nthreads):
+    """d tr(D V^m)/dR [4, n_atoms, 3] from binary128 blocks of the differentiated shell pairs."""
+    dbatch, sub = derivative_batch(batch, system.cart_order)
+    blocks, level, resid = truth_full_batch(dbatch, nthreads=nthreads)
+    off = dbatch.block_offsets()
+    bo = system.basis_offsets()
+    g = np.zeros((4, len(system.atoms), 3))
+    cl = {L: [tuple(c) for c in cartesian_list(L, system.cart_order)] for L in range(12)}
+    for t in range(len(batch.task_a)):
+        a, b, c = int(batch.task_a[t]), int(batch.task_b[t]), int(batch.task_c[t])
+        la, lb = int(batch.shell_L[a]), int(batch.shell_L[b])
+        A, B = batch.shell_origin[3 * a:3 * a + 3], batch.shell_origin[3 * b:3 * b + 3]
+        C = batch.centre_origin[3 * c:3 * c + 3]
+        Dab = D[bo[a]:bo[a] + ncart(la), bo[b]:bo[b] + ncart(lb)]
+        side = np.zeros((2, 3, 4))  # d/dA (bra), d/dB (ket) of sum_ij D_ij V_ij
+        for s, (td, tu, l_d, l_o) in enumerate(((sub[t][0], sub[t][1], la, lb), (sub[t][2], sub[t][3], lb, la))):
+            for m in range(4):
+                Vu = blocks[m][off[tu]:off[tu + 1]].reshape((ncart(la + 1), ncart(lb)) if s == 0 else (ncart(la), ncart(lb + 1)))
+                Vd = None
+                if td >= 0:
+                    Vd = blocks[m][off[td]:off[td + 1]].reshape((ncart(la - 1), ncart(lb)) if s == 0 else (ncart(la), ncart(lb - 1)))
+                for k in range(3):
+                    acc = 0.0
+                    for i, ci in enumerate(cl[l_d]):
+                        up_c = list(ci)
+                        up_c[k] += 1
+                        iu = cl[l_d + 1].index(tuple(up_c))
+                        row_u = Vu[iu, :] if s == 0 else Vu[:, iu]
+                        val = row_u.copy()
+                        if ci[k] > 0 and Vd is not None:
+                            dn_c = list(ci)
+                            dn_c[k] -= 1
+                            idn = cl[l_d - 1].index(tuple(dn_c))
+                            val = val - ci[k] * (Vd[idn, :] if s == 0 else Vd[:, idn])
+                        acc += float(np.dot(Dab[i, :], val)) if s == 0 else float(np.dot(Dab[:, i], val))
+                    side[s, k, m] = acc
+        atoms = [int(system.shell_atom[a]), int(system.shell_atom[b]), int(system.centre_atom[c])]
+        for q, at in enumerate(atoms):
+            if at in atoms[:q]:
+                continue
+            for diff_bra, f in gradient_terms(A, B, C, system.atoms[at]):
+                g[:, at, :] += f * side[0 if diff_bra else 1].T
+    return g, level, resid
+
+
+def make_gradient(nthreads):
+    batch, z = load_fixture("config3")
+    S = system_from_fixture(z)
+    D = z["D"]
+    t = time.time()
+    g, level, resid = truth_gradient(S, batch, D, nthreads)
+    print(f"config3: truth gradient of {len(batch.task_a)} tasks in {time.time() - t:.0f} s, deepest level "
+          f"{level.max()}, worst residual {resid.max():.1e}")
+    import copy
+    orc = load_oracle()
+    refdev = np.abs(orc.driver_grad_contract(S, batch, D, nthreads=nthreads) - g)
+    for mode in ENV_MODES:
+        sp = copy.copy(S)
+        if mode == 2:
+            sp.atoms = np.asarray(S.atoms) * (1 + 4 * U)
+        refdev = np.maximum(refdev, np.abs(orc.driver_grad_contract(sp, perturbed(batch, mode), D, nthreads=nthreads) - g))
+    e = np.abs(z["ref_grad"] - g)
+    print(f"  max |oracle - truth| {e.max():.2e} ({int(np.sum(e > strict_tol(g)))} elements beyond 1e-10/1e-9), "
+          f"max refdev {refdev.max():.2e}, max |g| {np.abs(g).max():.2e}")
+    out = os.path.join(HERE, "truth_config3.npz")
+    np.savez_compressed(out, truth_grad=g, refdev_grad=refdev, level=level, resid=resid)
+    print(f"  -> {os.path.relpath(out, ROOT)} ({os.path.getsize(out) / 1e3:.0f} kB)")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", nargs="*")
+    ap.add_argument("--threads", type=int, default=0)
+    args = ap.parse_args()
+    ref = load_ref()
+    if ref is None:
+        raise SystemExit("oracle/_ref/libgrpp_ref.so is not built (make -C oracle ref)")
+    for name in ("config1", "config1_moderate", "config2"):
+        if not args.only or name in args.only:
+            make_blocks(name, ref, args.threads)
+    if not args.only or "config3" in args.only:
+        make_gradient(args.threads)
+
+
+if __name__ == "__main__":
+    main()

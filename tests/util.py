@@ -11,6 +11,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "libgrpp_oracle.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libgrpp_ref.so")
+TRUTH_SO = os.path.join(ROOT, "oracle", "_build", "libgrpp_truth.so")
 COMPS = ("arep", "so_x", "so_y", "so_z")
 
 
@@ -19,6 +20,31 @@ def ensure_oracle():
         import subprocess
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True, capture_output=True)
     return ORACLE_SO
+
+
+def truth_full_batch(batch, t0=0, t1=None, nthreads=0):
+    """Extended-precision (binary128) full-GRPP blocks of tasks t0..t1-1 (oracle/truth_quad.c):
+    the four output arrays, the deepest radial grid level of each task and its radial
+    integrals' final change between levels relative to the sum of their absolute terms."""
+    import ctypes as ct
+    if not os.path.exists(TRUTH_SO):
+        import subprocess
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True, capture_output=True)
+    lib = ct.CDLL(TRUTH_SO)
+    D = ct.POINTER(ct.c_double)
+    Ip = ct.POINTER(ct.c_int)
+    lib.truth_full_batch.restype = ct.c_int
+    lib.truth_full_batch.argtypes = [ct.c_void_p, ct.c_int64, ct.c_int64, ct.c_int, D, D, D, D, Ip, D]
+    if t1 is None:
+        t1 = len(batch.task_a)
+    off = batch.block_offsets()
+    n = int(off[t1] - off[t0])
+    outs = [np.zeros(max(n, 1)) for _ in range(4)]
+    lev = np.zeros(max(t1 - t0, 1), dtype=np.int32)
+    res = np.zeros(max(t1 - t0, 1))
+    lib.truth_full_batch(ct.byref(batch.struct), t0, t1, nthreads, *[x.ctypes.data_as(D) for x in outs],
+                         lev.ctypes.data_as(Ip), res.ctypes.data_as(D))
+    return [x[:n] for x in outs], lev[:t1 - t0], res[:t1 - t0]
 
 
 def load_oracle():
@@ -168,6 +194,61 @@ def parity(got, want, env=None, abs_tol=1e-10, rel_tol=1e-9, env_factor=4.0):
     max_rel = float(np.max(err[big] / np.abs(want[big]))) if big.any() else 0.0
     n_env = int(np.sum(~strict_ok & (err <= tol)))
     return ok, float(err.max()) if err.size else 0.0, max_rel, n_env
+
+
+def strict_tol(ref, abs_tol=1e-10, rel_tol=1e-9):
+    """The tolerance of record per element: max(1e-10, 1e-9 |ref| for |ref| > 1e-6)."""
+    ref = np.asarray(ref)
+    tol = np.full(ref.shape, abs_tol)
+    big = np.abs(ref) > 1e-6
+    tol[big] = np.maximum(tol[big], rel_tol * np.abs(ref[big]))
+    return tol
+
+
+def load_truth(name):
+    """tests/golden/truth_<name>.npz (tests/golden/make_truth.py), or None."""
+    p = os.path.join(GOLDEN, f"truth_{name}.npz")
+    return np.load(p) if os.path.exists(p) else None
+
+
+TRUTH_FACTOR = 2.0  # an element judged against the exact value may be off by twice the reference's own distance
+
+
+def truth_parity(got, ref, truth=None, tr_sel=None, comp="arep"):
+    """Element-wise check of record against libgrpp with the extended-precision truth:
+      - every element: |got - ref| <= max(1e-10, 1e-9 |ref| for |ref| > 1e-6) (strict), or
+      - for the elements tr_sel of the tasks in the truth fixture, where libgrpp itself keeps
+        few digits: |got - truth| <= max(strict tolerance of truth, 2 refdev), refdev being the
+        largest distance from the truth of libgrpp's run and its ten perturbed re-runs.
+    Returns (ok, report dict)."""
+    got, ref = np.asarray(got), np.asarray(ref)
+    err = np.abs(got - ref)
+    strict = err <= strict_tol(ref)
+    ok = strict & np.isfinite(got)
+    rep = {"max_abs": float(err.max()) if err.size else 0.0, "strict_fail": int(np.sum(~strict)), "truth_checked": 0,
+           "truth_fail": 0, "worst_truth_ratio": 0.0, "max_ref_truth": 0.0, "max_got_truth": 0.0}
+    if truth is not None and tr_sel is not None and len(tr_sel):
+        tv = truth["truth_" + comp]
+        bound = np.maximum(strict_tol(tv), TRUTH_FACTOR * truth["refdev_" + comp])
+        e_t = np.abs(got[tr_sel] - tv)
+        t_ok = e_t <= bound
+        need = ~strict[tr_sel]
+        rep["truth_checked"] = int(np.sum(need))
+        rep["truth_fail"] = int(np.sum(need & ~t_ok))
+        rep["worst_truth_ratio"] = float(np.max(e_t[need] / bound[need])) if need.any() else 0.0
+        rep["max_ref_truth"] = float(np.max(np.abs(ref[tr_sel] - tv)))
+        rep["max_got_truth"] = float(np.max(e_t))
+        ok[tr_sel] = (strict[tr_sel] | t_ok) & np.isfinite(got[tr_sel])
+    return bool(np.all(ok)), rep
+
+
+def truth_selection(batch, truth):
+    """Element indices (into a fixture's output arrays) of the tasks a truth fixture covers, in
+    the truth arrays' order."""
+    if truth is None:
+        return None
+    off = batch.block_offsets()
+    return np.concatenate([np.arange(off[t], off[t + 1]) for t in truth["tasks"]]).astype(np.int64)
 
 
 def grad_envelope(lib, system, batch, D, nthreads=8, modes=ENV_MODES):
