@@ -18,7 +18,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 
-SOURCES = ["engine.cu", "tables.cpp", "capi.cpp", "noalloc.cu"]
+SOURCES = ["engine.cu", "tables.cpp", "capi.cpp", "fortran_abi.cpp", "noalloc.cu"]
 HEADERS = ["grpp_common.cuh", "specfunc.cuh", "mmd.cuh", "radial.cuh", "angular.cuh", "level_model.cuh", "gradient.cuh", "tables.h",
            "engine.h", "onee.cuh", "nucmodel.h"]
 
@@ -33,7 +33,7 @@ def _newer(target, deps):
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", h)
-                                                       for h in ("libgrpp.h", "libgrpp_b200.h")]
+                                                       for h in ("libgrpp.h", "libgrpp_b200.h", "libgrpp_f90.h")]
     objs = []
     for src in SOURCES:
         s = os.path.join(CSRC, src)

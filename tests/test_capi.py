@@ -15,9 +15,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     names = set()
-    for h in ("libgrpp.h", "libgrpp_b200.h"):
+    for h in ("libgrpp.h", "libgrpp_b200.h", "libgrpp_f90.h"):
         txt = open(os.path.join(ROOT, "include", h)).read()
-        names |= set(re.findall(r"\b(libgrpp_\w+)\s*\(", txt))
+        names |= set(re.findall(r"\b(libgrpp_\w+|evaluate_overlap_integral_contracted_|radial_gto_norm_factor_)\s*\(", txt))
     return sorted(names)
 
 
