@@ -18,8 +18,13 @@ learned_over_plain their ratio (results are bit-identical); e2e = the same
 tasks through the public batched C-ABI call with host inputs and outputs
 (packing, host->device and device->host copies included; the outputs go to
 page-locked host arrays allocated once through libgrpp_b200_host_alloc).
---impl reference times libgrpp itself (oracle/_ref, compiled from its
-sources) on this host's cores over a bounded sample of each step's tasks.
+cpu_baseline and --impl reference time libgrpp itself (oracle/_ref, compiled
+from its sources) on this host's cores: a class-stratified seeded sample of a
+step's tasks, serially per (la, lb, lpot) class and on all cores, extrapolated to
+the whole step by class counts. The default line also carries the gradient
+workload (config3: d tr(D V)/dR of the config-2 system) and the uneven
+multi-molecule batch (config4), each with learned vs plain, CUDA-event kernel
+times and its roofline.
 """
 from __future__ import annotations
 
@@ -141,6 +146,55 @@ def cpu_reference_rate(batch_fn, n_sample: int, threads: int, seed: int = 0):
     return n_sample / dt, dt
 
 
+def task_classes(S, a, b, c):
+    """(la, lb, lpot) class of every task: shell angular momenta and the centre's largest projector L."""
+    La = np.array([s.L for s in S.shells])
+    lpot = np.array([max([p.L for p in g.arep + g.so] + [0]) for g in S.grpps])
+    cg = np.array([cc[1] for cc in S.centres])
+    return (La[a] * 16 + La[b]) * 16 + lpot[cg[c]]
+
+
+def cpu_reference_stratified(S, a, b, c, per_class: int, threads: int, seed: int = 0):
+    """libgrpp (oracle/_ref, compiled from its sources) on a class-stratified sample of a task list:
+    per_class seeded tasks of every (la, lb, lpot) class, run serially class by class (mean
+    seconds per task of each class) and then all together on `threads` threads (parallel
+    efficiency of the sample). The list's serial time is extrapolated as sum over classes of
+    (tasks in the class) x (mean seconds per task of the class); the all-cores time as that
+    over threads x efficiency. Returns the serial and all-cores tasks/s and a description."""
+    from libgrpp_b200.capi import LibGRPP
+    ref = LibGRPP(os.path.join(ROOT, "oracle", "_ref", "libgrpp_ref.so"))
+    cls = task_classes(S, a, b, c)
+    rng = np.random.default_rng(seed)
+    keys, counts = np.unique(cls, return_counts=True)
+    sel_all, serial_work, t_ser_sample = [], 0.0, 0.0
+    for key, n in zip(keys, counts):
+        idx = np.where(cls == key)[0]
+        sel = np.sort(rng.choice(idx, min(per_class, len(idx)), replace=False))
+        sel_all.append(sel)
+        t0 = time.perf_counter()
+        ref.driver_full_batch(S.batch(a[sel], b[sel], c[sel]), nthreads=1)
+        dt = time.perf_counter() - t0
+        t_ser_sample += dt
+        serial_work += n * dt / len(sel)
+    sel = np.sort(np.concatenate(sel_all))
+    # parallel efficiency on the sample repeated to at least 8 tasks per thread (a step has
+    # 65536: the all-cores run of a short sample would measure its load imbalance instead)
+    reps = max(1, -(-8 * threads // len(sel)))
+    rep = np.tile(sel, reps)
+    t0 = time.perf_counter()
+    ref.driver_full_batch(S.batch(a[rep], b[rep], c[rep]), nthreads=threads)
+    t_par = time.perf_counter() - t0
+    eff = reps * t_ser_sample / (threads * t_par)
+    n = len(a)
+    return {"serial": n / serial_work, "all_cores": n * threads * eff / serial_work, "efficiency": eff,
+            "sample_tasks": int(len(sel)), "classes": int(len(keys)), "seconds": t_ser_sample + t_par,
+            "parallel_copies": reps,
+            "sample": f"{len(sel)} seeded tasks, {min(per_class, int(counts.min()))}..{per_class} of each of the "
+                      f"{len(keys)} (la, lb, lpot) classes of the {n}-task step, serially per class, then "
+                      f"{reps} copies of the sample on {threads} threads (efficiency {eff:.2f}); rates extrapolated "
+                      f"by class counts"}
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -152,22 +206,26 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     threads = host_threads()
-    n_sample = args.ref_sample
+    S = system()
     for w in range(args.warmup):
         cpu_reference_rate(lambda: step_tasks(w), max(8, threads), threads, seed=100 + w)
-    rates, secs = [], []
-    for s in range(args.steps):
-        r, dt = cpu_reference_rate(lambda: step_tasks(s), n_sample, threads, seed=s)
-        rates.append(r)
-        secs.append(dt)
-    rate = len(rates) * n_sample / sum(secs)
-    sample = f"{n_sample} seeded random tasks of each step's 65536-task block, {threads} threads"
+    serial, allc, secs, desc = [], [], [], ""
+    for st in range(args.steps):
+        a, b, c = step_tasks(st)
+        r = cpu_reference_stratified(S, a, b, c, args.ref_per_class, threads, seed=st)
+        serial.append(r["serial"])
+        allc.append(r["all_cores"])
+        secs.append(r["seconds"])
+        desc = r["sample"]
+    rate = len(allc) / sum(1.0 / x for x in allc)  # tasks/s over the steps' extrapolated times
+    rate_serial = len(serial) / sum(1.0 / x for x in serial)
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": "tasks/s", "n_gpus": 0, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": 1e3 * 65536 / rate, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": {"workload": WORKLOAD, "l2": "n/a (CPU)"},
-        "cpu_baseline": {"value": rate, "unit": "tasks/s", "cores": threads, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": rate, "unit": "tasks/s", "cores": threads, "kind": "reference", "sample": desc,
+                         "serial": rate_serial, "measured_seconds": sum(secs)},
         "e2e": {"value": rate, "unit": "tasks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -218,6 +276,22 @@ def time_plans(plans, flush, local):
     return float(sum(ms)), kms, cnt, fallbacks, clk.summary()
 
 
+def count_type1(plans, cnt, scale=1.0):
+    """The type 1 kernel's operation counts, from one more, untimed execution of each plan (its
+    counting build is slower); the radial counters of the timed runs are kept."""
+    if not cnt:
+        return
+    for k in ("mmd_triples", "mmd_flops"):
+        cnt[k] = 0
+    for p in plans:
+        p.set_counting(True)
+        p.execute()
+        mc = p.counters()
+        p.set_counting(False)
+        for k in ("mmd_triples", "mmd_flops"):
+            cnt[k] += mc[k] * scale
+
+
 def run_ours(args, rank, world, local):
     import torch
     from libgrpp_b200 import engine
@@ -255,18 +329,7 @@ def run_ours(args, rank, world, local):
         total_ms, kms, cnt, fallbacks, clocks = time_plans(plans, flush, local)
         total_ms, tasks = reduce_time_and_work(dist, total_ms, float(sum(n_tasks)), "cuda")
         st0 = plans[0].stats()
-        # the type 1 kernel's operation counts come from one more, untimed execution
-        # (its counting build is slower); the radial counters of the timed runs are kept
-        if cnt:
-            for k in ("mmd_triples", "mmd_flops"):
-                cnt[k] = 0
-            for p in plans:
-                p.set_counting(True)
-                p.execute()
-                mc = p.counters()
-                p.set_counting(False)
-                for k in ("mmd_triples", "mmd_flops"):
-                    cnt[k] += mc[k]
+        count_type1(plans, cnt)
         res[name] = {"value": tasks / (total_ms / 1e3), "ms_per_step": total_ms / len(plans),
                      "kernel_ms_per_step": {k: v / len(plans) for k, v in kms.items()},
                      "counters": {k: v / len(plans) for k, v in cnt.items()} if cnt else None,
@@ -281,7 +344,7 @@ def run_ours(args, rank, world, local):
 
     # end to end through the public batched call (host in, host out): outputs land in
     # page-locked host arrays the caller allocated once (libgrpp_b200_host_alloc)
-    e2e_batches = batches[: max(1, min(len(batches), args.e2e_steps))]
+    e2e_batches = batches[: max(1, min(len(batches), args.e2e_steps))] if args.e2e_steps > 0 else batches
     n_out = max(int(b.block_offsets()[-1]) for b in e2e_batches)
     outs = [lib.pinned_empty(n_out) for _ in range(4)]
     lib.full_grpp_batch(e2e_batches[0], modes[main_mode], out=outs)
@@ -314,18 +377,31 @@ def run_ours(args, rank, world, local):
         line["learned_fallbacks_per_step"] = R["fallbacks_per_step"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
-        rate, dt = cpu_reference_rate(lambda: step_tasks(idxs[0]), args.ref_sample, threads)
-        line["cpu_baseline"] = {"value": rate, "unit": "tasks/s", "cores": threads, "kind": "reference",
-                                "sample": f"{args.ref_sample} seeded random tasks of the first step's block "
-                                          f"({dt:.1f} s on {threads} threads)"}
+        r = cpu_reference_stratified(S, *step_tasks(idxs[0]), args.ref_per_class, threads)
+        line["cpu_baseline"] = {"value": r["all_cores"], "unit": "tasks/s", "cores": threads, "kind": "reference",
+                                "sample": r["sample"], "serial": r["serial"], "serial_cores": 1,
+                                "measured_seconds": r["seconds"]}
     peak = lib.fp64_peak()
     line["roofline"] = roofline(R["kernel_ms_per_step"], R["counters"], peak)
+    line["roofline"]["traffic"] = TRAFFIC_PER_TASK.get(line["roofline"]["kernel"], 0.0) * n_tasks[0] or None
+    if line["roofline"]["traffic"]:
+        line["roofline"]["traffic_source"] = TRAFFIC_SOURCE
+    if rank == 0 and world == 1 and not args.no_extra:
+        # north_star's other workloads in the same run: the gradient (config 3) and the uneven batch (config 4)
+        line["config3"], _ = gradient_leg(args, lib, local, flush, max(1, min(args.steps, 3)))
+        line["config4"], _ = config4_leg(args, lib, local, flush, 1)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
 
+
+# DRAM bytes per task of the dominant kernel, from one ncu capture of it (dram__bytes_read.sum +
+# dram__bytes_write.sum over the captured launch / its tasks); see profiles/
+TRAFFIC_PER_TASK = {"ms_screen": (19.929856e6 + 19.016704e6) / 4096}
+TRAFFIC_SOURCE = ("ncu --set full of radial_screen_flat_kernel on 4096 tasks of the first config-1 step: 38.95 MB "
+                  "DRAM read+write, scaled to the step's tasks (profiles/screen_kernel_full_4096tasks.md)")
 
 # FLOP model of the radial path (count of FP64 add/mul, FMA = 2, each exp/pow/sqrt/log/erf = 1,
 # per operation of libgrpp's algorithm, libgrpp/radial_type2_integral.c and screening.c):
@@ -381,109 +457,147 @@ def config4_tasks(n_mol):
     return M, a, b, c
 
 
+def config4_leg(args, lib, local, flush, steps):
+    """Uneven batch: the first --molecules molecules of config 4 (2..24 atoms each, full GRPP,
+    basis l <= 6, projectors l <= 5) as one class-sorted task list in chunks of 65536 tasks; a
+    step is one pass over all chunks (CUDA events per kernel), learned and plain alike."""
+    M, a, b, c = config4_tasks(args.molecules)
+    chunks = [M.batch(a[i:i + 65536], b[i:i + 65536], c[i:i + 65536]) for i in range(0, len(a), 65536)]
+    res, outs = {}, {}
+    peak = lib.fp64_peak()
+    for name, mode in (("plain", 0), ("learned", 1)):
+        plans = [lib.plan(ch, mode) for ch in chunks]
+        for p in plans[: max(1, args.warmup)]:
+            p.execute()
+        tot, kms, cnt, fb, clk = 0.0, None, None, 0, None
+        for _ in range(steps):
+            t, k, cn, f, clk = time_plans(plans, flush, local)
+            tot += t
+            fb += f
+            kms = k if kms is None else {q: kms[q] + k[q] for q in k}
+            cnt = cn if cnt is None else {q: cnt[q] + cn[q] for q in cn}
+        outs[name] = [np.concatenate([p.outputs()[m] for p in plans]) for m in range(4)]
+        kms = {q: v / steps for q, v in kms.items()}
+        cnt = {q: v / steps for q, v in cnt.items()}
+        count_type1(plans, cnt)
+        res[name] = {"value": steps * len(a) / (tot / 1e3), "ms_per_step": tot / steps, "kernel_ms_per_step": kms,
+                     "fallbacks_per_step": fb / steps, "clocks": clk,
+                     "roofline": {k: v for k, v in roofline(kms, cnt, peak).items() if k not in ("counters",)}}
+        for p in plans:
+            p.close()
+    max_err = max(float(np.max(np.abs(x - y))) for x, y in zip(outs["learned"], outs["plain"]))
+    out = {"workload": f"config4: first {args.molecules} of 512 molecules (2..24 atoms, full GRPP, l <= 6), {len(a)} "
+                       f"tasks sorted by (la, lb, lpot), {len(chunks)} chunks of 65536, L2 flushed before every chunk",
+           "value": res["learned"]["value"], "unit": "tasks/s", "steps": steps, "learned": res["learned"],
+           "plain": res["plain"], "learned_over_plain": res["learned"]["value"] / res["plain"]["value"],
+           "learned_fallback_rate": res["learned"]["fallbacks_per_step"] / len(a),
+           "max_abs_diff_learned_vs_plain": max_err}
+    return out, (M, a, b, c)
+
+
+def gradient_leg(args, lib, local, flush, steps):
+    """Density-contracted gradient d tr(D V)/dR (four matrices, all atoms) of the config-2 system
+    (16 heavy atoms + 32 H, basis up to h, random symmetric D) over its first --tasks
+    class-sorted tasks: wall clock of the host-in/host-out call (libgrpp_b200_grpp_gradient_contract,
+    and its symmetric-density form with the shell pairs folded), and CUDA-event kernel times of
+    the derivative blocks the call evaluates, for one chunk of 16384 tasks."""
+    from libgrpp_b200 import gradient, synthetic
+    S = synthetic.config2()
+    D = synthetic.config3_density(S)
+    a, b, c = synthetic.sort_tasks(S, *S.all_tasks())
+    n = min(args.tasks, len(a))
+    batch = S.batch(a[:n], b[:n], c[:n])
+    e2e = {}
+    for name, mode, sym in (("plain", 0, False), ("learned", 1, False), ("learned_folded", 1, True)):
+        for _ in range(max(args.warmup, 1)):
+            lib.grad_contract(S, batch, D, radial_mode=mode, symmetric=sym)
+        times = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            lib.grad_contract(S, batch, D, radial_mode=mode, symmetric=sym)
+            times.append(time.perf_counter() - t0)
+        e2e[name] = {"value": n / float(np.median(times)), "seconds_per_step": float(np.median(times))}
+    nk = min(16384, n)
+    dbatch, _ = gradient.derivative_batch(S.batch(a[:nk], b[:nk], c[:nk]), S.cart_order)
+    kern = {}
+    peak = lib.fp64_peak()
+    for name, mode in (("plain", 0), ("learned", 1)):
+        plan = lib.plan(dbatch, mode)
+        for _ in range(max(args.warmup, 1)):
+            plan.execute()
+        tot, kms, cnt, clk = 0.0, None, None, None
+        for _ in range(steps):
+            t, k, cn, _, clk = time_plans([plan], flush, local)
+            tot += t
+            kms = k if kms is None else {q: kms[q] + k[q] for q in k}
+            cnt = cn if cnt is None else {q: cnt[q] + cn[q] for q in cn}
+        kms = {q: v / steps for q, v in kms.items()}
+        cnt = {q: v / steps for q, v in cnt.items()}
+        count_type1([plan], cnt)
+        plan.close()
+        kern[name] = {"tasks_per_s": nk / (tot / steps / 1e3), "derivative_blocks": len(dbatch.task_a),
+                      "ms_per_chunk": tot / steps, "kernel_ms_per_chunk": kms, "clocks": clk,
+                      "roofline": {k: v for k, v in roofline(kms, cnt, peak).items() if k not in ("counters",)}}
+    return {"workload": f"config3: first {n} of {len(a)} class-sorted tasks of config 2 (d tr(D V)/dR, 4 matrices); "
+                        f"e2e = host in / host out wall clock, kernels = CUDA events on {nk} tasks' derivative blocks",
+            "value": e2e["learned"]["value"], "unit": "tasks/s", "steps": steps, "e2e": e2e,
+            "folded_over_full": e2e["learned_folded"]["value"] / e2e["learned"]["value"],
+            "kernels": kern, "learned_over_plain": kern["learned"]["tasks_per_s"] / kern["plain"]["tasks_per_s"]}, \
+        (S, D, a[:n], b[:n], c[:n])
+
+
 def run_config4(args, rank, world, local):
-    """Uneven batch: the first --molecules molecules of config 4 (2..24 atoms each, full
-    GRPP, basis l <= 6, projectors l <= 5) as one class-sorted task list, run as chunks of
-    65536 tasks; a step is one pass over all chunks, learned and plain timed alike."""
     import torch
     from libgrpp_b200 import engine
     if rank != 0:
         return
     torch.cuda.set_device(local)
     lib = engine.load()
-    M, a, b, c = config4_tasks(args.molecules)
-    chunks = [M.batch(a[i:i + 65536], b[i:i + 65536], c[i:i + 65536]) for i in range(0, len(a), 65536)]
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    res, outs = {}, {}
-    for name, mode in (("plain", 0), ("learned", 1)):
-        plans = [lib.plan(ch, mode) for ch in chunks]
-        for p in plans[: max(1, args.warmup)]:
-            p.execute()
-        tot = 0.0
-        fb = 0
-        with ClockSampler(local) as clk:
-            for _ in range(args.steps):
-                for p in plans:
-                    flush.fill_(1.0)
-                    torch.cuda.synchronize()
-                    p.execute()
-                    tot += p.stats()["ms_total"]
-                    fb += p.learned_stats()["fallbacks"]
-        outs[name] = [np.concatenate([p.outputs()[m] for p in plans]) for m in range(4)]
-        res[name] = {"value": args.steps * len(a) / (tot / 1e3), "ms_per_step": tot / args.steps,
-                     "fallbacks_per_step": fb / args.steps, "clocks": clk.summary()}
-        for p in plans:
-            p.close()
-    max_err = max(float(np.max(np.abs(x - y))) for x, y in zip(outs["learned"], outs["plain"]))
-    line = {"metric": METRIC, "value": res["learned"]["value"], "unit": "tasks/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": res["learned"]["ms_per_step"], "higher_is_better": True,
+    leg, (M, a, b, c) = config4_leg(args, lib, local, flush, args.steps)
+    line = {"metric": METRIC, "value": leg["value"], "unit": "tasks/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": leg["learned"]["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config 4)",
-            "config": {"workload": f"config4: first {args.molecules} of 512 molecules (2..24 atoms, full GRPP, l <= 6), "
-                                   f"{len(a)} tasks sorted by (la, lb, lpot), {len(chunks)} chunks of 65536",
-                       "l2": "flushed before every chunk"},
-            "plain": res["plain"], "learned_over_plain": res["learned"]["value"] / res["plain"]["value"],
-            "learned_fallback_rate": res["learned"]["fallbacks_per_step"] / len(a),
-            "max_abs_diff_learned_vs_plain": max_err, "clocks": res["learned"]["clocks"]}
+            "config": {"workload": leg["workload"]}, "clocks": leg["learned"]["clocks"], "config4": leg}
     if not args.no_cpu_baseline:
-        from libgrpp_b200.capi import LibGRPP
-        ref = LibGRPP(os.path.join(ROOT, "oracle", "_ref", "libgrpp_ref.so"))
-        sel = np.sort(np.random.default_rng(0).choice(len(a), args.ref_sample, replace=False))
-        threads = host_threads()
-        t0 = time.perf_counter()
-        ref.driver_full_batch(M.batch(a[sel], b[sel], c[sel]), nthreads=threads)
-        dt = time.perf_counter() - t0
-        line["cpu_baseline"] = {"value": args.ref_sample / dt, "unit": "tasks/s", "cores": threads, "kind": "reference",
-                                "sample": f"{args.ref_sample} seeded random tasks of the batch ({dt:.1f} s)"}
+        r = cpu_reference_stratified(M, a, b, c, args.ref_per_class, host_threads())
+        line["cpu_baseline"] = {"value": r["all_cores"], "unit": "tasks/s", "cores": host_threads(), "kind": "reference",
+                                "sample": r["sample"], "serial": r["serial"]}
     print(json.dumps(line), flush=True)
 
 
 def run_config3(args, rank, world, local):
-    """Density-contracted gradient d tr(D V)/dR (all four matrices, all atoms) of the
-    config-2 system (16 heavy atoms + 32 H, basis up to h) with a random symmetric D,
-    over its first --tasks class-sorted tasks (shell pair x centre)."""
     import torch
-    from libgrpp_b200 import engine, synthetic
+    from libgrpp_b200 import engine
     if rank != 0:
         return
     torch.cuda.set_device(local)
     lib = engine.load()
-    S = synthetic.config2()
-    D = synthetic.config3_density(S)
-    a, b, c = synthetic.sort_tasks(S, *S.all_tasks())
-    n = min(args.tasks, len(a))
-    batch = S.batch(a[:n], b[:n], c[:n])
-    res = {}
-    for name, mode in (("plain", 0), ("learned", 1)):
-        # warm-up at full size: angular tables of every (L, l) class and buffer growth happen here
-        for _ in range(max(args.warmup, 1)):
-            lib.grad_contract(S, batch, D, radial_mode=mode)
-        times = []
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            g = lib.grad_contract(S, batch, D, radial_mode=mode)
-            times.append(time.perf_counter() - t0)
-        dt = float(np.median(times))  # wall clock of a host-in/host-out call: the median of the steps
-        res[name] = {"value": n / dt, "seconds_per_step": dt, "seconds_all_steps": times,
-                     "max_abs_grad": float(np.abs(g).max())}
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    leg, (S, D, a, b, c) = gradient_leg(args, lib, local, flush, args.steps)
     line = {"metric": "shell-pair x RPP-centre gradient tasks/s (d tr(D V)/dR, 4 matrices, FP64)",
-            "value": res["learned"]["value"], "unit": "tasks/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": max(args.warmup, 1), "ms_per_step": 1e3 * res["learned"]["seconds_per_step"], "higher_is_better": True,
+            "value": leg["value"], "unit": "tasks/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 1),
+            "ms_per_step": 1e3 * leg["e2e"]["learned"]["seconds_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config 2 system, D seed 3)",
-            "config": {"workload": f"config3: first {n} of {len(a)} class-sorted tasks of config 2, host in / host out "
-                                   "(libgrpp_b200_grpp_gradient_contract, wall clock)"},
-            "plain": res["plain"], "learned_over_plain": res["learned"]["value"] / res["plain"]["value"]}
+            "config": {"workload": leg["workload"]}, "config3": leg}
     if not args.no_cpu_baseline:
-        from libgrpp_b200.capi import LibGRPP
-        ref = LibGRPP(os.path.join(ROOT, "oracle", "_build", "libgrpp_oracle.so"))
-        sel = np.sort(np.random.default_rng(0).choice(n, args.ref_sample, replace=False))
-        threads = host_threads()
-        t0 = time.perf_counter()
-        ref.driver_grad_contract(S, S.batch(a[sel], b[sel], c[sel]), D, nthreads=threads)
-        dt = time.perf_counter() - t0
-        line["cpu_baseline"] = {"value": args.ref_sample / dt, "unit": "tasks/s", "cores": threads, "kind": "port",
-                                "sample": f"{args.ref_sample} seeded random tasks, the oracle's restated "
-                                          f"libgrpp_full_grpp_integrals_gradient per atom ({dt:.1f} s)"}
+        line["cpu_baseline"] = gradient_cpu_baseline(args, S, D, a, b, c)
     print(json.dumps(line), flush=True)
+
+
+def gradient_cpu_baseline(args, S, D, a, b, c):
+    """The oracle's restated libgrpp_full_grpp_integrals_gradient contracted with D (libgrpp's own
+    gradient reads outside its L-1 block and can return NaN), all cores, on a seeded sample."""
+    from libgrpp_b200.capi import LibGRPP
+    ref = LibGRPP(os.path.join(ROOT, "oracle", "_build", "libgrpp_oracle.so"))
+    ns = min(args.ref_sample, len(a))
+    sel = np.sort(np.random.default_rng(0).choice(len(a), ns, replace=False))
+    threads = host_threads()
+    t0 = time.perf_counter()
+    ref.driver_grad_contract(S, S.batch(a[sel], b[sel], c[sel]), D, nthreads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": ns / dt, "unit": "tasks/s", "cores": threads, "kind": "port",
+            "sample": f"{ns} seeded random tasks, the oracle's restated gradient per atom ({dt:.1f} s)"}
 
 
 def main():
@@ -494,8 +608,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--mode", choices=["plain", "learned"], default="learned",
                     help="headline radial mode; learned also times plain on the same steps")
-    ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--ref-sample", type=int, default=256)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="steps timed end to end; 0 = every timed step")
+    ap.add_argument("--ref-sample", type=int, default=256, help="config3 CPU baseline: sampled tasks")
+    ap.add_argument("--ref-per-class", type=int, default=6,
+                    help="CPU baseline: seeded tasks per (la, lb, lpot) class of the stratified sample")
+    ap.add_argument("--no-extra", action="store_true", help="leave the config3 / config4 legs out of the default line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tasks-per-step", type=int, default=0,
                     help="evenly spaced subset of each step's tasks (profiling runs); 0 = the full block")

@@ -207,6 +207,10 @@ enum {
 void libgrpp_nuclear_attraction_integrals(libgrpp_shell_t *shell_A, libgrpp_shell_t *shell_B, double *charge_origin,
                                           int charge, int nuclear_model, double *model_params, double *coulomb_matrix);
 
+/* The model-specific forms below pass libgrpp_nuclear_attraction_integrals the array
+ * {charge, parameters...}, as libgrpp's do (nuclear_attraction.c:177-236); the generic function
+ * reads the model's parameters from the first element, so these forms use the charge as the
+ * first model parameter, exactly as in libgrpp. */
 void libgrpp_nuclear_attraction_integrals_point_charge(libgrpp_shell_t *shell_A, libgrpp_shell_t *shell_B,
                                                        double *charge_origin, int charge, double *coulomb_matrix);
 

@@ -178,6 +178,17 @@ int libgrpp_b200_nuclear_attraction_batch(const libgrpp_b200_batch_t *batch, int
  * independent evaluation of the same integrals libgrpp_type1_integrals gives. L_A + L_B <= 12. */
 int libgrpp_b200_type1_numeric_batch(const libgrpp_b200_batch_t *batch, double *arep);
 
+/* The same gradient for a symmetric density (checked: |D_ij - D_ji| <= 1e-14 max|D|, else
+ * LIBGRPP_B200_ERR_INVALID). A task (B, A, C) then contributes to tr(D V_arep) what (A, B, C)
+ * does, and every spin-orbit contraction tr(D V_so) vanishes (the SO matrices are
+ * antisymmetric): the ordered tasks are folded onto A <= B (each shell-pair block and its
+ * derivatives evaluated once, weight 2 where both orders are listed), no spin-orbit
+ * potential is evaluated, and g[1..3][..] (so_x, so_y, so_z), whose exact value is zero,
+ * receive no contribution. */
+int libgrpp_b200_grpp_gradient_contract_symmetric(const libgrpp_b200_batch_t *batch, int radial_mode,
+                                                  const int *shell_atom, const int *centre_atom, const double *atom_xyz,
+                                                  int n_atoms, const int *bf_off, int n_bf, const double *D, double *g);
+
 /* Learned grid-level model (no counterpart in libgrpp).
  *
  * libgrpp's type 2 radial quadrature (radial_type2_integral.c:242-318) doubles a

@@ -98,6 +98,8 @@ class LibGRPP:
         self._opt("libgrpp_b200_plan_learned_stats", ct.c_int, [_V, _D, ct.POINTER(ct.c_int64)])
         self._opt("libgrpp_b200_grpp_gradient_contract", ct.c_int,
                   [_V, ct.c_int, _I, _I, _D, ct.c_int, _I, ct.c_int, _D, _D])
+        self._opt("libgrpp_b200_grpp_gradient_contract_symmetric", ct.c_int,
+                  [_V, ct.c_int, _I, _I, _D, ct.c_int, _I, ct.c_int, _D, _D])
         self._opt("libgrpp_b200_set_level_model", ct.c_int, [_F])
         self._opt("libgrpp_b200_level_samples", ct.c_int, [_V, _F, _B, ct.POINTER(ct.c_int64)])
         self._opt("libgrpp_overlap_integrals", None, [_V, _V, _D])
@@ -352,9 +354,11 @@ class LibGRPP:
             raise RuntimeError(self.last_error_message())
         return v.value
 
-    def grad_contract(self, system, batch, D, radial_mode=0):
+    def grad_contract(self, system, batch, D, radial_mode=0, symmetric=False):
         """d tr(D V^m) / d R for the four matrices m over the batch's tasks: [4, n_atoms, 3]
-        (libgrpp_b200_grpp_gradient_contract; same quantity as the oracle's driver_grad_contract)."""
+        (libgrpp_b200_grpp_gradient_contract; same quantity as the oracle's driver_grad_contract).
+        symmetric: libgrpp_b200_grpp_gradient_contract_symmetric (D symmetric: shell pairs folded,
+        spin-orbit parts zero)."""
         if radial_mode == 1:
             self.ensure_level_model()
         nat = len(system.atoms)
@@ -364,8 +368,9 @@ class LibGRPP:
         xyz = np.ascontiguousarray(system.atoms, dtype=np.float64)
         bo = np.ascontiguousarray(system.basis_offsets()[:-1], dtype=np.int32)
         Dm = np.ascontiguousarray(D, dtype=np.float64)
-        rc = self.lib.libgrpp_b200_grpp_gradient_contract(ct.byref(batch.struct), radial_mode, _ip(sa), _ip(ca), _dp(xyz),
-                                                          nat, _ip(bo), int(Dm.shape[0]), _dp(Dm), _dp(g))
+        f = self.lib.libgrpp_b200_grpp_gradient_contract_symmetric if symmetric else self.lib.libgrpp_b200_grpp_gradient_contract
+        rc = f(ct.byref(batch.struct), radial_mode, _ip(sa), _ip(ca), _dp(xyz), nat, _ip(bo), int(Dm.shape[0]), _dp(Dm),
+               _dp(g))
         self._check(rc, "libgrpp_b200_grpp_gradient_contract")
         return g
 

@@ -165,6 +165,7 @@ __global__ void oc_proj_kernel(OcProjArgs a)
 constexpr int kFinThreads = 128;
 constexpr int kFinElemPerThread = 8;  // up to 1024 Cartesian pairs
 constexpr int kFinMaxLam = 24;
+constexpr int kLmatPairs = 100;  // (m1, m2) pairs of the L matrices with a non-zero component: 10L - 4 <= 96 for L <= 10
 constexpr int kFinMaxSl = 24;         // semilocal potentials per centre
 constexpr int kFinMaxOc = 32;         // outercore shells per centre
 
@@ -355,6 +356,11 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
     // chain of products 1 * u * u ... as the reference's per-term loops
     __shared__ double upow[2][3][kFinMaxLam + 1];
     __shared__ int8_t nabcA[n_abc(kMaxL)], nabcB[n_abc(kMaxL)];  // |abc| of each abc index
+    // spin-orbit: the (m1, m2) pairs, in m1-major order, at which some L matrix component is
+    // non-zero (spin_orbit_integrals.c:206-222 skips the others), with the three values
+    __shared__ int8_t lpm1[kLmatPairs], lpm2[kLmatPairs];
+    __shared__ double lpv[3][kLmatPairs];
+    __shared__ int s_npair;
     const int tid = threadIdx.x;
     double *rshA = dsm, *rshB = rshA + sm.n_rsh, *omA = rshB + sm.n_rsh, *omB = omA + sm.n_omega, *Qs = omB + sm.n_omega,
            *V = Qs + sm.n_q;
@@ -551,6 +557,23 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                 }
                 for (int e = tid; e < d1 * d2 * dn; e += kFinThreads) Qs[e] = a.Q[qbase + qoff + e];
                 qoff += (int64_t)d1 * d2 * dn;
+                if (so && tid == 0) {
+                    int np = 0;
+                    for (int m1 = -L; m1 <= L; m1++)
+                        for (int m2 = -L; m2 <= L; m2++) {
+                            const double lx = lmat_val(L, 0, m1, m2), ly = lmat_val(L, 1, m1, m2), lz = lmat_val(L, 2, m1, m2);
+                            if (fabs(lx) < kZeroThresh && fabs(ly) < kZeroThresh && fabs(lz) < kZeroThresh) continue;
+                            if (np < kLmatPairs) {
+                                lpm1[np] = (int8_t)(m1 + L);
+                                lpm2[np] = (int8_t)(m2 + L);
+                                lpv[0][np] = lx;
+                                lpv[1][np] = ly;
+                                lpv[2][np] = lz;
+                            }
+                            np++;
+                        }
+                    s_npair = np;  // never above kLmatPairs for L <= 10 (10L - 4 pairs)
+                }
                 __syncthreads();
 
                 const int ncomp = so ? 3 : 1;
@@ -585,19 +608,18 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                                     }
                                     v0 += QN * sa2;
                                 } else {
+                                    // the non-zero (m1, m2) pairs in the reference's loop order: the same terms,
+                                    // added in the same order, as the dense double loop with its skip
                                     double sx = 0.0, sy = 0.0, sz = 0.0;
-                                    for (int m1 = -L; m1 <= L; m1++)
-                                        for (int m2 = -L; m2 <= L; m2++) {
-                                            const double lx = lmat_val(L, 0, m1, m2), ly = lmat_val(L, 1, m1, m2),
-                                                         lz = lmat_val(L, 2, m1, m2);
-                                            if (fabs(lx) < kZeroThresh && fabs(ly) < kZeroThresh && fabs(lz) < kZeroThresh) continue;
-                                            const double o1 = w1[m1 + L];
-                                            if (fabs(o1) < kZeroThresh) continue;
-                                            const double o2 = w2[m2 + L];
-                                            sx += o1 * o2 * lx;
-                                            sy += o1 * o2 * ly;
-                                            sz += o1 * o2 * lz;
-                                        }
+                                    const int npair = min(s_npair, kLmatPairs);
+                                    for (int q = 0; q < npair; q++) {
+                                        const double o1 = w1[lpm1[q]];
+                                        if (fabs(o1) < kZeroThresh) continue;
+                                        const double o2 = w2[lpm2[q]];
+                                        sx += o1 * o2 * lpv[0][q];
+                                        sy += o1 * o2 * lpv[1][q];
+                                        sz += o1 * o2 * lpv[2][q];
+                                    }
                                     v0 += QN * sx;
                                     v1 += QN * sy;
                                     v2 += QN * sz;

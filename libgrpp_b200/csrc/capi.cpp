@@ -13,7 +13,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "../../include/libgrpp.h"
@@ -742,9 +744,71 @@ int libgrpp_b200_plan_set_counting(libgrpp_b200_plan_t *plan, int on)
     return 0;
 }
 
+static int grad_contract_impl(const libgrpp_b200_batch_t *b, int radial_mode, const int *shell_atom,
+                              const int *centre_atom, const double *atom_xyz, int n_atoms, const int *bf_off, int n_bf,
+                              const double *D, double *g, const double *task_weight, bool arep_only);
+
 int libgrpp_b200_grpp_gradient_contract(const libgrpp_b200_batch_t *b, int radial_mode, const int *shell_atom,
                                         const int *centre_atom, const double *atom_xyz, int n_atoms, const int *bf_off,
                                         int n_bf, const double *D, double *g)
+{
+    return grad_contract_impl(b, radial_mode, shell_atom, centre_atom, atom_xyz, n_atoms, bf_off, n_bf, D, g, nullptr,
+                              false);
+}
+
+// Symmetric density: the task (B, A, C) contributes to the arep gradient exactly what (A, B, C)
+// does (D_BA = D_AB^T, V_BA = V_AB^T), and every spin-orbit contraction vanishes (the SO
+// matrices and their derivatives are antisymmetric). The ordered task list is folded onto
+// A <= B with weight 2 for A < B when both orders are present, spin-orbit potentials are left
+// out of the derivative batch, and the spin-orbit gradient is returned as exact zeros.
+int libgrpp_b200_grpp_gradient_contract_symmetric(const libgrpp_b200_batch_t *b, int radial_mode, const int *shell_atom,
+                                                  const int *centre_atom, const double *atom_xyz, int n_atoms,
+                                                  const int *bf_off, int n_bf, const double *D, double *g)
+{
+    if (!check_init()) return LIBGRPP_B200_ERR_NOT_INIT;
+    grpp::set_error(0, "");
+    auto invalid = [](const char *m) {
+        grpp::set_error(LIBGRPP_B200_ERR_INVALID, m);
+        return LIBGRPP_B200_ERR_INVALID;
+    };
+    if (!b || !D || !g || n_bf <= 0 || b->n_tasks < 0) return invalid("gradient contraction: null argument or empty size");
+    double dmax = 0.0;
+    for (int64_t i = 0; i < (int64_t)n_bf * n_bf; i++) dmax = std::max(dmax, std::fabs(D[i]));
+    for (int i = 0; i < n_bf; i++)
+        for (int j = 0; j < i; j++)
+            if (std::fabs(D[(int64_t)i * n_bf + j] - D[(int64_t)j * n_bf + i]) > 1e-14 * dmax)
+                return invalid("gradient contraction: the density matrix is not symmetric");
+    // fold (a, b, c) and (b, a, c) onto a <= b
+    std::map<std::tuple<int, int, int>, int> seen;
+    std::vector<int> fa, fb, fc;
+    std::vector<double> w;
+    for (int64_t t = 0; t < b->n_tasks; t++) {
+        const int a = std::min(b->task_a[t], b->task_b[t]), bb = std::max(b->task_a[t], b->task_b[t]), c = b->task_c[t];
+        auto it = seen.find({a, bb, c});
+        if (it == seen.end()) {
+            seen[{a, bb, c}] = (int)fa.size();
+            fa.push_back(a);
+            fb.push_back(bb);
+            fc.push_back(c);
+            w.push_back(1.0);
+        } else {
+            w[it->second] += 1.0;
+        }
+    }
+    libgrpp_b200_batch_t v = *b;
+    v.n_tasks = (int64_t)fa.size();
+    v.task_a = fa.data();
+    v.task_b = fb.data();
+    v.task_c = fc.data();
+    std::vector<int> no_so(b->n_grpps, 0);
+    v.grpp_n_so = no_so.data();
+    return grad_contract_impl(&v, radial_mode, shell_atom, centre_atom, atom_xyz, n_atoms, bf_off, n_bf, D, g, w.data(),
+                              true);
+}
+
+static int grad_contract_impl(const libgrpp_b200_batch_t *b, int radial_mode, const int *shell_atom,
+                              const int *centre_atom, const double *atom_xyz, int n_atoms, const int *bf_off, int n_bf,
+                              const double *D, double *g, const double *task_weight, bool arep_only)
 {
     if (!check_init()) return LIBGRPP_B200_ERR_NOT_INIT;
     grpp::set_error(0, "");
@@ -887,13 +951,16 @@ int libgrpp_b200_grpp_gradient_contract(const libgrpp_b200_batch_t *b, int radia
             const double *A = b->shell_origin + 3 * a, *B = b->shell_origin + 3 * bb, *C = b->centre_origin + 3 * c;
             const int atoms[3] = {shell_atom[a], shell_atom[bb], centre_atom[c]};
             const double *o = out24.data() + (t - t0) * 24;
+            const double wt = task_weight ? task_weight[t] : 1.0;
+            const int nm = arep_only ? 1 : 4;
             for (int q = 0; q < 3; q++) {
                 const int at = atoms[q];
                 if ((q > 0 && atoms[0] == at) || (q > 1 && atoms[1] == at)) continue;
                 for (const GradContribution &tcn : gradient_terms(A, B, C, atom_xyz + 3 * at)) {
                     const int side = tcn.diff_bra ? 0 : 1;
                     for (int k = 0; k < 3; k++)
-                        for (int m = 0; m < 4; m++) g[((size_t)m * n_atoms + at) * 3 + k] += tcn.factor * o[side * 12 + k * 4 + m];
+                        for (int m = 0; m < nm; m++)
+                            g[((size_t)m * n_atoms + at) * 3 + k] += wt * (tcn.factor * o[side * 12 + k * 4 + m]);
                 }
             }
         }
@@ -1038,26 +1105,35 @@ void libgrpp_nuclear_attraction_integrals_point_charge(libgrpp_shell_t *A, libgr
 {
     libgrpp_nuclear_attraction_integrals(A, B, C, charge, LIBGRPP_NUCLEAR_MODEL_POINT_CHARGE, nullptr, m);
 }
+// The model-specific wrappers pass libgrpp_nuclear_attraction_integrals the array
+// {charge, model parameters...}, which the generic function reads from its first element on
+// (nuclear_attraction.c:125-170, 193-236): in libgrpp these wrappers therefore evaluate the
+// model with the charge as its first parameter (R_rms, or c) and the remaining parameters
+// shifted by one. The same array is passed here, so the wrappers return libgrpp's values;
+// libgrpp_nuclear_attraction_integrals with model_params = {R_rms} / {c, a} / {c, a, k} is the
+// form that evaluates the model with the given parameters.
 void libgrpp_nuclear_attraction_integrals_charged_ball(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, int charge,
                                                        double r_rms, double *m)
 {
-    libgrpp_nuclear_attraction_integrals(A, B, C, charge, LIBGRPP_NUCLEAR_MODEL_CHARGED_BALL, &r_rms, m);
+    double p[10] = {(double)charge, r_rms};
+    libgrpp_nuclear_attraction_integrals(A, B, C, charge, LIBGRPP_NUCLEAR_MODEL_CHARGED_BALL, p, m);
 }
 void libgrpp_nuclear_attraction_integrals_gaussian_model(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, int charge,
                                                          double r_rms, double *m)
 {
-    libgrpp_nuclear_attraction_integrals(A, B, C, charge, LIBGRPP_NUCLEAR_MODEL_GAUSSIAN, &r_rms, m);
+    double p[10] = {(double)charge, r_rms};
+    libgrpp_nuclear_attraction_integrals(A, B, C, charge, LIBGRPP_NUCLEAR_MODEL_GAUSSIAN, p, m);
 }
 void libgrpp_nuclear_attraction_integrals_fermi_model(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, int charge,
                                                       double fermi_param_c, double fermi_param_a, double *m)
 {
-    double p[2] = {fermi_param_c, fermi_param_a};
+    double p[10] = {(double)charge, fermi_param_c, fermi_param_a};
     libgrpp_nuclear_attraction_integrals(A, B, C, charge, LIBGRPP_NUCLEAR_MODEL_FERMI, p, m);
 }
 void libgrpp_nuclear_attraction_integrals_fermi_bubble_model(libgrpp_shell_t *A, libgrpp_shell_t *B, double *C, int charge,
                                                              double param_c, double param_a, double param_k, double *m)
 {
-    double p[3] = {param_c, param_a, param_k};
+    double p[10] = {(double)charge, param_c, param_a, param_k};
     libgrpp_nuclear_attraction_integrals(A, B, C, charge, LIBGRPP_NUCLEAR_MODEL_FERMI_BUBBLE, p, m);
 }
 

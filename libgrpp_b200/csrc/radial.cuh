@@ -218,8 +218,10 @@ __device__ __forceinline__ double ipow(double x, int n)
     return r;
 }
 
-// M_a(x) and M_b(x) with (a, b) = (1, 0) if l = 0, else (l-1, l) (screening.c:329-346):
-// the numerator and denominator of the ratio the fixed-point step uses
+// M_a(x) and M_b(x) with (a, b) = (1, 0) if l = 0, else (l-1, l) (screening.c:329-346), up to
+// a common factor: the numerator and denominator of the ratio the fixed-point step uses.
+// Above x = 16 both are the asymptotic series sum_k c_k (-1/x)^k / (2x); the 1/(2x) factor
+// cancels in the ratio and is left out, so one reciprocal of x serves both.
 __device__ __forceinline__ void scr_ratio_parts(int l, double x, double &num, double &den)
 {
     const int na = l == 0 ? 1 : l - 1, nb = l == 0 ? 0 : l;
@@ -233,9 +235,32 @@ __device__ __forceinline__ void scr_ratio_parts(int l, double x, double &num, do
         num = taylor4(row + 5 * na, dx);
         den = taylor4(row + 5 * nb, dx);
     } else {
-        num = bessel_asym(na, x);
-        den = bessel_asym(nb, x);
+        const double ninv = -1.0 / x;
+        const double *ca = c_tab.rfun + na * kRfunL, *cb = c_tab.rfun + nb * kRfunL;
+        double pw = 1.0, sa = 0.0, sb = 0.0;
+        const int kmax = na > nb ? na : nb;
+        for (int k = 0; k <= kmax; k++) {
+            if (k <= na) sa += __ldg(ca + k) * pw;
+            if (k <= nb) sb += __ldg(cb + k) * pw;
+            pw *= ninv;
+        }
+        num = sa;
+        den = sb;
     }
+}
+
+// M_l(x) with one reciprocal of x in the asymptotic range (bessel_scaled divides twice there)
+__device__ __forceinline__ double bessel_scaled_1r(int n, double x)
+{
+    if (x <= 16.0) return bessel_scaled(n, x);
+    const double inv = 1.0 / x, ninv = -inv;
+    const double *c = c_tab.rfun + n * kRfunL;
+    double pw = 1.0, sum = 0.0;
+    for (int k = 0; k <= n; k++) {
+        sum += __ldg(c + k) * pw;
+        pw *= ninv;
+    }
+    return sum * (0.5 * inv);
 }
 
 // Primitive screening estimate (screening.c:243-318) with CA, CB as distances.
@@ -298,7 +323,7 @@ __device__ __forceinline__ bool scr_prim_flat(int l1, int l2, int n, double CA, 
     }
     const double z2 = p * r0 * r0;
     const double erf_part = z2 > 49.0 ? 2.0 : 1 + erf(sqrt(p) * r0);
-    *val = sqrt(kPi * inv_p) * ipow(r0, n) * bessel_scaled(l1, k1 * r0) * bessel_scaled(l2, k2 * r0) * ex * 0.5 *
+    *val = sqrt(kPi * inv_p) * ipow(r0, n) * bessel_scaled_1r(l1, k1 * r0) * bessel_scaled_1r(l2, k2 * r0) * ex * 0.5 *
            erf_part;
     return false;
 }

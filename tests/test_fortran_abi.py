@@ -104,6 +104,10 @@ def test_f90_entry_points_match_reference(gpu_lib, ref_lib):
                  ("libgrpp_momentum_integrals_", lambda a: a.shell(si) + a.shell(sj), 3),
                  ("libgrpp_nuclear_attraction_integrals_point_charge_",
                   lambda a: a.shell(si) + a.shell(sj) + [a.d(C), a.i(55)], 1),
+                 ("libgrpp_nuclear_attraction_integrals_charged_ball_",
+                  lambda a: a.shell(si) + a.shell(sj) + [a.d(C), a.i(55), a.d(1.3e-4)], 1),
+                 ("libgrpp_nuclear_attraction_integrals_",
+                  lambda a: a.shell(si) + a.shell(sj) + [a.d(C), a.i(55), a.i(3), a.d([1.1e-4, 1.0e-5, 0.0])], 1),
                  ("libgrpp_nuclear_attraction_integrals_gaussian_model_",
                   lambda a: a.shell(si) + a.shell(sj) + [a.d(C), a.i(55), a.d(1.3e-4)], 1),
                  ("libgrpp_nuclear_attraction_integrals_fermi_model_",

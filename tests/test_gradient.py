@@ -33,6 +33,25 @@ def test_gradient_contract_matches_oracle(gpu_lib, mode):
     assert ok, rep
 
 
+def test_symmetric_density_folding(gpu_lib):
+    """libgrpp_b200_grpp_gradient_contract_symmetric: shell pairs folded onto A <= B and no
+    spin-orbit work. The arep gradient equals the unfolded one (and the truth where the oracle
+    keeps few digits), the spin-orbit gradient is the exact zero the unfolded one approximates."""
+    batch, z = load_fixture("config3")
+    S = system_from_fixture(z)
+    truth = load_truth("config3")
+    full = gpu_lib.grad_contract(S, batch, z["D"])
+    sym = gpu_lib.grad_contract(S, batch, z["D"], symmetric=True)
+    tr = {"truth_grad": truth["truth_grad"][0].ravel(), "refdev_grad": truth["refdev_grad"][0].ravel()}
+    ok, rep = truth_parity(sym[0].ravel(), z["ref_grad"][0].ravel(), tr, np.arange(sym[0].size), "grad")
+    assert ok, rep
+    assert np.all(sym[1:] == 0.0)
+    scale = np.abs(full[0]).max()
+    assert np.all(np.abs(full[1:]) <= 1e-10 * scale)  # the unfolded SO contractions are rounding noise
+    print(f"folded vs unfolded arep gradient: max abs {np.abs(sym[0] - full[0]).max():.2e} (max |g| {scale:.2e}); "
+          f"unfolded SO max {np.abs(full[1:]).max():.2e}")
+
+
 def _small_system(shift=None):
     """Two heavy atoms with the full GRPP (U_L, projectors l <= 2, SO l <= 2, outercore
     s,p) and one H; shells s..d of 4 primitives with exponents in [0.3, 8]."""
