@@ -7,7 +7,8 @@ import numpy as np
 import pytest
 
 from libgrpp_b200 import synthetic
-from tests.util import COMPS, fixture_subset, load_fixture, load_truth, truth_parity, truth_selection
+from tests.util import (COMPS, assemble_lower, fixture_subset, full_system, load_fixture, load_truth, truth_parity,
+                        truth_selection)
 
 SUBSET = {"config1": 96, "config1_moderate": 96, "config2": 24}  # tasks of the synthetic fixtures checked on the CPU
 
@@ -39,6 +40,20 @@ def test_oracle_matches_golden(oracle_lib, name):
     for m, comp in enumerate(COMPS):
         ok, rep = truth_parity(outs[m], z["ref_" + comp])
         assert ok, (name, comp, rep)
+
+
+def test_oracle_full_kcs_matrices_against_shipped(oracle_lib):
+    """The full KCs AREP and SO matrices (54 basis shells, 2 centres, outercore terms) from the
+    oracle against libgrpp's shipped matrices (test/KCs/*.txt); the one element where libgrpp's
+    C path and its shipped Fortran-driver matrix disagree is judged against its binary128 value."""
+    batch, z = full_system("kcs")
+    got = assemble_lower(batch, oracle_lib.driver_full_batch(batch, nthreads=8), int(z["n_shells"]))
+    sel = z["truth_idx"]
+    assert len(sel) == 1
+    truth = {k: z[k] for k in z.files if k.startswith(("truth_", "refdev_"))}
+    for comp, g in zip(COMPS, got):
+        ok, rep = truth_parity(g, z["shipped_" + comp], truth, sel, comp)
+        assert ok, (comp, rep)
 
 
 def test_oracle_h2o_gradient_entry(oracle_lib):

@@ -242,6 +242,39 @@ def truth_parity(got, ref, truth=None, tr_sel=None, comp="arep"):
     return bool(np.all(ok)), rep
 
 
+def full_system(name):
+    """A full-matrix fixture (tests/golden/full_<name>.npz) and its batch of every ordered pair
+    of basis shells x every centre, in the C driver's order (test_libgrpp_c/eval_integrals.c)."""
+    from libgrpp_b200.system import BatchArrays
+    z = np.load(os.path.join(GOLDEN, f"full_{name}.npz"))
+    arr = {k[2:]: np.ascontiguousarray(z[k]) for k in z.files if k.startswith("b_")}
+    ns, nc = int(z["n_shells"]), len(arr["centre_grpp"])
+    a, b, c = np.meshgrid(np.arange(ns), np.arange(ns), np.arange(nc), indexing="ij")
+    arr["task_a"], arr["task_b"], arr["task_c"] = [np.ascontiguousarray(x.ravel(), dtype=np.int32) for x in (a, b, c)]
+    return BatchArrays(**arr), z
+
+
+def assemble_lower(batch, outs, n_shells):
+    """Sum the task blocks of ``outs`` (one array per component, blocks row-major in task order)
+    into the dense matrices over the first n_shells shells, as libgrpp's drivers accumulate them,
+    and return each matrix's lower triangle (np.tril_indices order)."""
+    from libgrpp_b200.system import ncart
+    L = batch.shell_L[:n_shells]
+    off = np.zeros(n_shells + 1, dtype=np.int64)
+    off[1:] = np.cumsum([ncart(int(x)) for x in L])
+    n = int(off[-1])
+    sz = np.array([ncart(int(x)) for x in L], dtype=np.int64)
+    ta, tb = batch.task_a.astype(np.int64), batch.task_b.astype(np.int64)
+    rows, cols = [], []
+    for t in range(len(ta)):  # element (i, j) of task t's block sits at row off[a] + i, column off[b] + j
+        na, nb = sz[ta[t]], sz[tb[t]]
+        rows.append(np.repeat(off[ta[t]] + np.arange(na), nb))
+        cols.append(np.tile(off[tb[t]] + np.arange(nb), na))
+    flat = np.concatenate(rows) * n + np.concatenate(cols)
+    tri = np.tril_indices(n)
+    return [np.bincount(flat, weights=np.asarray(o, dtype=np.float64), minlength=n * n).reshape(n, n)[tri] for o in outs]
+
+
 def truth_selection(batch, truth):
     """Element indices (into a fixture's output arrays) of the tasks a truth fixture covers, in
     the truth arrays' order."""
