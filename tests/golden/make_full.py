@@ -14,11 +14,14 @@ dense lower triangles. These are the matrices libgrpp's own ctest compares its o
 libgrpp compiled here (oracle/_ref, the C driver's full-GRPP calls) reproduces the shipped
 ThO and UO2 matrices to 1e-13. The shipped KCs matrices come from libgrpp's Fortran driver
 (test/KCs/run_test.sh), which sums type 1, type 2 per L and outercore terms from separate
-calls, each with its own radial-grid convergence; five of its arep elements sit 1.7e-10 to
-2.1e-10 from the C path. For every element where the C path and the shipped matrix differ
-beyond the tolerance of record, the fixture holds the binary128 value (oracle/truth_quad.c,
-summed over the element's tasks) as truth_<comp>[truth_idx], and refdev_<comp> = the larger
-of the two libgrpp paths' distances from it.
+calls; one of its arep elements sits 2.1e-10 from the C path. On some elements libgrpp
+keeps few digits: i-shell pairs on Th with the O potential 3.7 bohr away carry errors up
+to 8e-7 against the exact value in libgrpp's own result, from cancellation in the binomial
+re-centring sum. Those elements are found by running libgrpp on the inputs and on thirty
+copies moved by a few units in the last place; for each element where a run lands more than
+an eighth of the tolerance from the shipped value, the fixture holds the binary128 value
+(oracle/truth_quad.c, summed over the element's tasks) as truth_<comp>[truth_idx], and
+refdev_<comp>, the largest distance from it of the shipped value and of the 31 runs.
 """
 from __future__ import annotations
 
@@ -33,8 +36,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from libgrpp_b200.formats import read_lower_triangle, read_system  # noqa: E402
-from tests.util import (assemble_lower, full_system, load_ref, strict_tol,  # noqa: E402
-                        truth_full_batch)
+from tests.util import (REFDEV_MODES, assemble_lower, full_system, load_ref, perturbed,  # noqa: E402
+                        strict_tol, truth_full_batch)
 
 COMPS = ("arep", "so_x", "so_y", "so_z")
 
@@ -63,18 +66,27 @@ def main():
 
 
 def add_truth(path, n):
-    """Truth for the elements where libgrpp's C path and the shipped matrix disagree."""
+    """Truth for the elements on which libgrpp keeps few digits: those where libgrpp's C path,
+    run on the inputs and on thirty copies moved by a few units in the last place
+    (tests.util.perturbed, REFDEV_MODES), lands more than an eighth of the tolerance from the
+    shipped value."""
     name = os.path.basename(path)[5:-4]
     batch, z = full_system(name)
     ns = int(z["n_shells"])
-    ref = assemble_lower(batch, load_ref().driver_full_batch(batch, nthreads=os.cpu_count()), ns)
-    bad = np.zeros(len(ref[0]), dtype=bool)
-    for c, r in zip(COMPS, ref):
-        d = np.abs(r - z["shipped_" + c])
-        bad |= d > strict_tol(z["shipped_" + c])
-        print(f"  {name} {c}: libgrpp C path vs shipped max abs {d.max():.2e}, beyond tolerance {int(np.sum(d > strict_tol(z['shipped_' + c])))}")
+    lib = load_ref()
+    nt = os.cpu_count()
+    runs = [assemble_lower(batch, lib.driver_full_batch(batch, nthreads=nt), ns)]
+    for mode in REFDEV_MODES:
+        runs.append(assemble_lower(batch, lib.driver_full_batch(perturbed(batch, mode), nthreads=nt), ns))
+    sens = np.zeros(len(runs[0][0]), dtype=bool)
+    for m, c in enumerate(COMPS):
+        tol = strict_tol(z["shipped_" + c])
+        d = np.abs(runs[0][m] - z["shipped_" + c])
+        print(f"  {name} {c}: libgrpp C path vs shipped max abs {d.max():.2e}, beyond tolerance {int(np.sum(d > tol))}")
+        for r in runs:
+            sens |= np.abs(r[m] - z["shipped_" + c]) > tol / 8
     data = dict(z)
-    idx = np.flatnonzero(bad)
+    idx = np.flatnonzero(sens)
     data["truth_idx"] = idx.astype(np.int64)
     if len(idx):
         from libgrpp_b200.system import ncart
@@ -87,17 +99,17 @@ def add_truth(path, n):
         tb = np.array([b for a, b in pairs for _ in range(nc)], dtype=np.int32)
         tc = np.array([c for _ in pairs for c in range(nc)], dtype=np.int32)
         sub = batch.with_tasks(ta, tb, tc)
-        truth, lev, res = truth_full_batch(sub, nthreads=os.cpu_count())
-        print(f"  {name}: truth for {len(idx)} elements from {len(ta)} tasks, deepest level {lev.max()}, "
-              f"worst residual {res.max():.1e}")
+        truth, lev, res = truth_full_batch(sub, nthreads=nt)
+        print(f"  {name}: truth for {len(idx)} elements of {len(pairs)} shell pairs ({len(ta)} tasks), deepest "
+              f"level {lev.max()}, worst residual {res.max():.1e}")
         tl = assemble_lower(sub, truth, ns)
-        for c, r, t in zip(COMPS, ref, tl):
-            data["truth_" + c] = t[idx]
-            data["refdev_" + c] = np.maximum(np.abs(z["shipped_" + c][idx] - t[idx]), np.abs(r[idx] - t[idx]))
-            print(f"  {name} {c}: shipped - truth max {np.abs(z['shipped_' + c][idx] - t[idx]).max():.2e}, "
-                  f"C path - truth max {np.abs(r[idx] - t[idx]).max():.2e}")
+        for m, c in enumerate(COMPS):
+            t = tl[m][idx]
+            data["truth_" + c] = t
+            data["refdev_" + c] = np.max([np.abs(z["shipped_" + c][idx] - t)] + [np.abs(r[m][idx] - t) for r in runs], axis=0)
+            print(f"  {name} {c}: shipped - truth max {np.abs(z['shipped_' + c][idx] - t).max():.2e}, "
+                  f"max refdev {data['refdev_' + c].max():.2e}")
     np.savez_compressed(path, **data)
-
 
 if __name__ == "__main__":
     main()

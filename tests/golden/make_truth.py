@@ -19,9 +19,9 @@ Per fixture, written to tests/golden/truth_<name>.npz:
                      with an element whose reference spread env exceeds 1/8 of the
                      strict tolerance max(1e-10, 1e-9 |ref|)
   truth_<comp>       binary128 blocks of those tasks, rounded to double
-  refdev_<comp>      max over the reference run and its ten perturbed re-runs
-                     (tests/util.py ENV_MODES) of |ref_p - truth|: how far libgrpp
-                     itself lands from the exact value
+  refdev_<comp>      max over the reference run and its thirty perturbed re-runs
+                     (tests/util.py REFDEV_MODES) of |ref_p - truth|: how far
+                     libgrpp itself lands from the exact value
   truthdev_<comp>    max over two perturbed inputs (modes 3, 4) of
                      |truth_p - truth|: the exact value's own sensitivity to the
                      same input changes (small: the loss of digits is in the
@@ -51,7 +51,7 @@ sys.path.insert(0, ROOT)
 
 from libgrpp_b200.gradient import derivative_batch, gradient_terms  # noqa: E402
 from libgrpp_b200.system import cartesian_list, ncart  # noqa: E402
-from tests.util import (COMPS, ENV_MODES, fixture_subset, load_fixture, load_oracle, load_ref,  # noqa: E402
+from tests.util import (COMPS, ENV_MODES, REFDEV_MODES, fixture_subset, load_fixture, load_oracle, load_ref,  # noqa: E402
                         perturbed, strict_tol, system_from_fixture, truth_full_batch)
 
 U = 2.0 ** -53
@@ -66,25 +66,36 @@ def flagged_tasks(batch, z):
     return sorted(flag)
 
 
-def make_blocks(name, ref_lib, nthreads):
+def make_blocks(name, ref_lib, nthreads, refdev_only=False):
+    """Truth of the flagged tasks of a fixture; with refdev_only, the truth already on disk is
+    kept and only libgrpp's distances from it are recomputed."""
     batch, z = load_fixture(name)
-    idx = flagged_tasks(batch, z)
-    sub, _, _ = fixture_subset(batch, z, idx)
-    t = time.time()
-    truth, level, resid = truth_full_batch(sub, nthreads=nthreads)
-    print(f"{name}: {len(idx)} tasks, truth in {time.time() - t:.0f} s, deepest level {level.max()}, "
-          f"worst residual {resid.max():.1e}")
+    out = os.path.join(HERE, f"truth_{name}.npz")
+    if refdev_only:
+        old = np.load(out)
+        idx = [int(t) for t in old["tasks"]]
+        sub, _, _ = fixture_subset(batch, z, idx)
+        truth = [old["truth_" + c] for c in COMPS]
+        level, resid = old["level"], old["resid"]
+        truthdev = [old["truthdev_" + c] for c in COMPS]
+    else:
+        idx = flagged_tasks(batch, z)
+        sub, _, _ = fixture_subset(batch, z, idx)
+        t = time.time()
+        truth, level, resid = truth_full_batch(sub, nthreads=nthreads)
+        print(f"{name}: {len(idx)} tasks, truth in {time.time() - t:.0f} s, deepest level {level.max()}, "
+              f"worst residual {resid.max():.1e}")
+        truthdev = [np.zeros_like(x) for x in truth]
+        for mode in (3, 4):
+            tp, _, _ = truth_full_batch(perturbed(sub, mode), nthreads=nthreads)
+            for m in range(4):
+                truthdev[m] = np.maximum(truthdev[m], np.abs(tp[m] - truth[m]))
     base = ref_lib.driver_full_batch(sub, nthreads=nthreads)
     refdev = [np.abs(base[m] - truth[m]) for m in range(4)]
-    for mode in ENV_MODES:
+    for mode in REFDEV_MODES:
         p = ref_lib.driver_full_batch(perturbed(sub, mode), nthreads=nthreads)
         for m in range(4):
             refdev[m] = np.maximum(refdev[m], np.abs(p[m] - truth[m]))
-    truthdev = [np.zeros_like(x) for x in truth]
-    for mode in (3, 4):
-        tp, _, _ = truth_full_batch(perturbed(sub, mode), nthreads=nthreads)
-        for m in range(4):
-            truthdev[m] = np.maximum(truthdev[m], np.abs(tp[m] - truth[m]))
     data = dict(tasks=np.array(idx, dtype=np.int32), level=level, resid=resid)
     for m, c in enumerate(COMPS):
         data["truth_" + c] = truth[m]
@@ -93,7 +104,6 @@ def make_blocks(name, ref_lib, nthreads):
         e = np.abs(base[m] - truth[m])
         print(f"  {c}: max |ref - truth| {e.max():.2e} ({int(np.sum(e > strict_tol(truth[m])))} elements beyond "
               f"1e-10/1e-9), max refdev {refdev[m].max():.2e}, max truthdev {truthdev[m].max():.2e}")
-    out = os.path.join(HERE, f"truth_{name}.npz")
     np.savez_compressed(out, **data)
     print(f"  -> {os.path.relpath(out, ROOT)} ({os.path.getsize(out) / 1e3:.0f} kB)")
 
@@ -145,18 +155,23 @@ def truth_gradient(system, batch, D, nthreads):
     return g, level, resid
 
 
-def make_gradient(nthreads):
+def make_gradient(nthreads, refdev_only=False):
     batch, z = load_fixture("config3")
     S = system_from_fixture(z)
     D = z["D"]
-    t = time.time()
-    g, level, resid = truth_gradient(S, batch, D, nthreads)
-    print(f"config3: truth gradient of {len(batch.task_a)} tasks in {time.time() - t:.0f} s, deepest level "
-          f"{level.max()}, worst residual {resid.max():.1e}")
+    out = os.path.join(HERE, "truth_config3.npz")
+    if refdev_only:
+        old = np.load(out)
+        g, level, resid = old["truth_grad"], old["level"], old["resid"]
+    else:
+        t = time.time()
+        g, level, resid = truth_gradient(S, batch, D, nthreads)
+        print(f"config3: truth gradient of {len(batch.task_a)} tasks in {time.time() - t:.0f} s, deepest level "
+              f"{level.max()}, worst residual {resid.max():.1e}")
     import copy
     orc = load_oracle()
     refdev = np.abs(orc.driver_grad_contract(S, batch, D, nthreads=nthreads) - g)
-    for mode in ENV_MODES:
+    for mode in REFDEV_MODES:
         sp = copy.copy(S)
         if mode == 2:
             sp.atoms = np.asarray(S.atoms) * (1 + 4 * U)
@@ -164,7 +179,6 @@ def make_gradient(nthreads):
     e = np.abs(z["ref_grad"] - g)
     print(f"  max |oracle - truth| {e.max():.2e} ({int(np.sum(e > strict_tol(g)))} elements beyond 1e-10/1e-9), "
           f"max refdev {refdev.max():.2e}, max |g| {np.abs(g).max():.2e}")
-    out = os.path.join(HERE, "truth_config3.npz")
     np.savez_compressed(out, truth_grad=g, refdev_grad=refdev, level=level, resid=resid)
     print(f"  -> {os.path.relpath(out, ROOT)} ({os.path.getsize(out) / 1e3:.0f} kB)")
 
@@ -173,15 +187,16 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*")
     ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--refdev-only", action="store_true", help="keep the truth on disk, recompute libgrpp's distances")
     args = ap.parse_args()
     ref = load_ref()
     if ref is None:
         raise SystemExit("oracle/_ref/libgrpp_ref.so is not built (make -C oracle ref)")
     for name in ("config1", "config1_moderate", "config2"):
         if not args.only or name in args.only:
-            make_blocks(name, ref, args.threads)
+            make_blocks(name, ref, args.threads, args.refdev_only)
     if not args.only or "config3" in args.only:
-        make_gradient(args.threads)
+        make_gradient(args.threads, args.refdev_only)
 
 
 if __name__ == "__main__":

@@ -8,7 +8,7 @@ no significant digits (tight high-l primitives, far potential centres): its
 result moves by up to the size of the values when its inputs move by a few
 units in the last place, while the exact value does not. For the tasks of those
 blocks tests/golden/truth_<name>.npz holds the exact values (binary128,
-oracle/truth_quad.c) and libgrpp's own distance from them over eleven runs
+oracle/truth_quad.c) and libgrpp's own distance from them over 31 runs
 (refdev); an element there that misses the strict bound must satisfy
     |gpu - truth| <= max(1e-10, 1e-9 |truth|, 2 refdev).
 Each test prints how many elements were judged against the truth.
