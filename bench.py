@@ -292,6 +292,38 @@ def count_type1(plans, cnt, scale=1.0):
             cnt[k] += mc[k] * scale
 
 
+def autotune_leg(lib, batches, mode, flush, local):
+    """Per-class block size of the assembly kernel: one pass over the batches with 128 threads
+    for every task (fixed), with the default rule, and with the autotuner's table (built on the
+    same batches beforehand, its time reported); the table stays in force afterwards."""
+    import torch
+    res = {}
+
+    def one_pass(threads):
+        plans = [lib.plan(b, mode, assembly_threads=threads) for b in batches]
+        plans[0].execute()
+        torch.cuda.synchronize()
+        tot, kms, _, _, _ = time_plans(plans, flush, local)
+        for p in plans:
+            p.close()
+        return {"ms_per_step": tot, "ms_assembly": kms["ms_assembly"]}
+
+    lib.autotune_reset()
+    res["fixed_128"] = one_pass(128)
+    res["default_rule"] = one_pass(0)
+    t0 = time.perf_counter()
+    table = {}
+    for b in batches:
+        table.update(lib.autotune_assembly(b, mode))
+    res["tuning_seconds"] = time.perf_counter() - t0
+    res["autotuned"] = one_pass(0)
+    res["classes"] = len(table)
+    res["choices"] = {str(s): sum(1 for v in table.values() if v[4] == s) for s in (128, 256, 512)}
+    res["autotuned_over_fixed"] = res["fixed_128"]["ms_per_step"] / res["autotuned"]["ms_per_step"]
+    res["assembly_autotuned_over_fixed"] = res["fixed_128"]["ms_assembly"] / res["autotuned"]["ms_assembly"]
+    return res
+
+
 def run_ours(args, rank, world, local):
     import torch
     from libgrpp_b200 import engine
@@ -318,6 +350,9 @@ def run_ours(args, rank, world, local):
         batches.append(S.batch(a, b, c))
     n_tasks = [len(b.task_a) for b in batches]
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    # the assembly kernel's block size per class: autotuned on this rank's batches (untimed
+    # setup, like building the plans); fixed-size and default-rule passes are reported beside it
+    tune = autotune_leg(lib, batches, {"plain": 0, "learned": 1}[args.mode], flush, local) if not args.no_autotune else None
     res = {}
     for name in ("plain", args.mode) if args.mode == "learned" else ("plain",):
         plans = [lib.plan(b, modes[name]) for b in batches]
@@ -369,6 +404,8 @@ def run_ours(args, rank, world, local):
                 "d2h_bytes_per_step": d2h},
         "clocks": R["clocks"],
     }
+    if tune is not None:
+        line["autotune"] = tune
     if main_mode == "learned":
         P = res["plain"]
         line["plain"] = {"value": P["value"], "ms_per_step": P["ms_per_step"],
@@ -464,6 +501,7 @@ def config4_leg(args, lib, local, flush, steps):
     M, a, b, c = config4_tasks(args.molecules)
     chunks = [M.batch(a[i:i + 65536], b[i:i + 65536], c[i:i + 65536]) for i in range(0, len(a), 65536)]
     res, outs = {}, {}
+    tune = autotune_leg(lib, chunks, 1, flush, local) if not args.no_autotune else None
     peak = lib.fp64_peak()
     for name, mode in (("plain", 0), ("learned", 1)):
         plans = [lib.plan(ch, mode) for ch in chunks]
@@ -492,6 +530,8 @@ def config4_leg(args, lib, local, flush, steps):
            "plain": res["plain"], "learned_over_plain": res["learned"]["value"] / res["plain"]["value"],
            "learned_fallback_rate": res["learned"]["fallbacks_per_step"] / len(a),
            "max_abs_diff_learned_vs_plain": max_err}
+    if tune is not None:
+        out["autotune"] = tune
     return out, (M, a, b, c)
 
 
@@ -612,6 +652,7 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=256, help="config3 CPU baseline: sampled tasks")
     ap.add_argument("--ref-per-class", type=int, default=6,
                     help="CPU baseline: seeded tasks per (la, lb, lpot) class of the stratified sample")
+    ap.add_argument("--no-autotune", action="store_true", help="skip the assembly autotuner (default rule only)")
     ap.add_argument("--no-extra", action="store_true", help="leave the config3 / config4 legs out of the default line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tasks-per-step", type=int, default=0,

@@ -121,6 +121,24 @@ int libgrpp_b200_fp64_peak(double *tflops);
 typedef struct libgrpp_b200_plan libgrpp_b200_plan_t;
 
 libgrpp_b200_plan_t *libgrpp_b200_plan_create(const libgrpp_b200_batch_t *batch, int radial_mode);
+
+/* plan_create with a fixed block size of the assembly kernel for every task (128, 256 or
+ * 512 threads); 0 uses the autotuner's per-class table, or the default rule where the table
+ * has no entry for a class. */
+libgrpp_b200_plan_t *libgrpp_b200_plan_create_ex(const libgrpp_b200_batch_t *batch, int radial_mode,
+                                                 int assembly_threads);
+
+/* Per-class autotuner of the assembly kernel (no counterpart in libgrpp). A class is
+ * (la, lb, largest semilocal L of the centre's GRPP, spin-orbit terms or not). Every class
+ * of `batch` runs as a launch of its own with 128, 256 and 512 threads per block, timed
+ * with CUDA events; the fastest size per class is kept for the later batches and plans of
+ * this device. Writes up to `cap` rows of 6 doubles: class key ((la*16+lb)*16+L)*2+so,
+ * tasks, milliseconds at 128, 256, 512 threads, chosen size. Returns the number of classes
+ * or a negative status code. */
+int libgrpp_b200_autotune_assembly(const libgrpp_b200_batch_t *batch, int radial_mode, double *rows, int cap);
+
+/* Forget the autotuner's table of the current device (the default rule applies again). */
+void libgrpp_b200_autotune_reset(void);
 int libgrpp_b200_plan_execute(libgrpp_b200_plan_t *plan);
 int libgrpp_b200_plan_outputs(libgrpp_b200_plan_t *plan, double *arep, double *so_x, double *so_y, double *so_z);
 /* ms[5] = kernel time of the last execute(): total, type 1, radial (screening + grid walk),

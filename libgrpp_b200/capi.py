@@ -87,6 +87,9 @@ class LibGRPP:
         self._opt("libgrpp_b200_fp64_peak", ct.c_int, [_D])
         self._opt("libgrpp_b200_type2_batch_noalloc", ct.c_int, [_V, _D])
         self._opt("libgrpp_b200_plan_create", _V, [_V, ct.c_int])
+        self._opt("libgrpp_b200_plan_create_ex", _V, [_V, ct.c_int, ct.c_int])
+        self._opt("libgrpp_b200_autotune_assembly", ct.c_int, [_V, ct.c_int, ct.POINTER(ct.c_double), ct.c_int])
+        self._opt("libgrpp_b200_autotune_reset", None, [])
         self._opt("libgrpp_b200_plan_execute", ct.c_int, [_V])
         self._opt("libgrpp_b200_plan_outputs", ct.c_int, [_V, _D, _D, _D, _D])
         self._opt("libgrpp_b200_plan_stats", ct.c_int, [_V, _D, ct.POINTER(ct.c_int64)])
@@ -438,10 +441,27 @@ class LibGRPP:
         if os.path.exists(level_model.MODEL_FILE):
             self.set_level_model(level_model.load()[0])
 
-    def plan(self, batch, radial_mode=0) -> "Plan":
+    def plan(self, batch, radial_mode=0, assembly_threads=0) -> "Plan":
+        """A prepared batch; assembly_threads fixes the assembly kernel's block size for every
+        task (128, 256, 512), 0 takes the autotuner's per-class table or the default rule."""
         if radial_mode == 1:
             self.ensure_level_model()
-        return Plan(self, batch, radial_mode)
+        return Plan(self, batch, radial_mode, assembly_threads)
+
+    def autotune_assembly(self, batch, radial_mode=0):
+        """Time every assembly class of the batch with 128, 256 and 512 threads per block and keep
+        the fastest per class for this device; returns {class key: (tasks, ms128, ms256, ms512, choice)}."""
+        if radial_mode == 1:
+            self.ensure_level_model()
+        cap = 4096
+        rows = np.zeros(6 * cap)
+        n = self.lib.libgrpp_b200_autotune_assembly(ct.byref(batch.struct), radial_mode, _dp(rows), cap)
+        self._check(min(n, 0), "libgrpp_b200_autotune_assembly")
+        r = rows[: 6 * min(n, cap)].reshape(-1, 6)
+        return {int(x[0]): (int(x[1]), float(x[2]), float(x[3]), float(x[4]), int(x[5])) for x in r}
+
+    def autotune_reset(self):
+        self.lib.libgrpp_b200_autotune_reset()
 
     def last_error(self) -> int:
         return int(self.lib.libgrpp_b200_last_error())
@@ -476,11 +496,11 @@ def dense_full(lib: LibGRPP, system, threads=None):
 class Plan:
     """A batch prepared on the device (libgrpp_b200_plan_*): execute() runs the kernels only."""
 
-    def __init__(self, lib: LibGRPP, batch, radial_mode=0):
+    def __init__(self, lib: LibGRPP, batch, radial_mode=0, assembly_threads=0):
         self.lib = lib
         self.batch = batch
         self.n_out = int(batch.block_offsets()[-1])
-        self.h = lib.lib.libgrpp_b200_plan_create(ct.byref(batch.struct), radial_mode)
+        self.h = lib.lib.libgrpp_b200_plan_create_ex(ct.byref(batch.struct), radial_mode, assembly_threads)
         if not self.h:
             raise RuntimeError(f"libgrpp_b200_plan_create failed: {lib.last_error_message()}")
 

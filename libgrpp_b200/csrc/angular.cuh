@@ -162,8 +162,9 @@ __global__ void oc_proj_kernel(OcProjArgs a)
 
 // ---- final per-task assembly -----------------------------------------------------
 
-constexpr int kFinThreads = 128;
-constexpr int kFinElemPerThread = 8;  // up to 1024 Cartesian pairs
+constexpr int kFinThreads = 128;       // omega tables; the assembly kernel is instantiated for 128, 256, 512
+constexpr int kFinMaxPairs = 1024;     // Cartesian pairs of one task block (i x i = 784)
+constexpr int kFinElemPerThread = kFinMaxPairs / kFinThreads;
 constexpr int kFinMaxLam = 24;
 constexpr int kLmatPairs = 100;  // (m1, m2) pairs of the L matrices with a non-zero component: 10L - 4 <= 96 for L <= 10
 constexpr int kFinMaxSl = 24;         // semilocal potentials per centre
@@ -347,8 +348,10 @@ __global__ void __launch_bounds__(kFinThreads) omega_tab_kernel(FinalArgs a, Fin
     }
 }
 
-__global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSmem sm)
+template <int NT>
+__global__ void __launch_bounds__(NT) final_kernel(FinalArgs a, FinalSmem sm)
 {
+    constexpr int EPT = kFinMaxPairs / NT;  // Cartesian pairs per thread
     extern __shared__ double dsm[];
     __shared__ double powA[3][kMaxL + 2], powB[3][kMaxL + 2];
     __shared__ double sCA[3], sCB[3];
@@ -380,9 +383,9 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
             t = s_next;
             if (t < 0) break;
         } else {
-            t = t_static;
+            if (t_static >= a.n_tasks) break;
+            t = a.order ? a.order[t_static] : t_static;
             t_static += gridDim.x;
-            if (t >= a.n_tasks) break;
         }
         const int sa = a.task_a[t], sb = a.task_b[t], c = a.task_c[t];
         const int la = a.shell_L[sa], lb = a.shell_L[sb], nA = ncart(la), nB = ncart(lb), nel = nA * nB;
@@ -399,10 +402,10 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
             for (int k = 0; k <= la; k++) powA[tid][k] = pow(sCA[tid], k);
             for (int k = 0; k <= lb; k++) powB[tid][k] = pow(sCB[tid], k);
         }
-        double acc[4][kFinElemPerThread];
+        double acc[4][EPT];
 #pragma unroll
-        for (int q = 0; q < kFinElemPerThread; q++) {
-            const int e = tid + q * kFinThreads;
+        for (int q = 0; q < EPT; q++) {
+            const int e = tid + q * NT;
             acc[0][q] = (e < nel && a.task_has_ul[t]) ? a.arep[oo + e] : 0.0;
             acc[1][q] = acc[2][q] = acc[3][q] = 0.0;
         }
@@ -424,7 +427,7 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
             // RSH values with stride rs (rsh_values uses 2*kFinMaxLam+1; use a local variant)
             const bool omt = a.omtab != nullptr;
             if (omt) {  // only the |abc| tables are needed: omega comes from the pair tables
-                for (int e = tid; e < n_abc(la) + n_abc(lb); e += kFinThreads) {
+                for (int e = tid; e < n_abc(la) + n_abc(lb); e += NT) {
                     const bool sideB = e >= n_abc(la);
                     const int l = sideB ? lb : la;
                     int idx = sideB ? e - n_abc(la) : e, aa, bb;
@@ -463,7 +466,7 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                         upow[side][d][i] = pw;
                     }
                 }
-                for (int e = tid; e < n_abc(la) + n_abc(lb); e += kFinThreads) {
+                for (int e = tid; e < n_abc(la) + n_abc(lb); e += NT) {
                     const bool sideB = e >= n_abc(la);
                     const int l = sideB ? lb : la;
                     int idx = sideB ? e - n_abc(la) : e, aa, bb;
@@ -482,7 +485,7 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                 __syncthreads();
                 // (l, mu) pairs e = l^2 + l + mu of both sides
                 const int nlm = (lam_max + 1) * (lam_max + 1);
-                for (int e = tid; e < 2 * nlm; e += kFinThreads) {
+                for (int e = tid; e < 2 * nlm; e += NT) {
                     const int side = e >= nlm, r = side ? e - nlm : e;
                     int l = (int)sqrtf((float)r);
                     while (l * l > r) l--;
@@ -529,12 +532,12 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                 __syncthreads();
                 // omega tables: omega[abc][slot][m] = sum_mu S_{lam mu} Atab (angular_integrals.c:78-108)
                 if (omt) {
-                    for (int e = tid; e < nabA * slA * nm; e += kFinThreads) omA[e] = a.omtab[omoA + e];
-                    for (int e = tid; e < nabB * slB * nm; e += kFinThreads) omB[e] = a.omtab[omoB + e];
+                    for (int e = tid; e < nabA * slA * nm; e += NT) omA[e] = a.omtab[omoA + e];
+                    for (int e = tid; e < nabB * slB * nm; e += NT) omB[e] = a.omtab[omoB + e];
                     omoA += nabA * slA * nm;
                     omoB += nabB * slB * nm;
                 }
-                for (int e = tid; !omt && e < nabA * slA * nm + nabB * slB * nm; e += kFinThreads) {
+                for (int e = tid; !omt && e < nabA * slA * nm + nabB * slB * nm; e += NT) {
                     const bool sideB = e >= nabA * slA * nm;
                     const int r = sideB ? e - nabA * slA * nm : e;
                     const int sl = sideB ? slB : slA, nab = sideB ? nabB : nabA, l = sideB ? lb : la;
@@ -555,7 +558,7 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                     }
                     (sideB ? omB : omA)[r] = w;
                 }
-                for (int e = tid; e < d1 * d2 * dn; e += kFinThreads) Qs[e] = a.Q[qbase + qoff + e];
+                for (int e = tid; e < d1 * d2 * dn; e += NT) Qs[e] = a.Q[qbase + qoff + e];
                 qoff += (int64_t)d1 * d2 * dn;
                 if (so && tid == 0) {
                     int np = 0;
@@ -579,15 +582,15 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                 const int ncomp = so ? 3 : 1;
                 const double thrF = so ? kZeroThresh : 1e-13, thrQ = so ? kZeroThresh : 1e-16, thrW = so ? kZeroThresh : 1e-16;
                 const int rows = max(1, min(nabA, sm.n_v / (nabB * ncomp)));
-                double gam[3][kFinElemPerThread];
+                double gam[3][EPT];
 #pragma unroll
-                for (int q = 0; q < kFinElemPerThread; q++) gam[0][q] = gam[1][q] = gam[2][q] = 0.0;
+                for (int q = 0; q < EPT; q++) gam[0][q] = gam[1][q] = gam[2][q] = 0.0;
 
                 for (int r0 = 0; r0 < nabA; r0 += rows) {
                     const int r1 = min(nabA, r0 + rows);
                     __syncthreads();
                     // V[abc][def] (type2_integrals.c:174-196, spin_orbit_integrals.c:197-224)
-                    for (int e = tid; e < (r1 - r0) * nabB; e += kFinThreads) {
+                    for (int e = tid; e < (r1 - r0) * nabB; e += NT) {
                         const int abc = r0 + e / nabB, def = e % nabB;
                         const int n1 = nabcA[abc], n2 = nabcB[def], N = n1 + n2;
                         double v0 = 0.0, v1 = 0.0, v2 = 0.0;
@@ -636,7 +639,7 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                     if (fact) {
                         double *W = V + sm.n_v;
                         const int nrow = r1 - r0;
-                        for (int e = tid; e < nB * nrow; e += kFinThreads) {
+                        for (int e = tid; e < nB * nrow; e += NT) {
                             const int j = e / nrow, ar = e % nrow;
                             const int bx = cB[3 * j], by = cB[3 * j + 1], bz = cB[3 * j + 2];
                             double w0 = 0.0, w1 = 0.0, w2 = 0.0;
@@ -663,8 +666,8 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                         }
                         __syncthreads();
 #pragma unroll
-                        for (int q = 0; q < kFinElemPerThread; q++) {
-                            const int el = tid + q * kFinThreads;
+                        for (int q = 0; q < EPT; q++) {
+                            const int el = tid + q * NT;
                             if (el >= nel) continue;
                             const int i = el / nB, j = el % nB;
                             const int ax = cA[3 * i], ay = cA[3 * i + 1], az = cA[3 * i + 2];
@@ -693,8 +696,8 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                     }
                     // Cartesian pairs: binomial re-centring sums over (a..f) in the reference's loop order
 #pragma unroll
-                    for (int q = 0; q < kFinElemPerThread; q++) {
-                        const int el = tid + q * kFinThreads;
+                    for (int q = 0; q < EPT; q++) {
+                        const int el = tid + q * NT;
                         if (el >= nel) continue;
                         const int i = el / nB, j = el % nB;
                         const int ax = cA[3 * i], ay = cA[3 * i + 1], az = cA[3 * i + 2];
@@ -732,7 +735,7 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
                 const double pi16 = 16 * kPi * kPi;
                 const double fso = a.raw_so ? 1.0 : 2.0 / (2 * L + 1);
 #pragma unroll
-                for (int q = 0; q < kFinElemPerThread; q++) {
+                for (int q = 0; q < EPT; q++) {
                     if (!so) {
                         acc[0][q] += 1.0 * (gam[0][q] * pi16);
                     } else {
@@ -751,8 +754,8 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
             const int ocoff = a.grpp_oc_off[g];
             const double *dl = a.oc_delta + a.grpp_delta_off[g];
 #pragma unroll
-            for (int q = 0; q < kFinElemPerThread; q++) {
-                const int el = tid + q * kFinThreads;
+            for (int q = 0; q < EPT; q++) {
+                const int el = tid + q * NT;
                 if (el >= nel) continue;
                 const int i = el / nB, j = el % nB;
                 double oa = 0.0, ox = 0.0, oy = 0.0, oz = 0.0;
@@ -845,8 +848,8 @@ __global__ void __launch_bounds__(kFinThreads) final_kernel(FinalArgs a, FinalSm
             }
         }
 #pragma unroll
-        for (int q = 0; q < kFinElemPerThread; q++) {
-            const int e = tid + q * kFinThreads;
+        for (int q = 0; q < EPT; q++) {
+            const int e = tid + q * NT;
             if (e < nel) {
                 a.arep[oo + e] = acc[0][q];
                 a.so_x[oo + e] = acc[1][q];

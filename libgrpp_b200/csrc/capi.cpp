@@ -691,6 +691,28 @@ libgrpp_b200_plan_t *libgrpp_b200_plan_create(const libgrpp_b200_batch_t *b, int
     return (libgrpp_b200_plan_t *)grpp::plan_create(b, opt);
 }
 
+libgrpp_b200_plan_t *libgrpp_b200_plan_create_ex(const libgrpp_b200_batch_t *b, int radial_mode, int assembly_threads)
+{
+    if (!check_init()) return nullptr;
+    grpp::RunOptions opt;
+    opt.radial_mode = radial_mode;
+    opt.fin_nt = assembly_threads;
+    return (libgrpp_b200_plan_t *)grpp::plan_create(b, opt);
+}
+
+int libgrpp_b200_autotune_assembly(const libgrpp_b200_batch_t *b, int radial_mode, double *rows, int cap)
+{
+    if (!check_init()) return LIBGRPP_B200_ERR_NOT_INIT;
+    std::vector<std::array<double, 6>> r;
+    const int rc = grpp::autotune_assembly(b, radial_mode, r);
+    if (rc) return rc;
+    for (int i = 0; i < (int)r.size() && i < cap; i++)
+        for (int k = 0; k < 6; k++) rows[6 * i + k] = r[i][k];
+    return (int)r.size();
+}
+
+void libgrpp_b200_autotune_reset(void) { grpp::autotune_reset(); }
+
 int libgrpp_b200_plan_execute(libgrpp_b200_plan_t *plan)
 {
     if (!plan) {

@@ -16,6 +16,7 @@
 // mmd_kernel and final_kernel run persistent grids that pop work from a queue ordered by
 // estimated work, largest first; the walk does the same in learned mode.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -36,7 +37,7 @@
 
 namespace grpp {
 
-constexpr size_t kFinSmemMax = 200 * 1024;  // dynamic shared memory of the assembly kernel
+constexpr size_t kFinSmemMax = 220 * 1024;  // dynamic shared memory of the assembly kernel (+ its static 3 kB)
 
 // ------------------------------------------------------------------ errors
 namespace {
@@ -124,6 +125,8 @@ struct DeviceState {
     std::vector<int64_t> atab_off;
     bool atab_dirty = true;  // atab_off has entries the device copy lacks
     DevBuf atab_off_dev;
+    std::vector<cudaEvent_t> gev[2];     // per buffer set: boundaries of the assembly launches (autotuning)
+    std::map<int, int> fin_tune;         // assembly class -> block size picked by the autotuner
     std::mutex mu;
 };
 
@@ -182,7 +185,9 @@ int init_device_state(DeviceState &st, int device)
     GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(radial_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-    GRPP_CUDA(cudaFuncSetAttribute(final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFinSmemMax));
+    GRPP_CUDA(cudaFuncSetAttribute(final_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFinSmemMax));
+    GRPP_CUDA(cudaFuncSetAttribute(final_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFinSmemMax));
+    GRPP_CUDA(cudaFuncSetAttribute(final_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFinSmemMax));
     GRPP_CUDA(cudaFuncSetAttribute(type1_num_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(t1_smem_doubles(kT1MaxLam) * sizeof(double))));
     GRPP_CUDA(cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_train_smem_bytes()));
@@ -336,6 +341,49 @@ static std::vector<int> order_by_cost(const std::vector<double> &cost)
     return out;
 }
 
+// Assembly classes and shared-memory layouts. A class is (la, lb, largest semilocal L, spin-orbit
+// terms or not); the layout holds the task's RSH rows, both sides' omega tables, its radial
+// table, the V rows of one potential (all rows when they fit in 6144 values) and W of the
+// factored re-centring sum. W holds ncart(lb) x rows x components values and rows is chosen so
+// that nabB x rows x components fits in V, so a W as large as V always suffices.
+static int fin_class_key(int la, int lb, int Lmax, bool so) { return ((la * 16 + lb) * 16 + Lmax) * 2 + (so ? 1 : 0); }
+
+static int fin_default_nt(int la, int lb)
+{
+    const int w = n_abc(la) * n_abc(lb);
+    return w < 1000 ? 128 : (w < 3000 ? 256 : 512);
+}
+
+static FinalSmem fin_layout(int lam, int n_omega, int n_q, int nabA, int nabB, int ncomp)
+{
+    FinalSmem fs{};
+    fs.rsh_stride = 2 * lam + 1;
+    fs.n_rsh = (lam + 1) * fs.rsh_stride;
+    fs.n_omega = n_omega;
+    fs.n_q = n_q;
+    fs.n_v = std::min(6144, std::max(nabA * nabB * ncomp, 3 * std::max(nabA, nabB)));
+    fs.n_v = std::max(fs.n_v, 3 * std::max(nabA, nabB));
+    fs.n_w = fs.n_v;
+    return fs;
+}
+
+static FinalSmem fin_merge(const FinalSmem &x, const FinalSmem &y)
+{
+    FinalSmem m{};
+    m.rsh_stride = std::max(x.rsh_stride, y.rsh_stride);
+    m.n_rsh = std::max(x.n_rsh, y.n_rsh);
+    m.n_omega = std::max(x.n_omega, y.n_omega);
+    m.n_q = std::max(x.n_q, y.n_q);
+    m.n_v = std::max(x.n_v, y.n_v);
+    m.n_w = std::max(x.n_w, y.n_w);
+    return m;
+}
+
+static size_t fin_smem_bytes(const FinalSmem &fs)
+{
+    return (size_t)(2 * fs.n_rsh + 2 * fs.n_omega + fs.n_q + fs.n_v + fs.n_w) * sizeof(double);
+}
+
 template <typename T>
 T *at(void *base, size_t off)
 {
@@ -461,6 +509,20 @@ int ensure_atab(DeviceState &st, int L, int l)
 
 }  // namespace
 
+// One launch of the assembly kernel: the tasks order[first .. first+count) of one block size, with
+// a shared-memory layout sized for the largest of them. Small tasks in a group of their own get
+// small layouts and many blocks per SM; the block size per assembly class comes from the
+// autotuner's table (libgrpp_b200_autotune_assembly) or the default rule.
+struct FinGroup {
+    int nt = 128;
+    int first = 0, count = 0;
+    int key = -1;  // assembly class when the groups are one per class (autotuning), else -1
+    FinalSmem fs{};
+    size_t smem = 0;
+    int blocks = 0;
+    float ms = 0.f;
+};
+
 struct Plan {
     DeviceState *st = nullptr;
     int set = 0;  // buffer set, events and status words of the device state it uses
@@ -490,9 +552,10 @@ struct Plan {
     size_t om_smem = 0;
     size_t rad_smem = 0;
     FinalArgs fin;
-    FinalSmem fin_smem_layout;
-    int fin_blocks = 0;
-    size_t fin_smem = 0;
+    FinalSmem fin_smem_layout;  // batch-wide layout (omega tables)
+    std::vector<FinGroup> fin_groups;
+    int *fin_queue = nullptr;   // one counter per group
+    bool time_groups = false;   // record an event between the assembly launches
     RunStats stats;
     bool count_ops = false;  // run the type 1 kernel's counting instantiation
 };
@@ -700,7 +763,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         const int A = ta[t], B = tb[t], C = tc[t], g = b->centre_grpp[C];
         const int la = sh_L[A], lb = sh_L[B];
         CHECK_INPUT(sh_np[A] >= 1 && sh_np[B] >= 1, "a shell of a task has no primitives");
-        CHECK_INPUT(ncart(la) * ncart(lb) <= kFinThreads * kFinElemPerThread, "shell pair block larger than 1024 Cartesian pairs");
+        CHECK_INPUT(ncart(la) * ncart(lb) <= kFinMaxPairs, "shell pair block larger than 1024 Cartesian pairs");
         out_off[t + 1] = out_off[t] + (int64_t)ncart(la) * ncart(lb);
         if (b->grpp_UL[g] >= 0 && p_n[b->grpp_UL[g]] > 0) {
             has_ul[t] = 1;
@@ -831,16 +894,68 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         mmd_order = order_by_cost(cost);
     }
 
-    // estimated work per task in the assembly: per semilocal potential, the V table and the
-    // re-centring sums of its Cartesian pairs
+    // Assembly launch groups. Per task: its class, the block size for the class (the caller's,
+    // the autotuner's table, or the default rule) and the shared memory its tables need. Tasks of
+    // one block size and one shared-memory tier form a group (one group per class when
+    // autotuning); within a group the queue takes the largest estimated work first: per
+    // semilocal potential, the V table and the re-centring sums of its Cartesian pairs.
     std::vector<int> fin_order;
+    std::vector<FinGroup> fin_groups;
     {
         std::vector<double> cost(nt);
+        std::map<int, int> gidx;
+        std::vector<std::vector<int>> members;
         for (int64_t t = 0; t < nt; t++) {
             const int la = sh_L[ta[t]], lb = sh_L[tb[t]], g = b->centre_grpp[tc[t]];
             cost[t] = 1.0 + (double)g_sl_n[g] * ((double)n_abc(la) * n_abc(lb) + 4.0 * ncart(la) * ncart(lb));
+            int lam = 0, nom = 1, nq = 1, Lmx = 0;
+            for (int i = 0; i < g_sl_n[g]; i++) {
+                const int L = p_L[sl_pot[g_sl_off[g] + i]];
+                Lmx = std::max(Lmx, L);
+                lam = std::max(lam, L + std::max(la, lb));
+                nom = std::max(nom, std::max(n_abc(la) * lam_slots(L, la), n_abc(lb) * lam_slots(L, lb)) * (2 * L + 1));
+                nq = std::max(nq, (L + la + 1) * (L + lb + 1) * (la + lb + 1));
+            }
+            const bool so = b->grpp_n_so[g] > 0;
+            const int cls = fin_class_key(la, lb, Lmx, so);
+            int ntb = opt.fin_nt;
+            if (ntb == 0) {
+                auto it = st.fin_tune.find(cls);
+                ntb = it != st.fin_tune.end() ? it->second : fin_default_nt(la, lb);
+            }
+            CHECK_INPUT(ntb == 128 || ntb == 256 || ntb == 512, "assembly block size must be 128, 256 or 512");
+            const FinalSmem fs = fin_layout(lam, nom, nq, n_abc(la), n_abc(lb), so ? 3 : 1);
+            const size_t bytes = fin_smem_bytes(fs);
+            const int tier = bytes <= 32 * 1024 ? 0 : (bytes <= 96 * 1024 ? 1 : 2);
+            const int key = opt.fin_by_class ? cls * 8 + ntb / 128 : ntb * 4 + tier;
+            auto it = gidx.find(key);
+            int gi;
+            if (it == gidx.end()) {
+                gi = (int)fin_groups.size();
+                gidx[key] = gi;
+                FinGroup G;
+                G.nt = ntb;
+                G.key = opt.fin_by_class ? cls : -1;
+                G.fs = fs;
+                fin_groups.push_back(G);
+                members.emplace_back();
+            } else {
+                gi = it->second;
+                fin_groups[gi].fs = fin_merge(fin_groups[gi].fs, fs);
+            }
+            members[gi].push_back((int)t);
         }
-        fin_order = order_by_cost(cost);
+        for (size_t gi = 0; gi < fin_groups.size(); gi++) {
+            auto &m = members[gi];
+            std::stable_sort(m.begin(), m.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+            fin_groups[gi].first = (int)fin_order.size();
+            fin_groups[gi].count = (int)m.size();
+            fin_order.insert(fin_order.end(), m.begin(), m.end());
+            FinalSmem &fs = fin_groups[gi].fs;
+            if (fin_smem_bytes(fs) > kFinSmemMax) fs.n_w = 0;  // term-by-term re-centring only
+            CHECK_INPUT(fin_smem_bytes(fs) <= kFinSmemMax, "assembly tables of this batch exceed the shared memory of one block");
+            fin_groups[gi].smem = fin_smem_bytes(fs);
+        }
     }
     std::vector<int> mmd_etab, mmd_etab_off, mmd_rtab_off;
     std::vector<int2> mmd_rtab;
@@ -1174,25 +1289,9 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         f.om_off = at<int64_t>(ib, o_omo);
         f.task_fpa = at<int>(ib, o_tfa);
         f.task_fpb = at<int>(ib, o_tfb);
-        FinalSmem fs{};
+        FinalSmem fs{};  // batch-wide layout of the omega-table kernel: RSH rows up to the largest lambda
         fs.rsh_stride = 2 * fin_lam + 1;
         fs.n_rsh = (fin_lam + 1) * fs.rsh_stride;
-        int n_om = 1, nabmax = 1;
-        for (auto &lp : atab_need) {
-            n_om = std::max(n_om, n_abc(lp.second) * lam_slots(lp.first, lp.second) * (2 * lp.first + 1));
-            nabmax = std::max(nabmax, n_abc(lp.second));
-        }
-        fs.n_omega = n_om;
-        fs.n_q = fin_nq;
-        fs.n_v = std::max(6144, 3 * nabmax);
-        // W for the factored re-centring sum: ncart(lb) x n_abc(la) x 3, if it fits in 64 kB
-        int lmax_task = 0;
-        for (int i = 0; i < ns; i++) lmax_task = std::max(lmax_task, sh_L[i]);
-        const int nw = ncart(lmax_task) * nabmax * 3;
-        const size_t smem_base = (size_t)(2 * fs.n_rsh + 2 * fs.n_omega + fs.n_q + fs.n_v) * sizeof(double);
-        CHECK_INPUT(smem_base <= kFinSmemMax, "assembly tables of this batch exceed the shared memory of one block");
-        fs.n_w = smem_base + (size_t)nw * sizeof(double) <= kFinSmemMax ? nw : 0;
-        const size_t smem = smem_base + (size_t)fs.n_w * sizeof(double);
         P.fin = f;
         P.fin_smem_layout = fs;
         P.omtab = omd;
@@ -1201,10 +1300,28 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         P.om_centre = at<int>(ib, o_fpc);
         P.om_smem = (size_t)fs.n_rsh * sizeof(double);
         P.om_blocks = (int)std::min<int64_t>((int64_t)fp_shell.size(), (int64_t)nsm * 8);
-        int fin_occ = 0;  // persistent grid over the task queue
-        GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fin_occ, final_kernel, kFinThreads, smem));
-        P.fin_blocks = (int)std::min<int64_t>(nt, (int64_t)nsm * std::max(fin_occ, 1));
-        P.fin_smem = smem;
+        // persistent grid per assembly group over its part of the task queue
+        for (auto &G : fin_groups) {
+            int occ = 0;
+            if (G.nt == 128) GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, final_kernel<128>, 128, G.smem));
+            else if (G.nt == 256) GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, final_kernel<256>, 256, G.smem));
+            else GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, final_kernel<512>, 512, G.smem));
+            G.blocks = (int)std::min<int64_t>(G.count, (int64_t)nsm * std::max(occ, 1));
+        }
+        // queue counters of the groups: status words 48..63 (zeroed with the status area before
+        // every execution); one group per class (autotuning) takes its tasks round-robin instead
+        CHECK_INPUT(opt.fin_by_class || fin_groups.size() <= 16, "more than 16 assembly launch groups");
+        P.fin_queue = opt.fin_by_class ? nullptr : statusd + 48;
+        P.fin_groups = fin_groups;
+        P.time_groups = opt.fin_by_class != 0;
+        if (P.time_groups) {
+            auto &gv = st.gev[set];
+            while (gv.size() < fin_groups.size() + 1) {
+                cudaEvent_t e;
+                GRPP_CUDA(cudaEventCreate(&e));
+                gv.push_back(e);
+            }
+        }
     }
     return 0;
 }
@@ -1216,7 +1333,7 @@ int plan_launch(Plan &P)
     cudaStream_t s = st.stream;
     cudaEvent_t *ev = st.ev[P.set];
     if (P.n_tasks == 0) return 0;
-    GRPP_CUDA(cudaMemsetAsync(P.status, 0, 16 * sizeof(int) + kRadCntNum * sizeof(unsigned long long), s));
+    GRPP_CUDA(cudaMemsetAsync(P.status, 0, 64 * sizeof(int), s));  // status, counters, assembly queues
     GRPP_CUDA(cudaEventRecord(ev[0], s));
     if (P.mmd_blocks > 0) {
         if (P.count_ops) {
@@ -1276,8 +1393,19 @@ int plan_launch(Plan &P)
                                                                     P.om_pairs, P.omtab);
         GRPP_CUDA(cudaGetLastError());
     }
-    final_kernel<<<P.fin_blocks, kFinThreads, P.fin_smem, s>>>(P.fin, P.fin_smem_layout);
-    GRPP_CUDA(cudaGetLastError());
+    for (size_t gi = 0; gi < P.fin_groups.size(); gi++) {
+        const FinGroup &G = P.fin_groups[gi];
+        FinalArgs f = P.fin;
+        f.order = P.fin.order + G.first;
+        f.n_tasks = G.count;
+        f.queue = P.fin_queue ? P.fin_queue + gi : nullptr;
+        if (P.time_groups) GRPP_CUDA(cudaEventRecord(st.gev[P.set][gi], s));
+        if (G.nt == 128) final_kernel<128><<<G.blocks, 128, G.smem, s>>>(f, G.fs);
+        else if (G.nt == 256) final_kernel<256><<<G.blocks, 256, G.smem, s>>>(f, G.fs);
+        else final_kernel<512><<<G.blocks, 512, G.smem, s>>>(f, G.fs);
+        GRPP_CUDA(cudaGetLastError());
+    }
+    if (P.time_groups) GRPP_CUDA(cudaEventRecord(st.gev[P.set][P.fin_groups.size()], s));
     GRPP_CUDA(cudaEventRecord(ev[3], s));
     int *hs = st.hstat[P.set];
     GRPP_CUDA(cudaMemcpyAsync(hs, P.status, 16 * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1304,6 +1432,9 @@ int plan_finish(Plan &P)
     P.stats.fallbacks = hstatus[4];
     cudaEventElapsedTime(&P.stats.ms_final, ev[2], ev[3]);
     cudaEventElapsedTime(&P.stats.ms_total, ev[0], ev[3]);
+    if (P.time_groups)
+        for (size_t gi = 0; gi < P.fin_groups.size(); gi++)
+            cudaEventElapsedTime(&P.fin_groups[gi].ms, st.gev[P.set][gi], st.gev[P.set][gi + 1]);
     P.stats.n_tasks = P.n_tasks;
     P.stats.n_radial = P.n_radial;
     P.stats.n_mmd = P.n_mmd;
@@ -2083,6 +2214,61 @@ int set_device(int device)
 {
     GRPP_CUDA(cudaSetDevice(device));
     return 0;
+}
+
+// Assembly autotuner: every class of the batch runs with each block size as a launch of its
+// own (round-robin over the class's tasks, CUDA events around each launch), twice; the second
+// timing counts. The fastest block size per class goes into the device's table, which the
+// planner uses for later batches. Rows: class key, tasks, ms at 128, 256, 512 threads, choice.
+int autotune_assembly(const libgrpp_b200_batch_t *b, int radial_mode, std::vector<std::array<double, 6>> &rows)
+{
+    set_error(0, "");
+    int rc = 0;
+    DeviceState *stp = get_state(rc);
+    if (!stp) return rc;
+    std::lock_guard<std::mutex> lk(stp->mu);
+    const int sizes[3] = {128, 256, 512};
+    std::map<int, std::array<double, 6>> tab;
+    for (int v = 0; v < 3; v++) {
+        RunOptions o;
+        o.radial_mode = radial_mode;
+        o.fin_nt = sizes[v];
+        o.fin_by_class = 1;
+        Plan P;
+        rc = plan_build(*stp, b, o, true, P);
+        if (rc == 0) rc = plan_execute(P);
+        if (rc == 0) rc = plan_execute(P);
+        if (rc == 0)
+            for (const FinGroup &G : P.fin_groups) {
+                auto &r = tab[G.key];
+                r[0] = G.key;
+                r[1] = G.count;
+                r[2 + v] = G.ms;
+            }
+        for (DevBuf *d : {&P.in, &P.scratch, &P.out})
+            if (d->p) cudaFree(d->p);
+        if (rc) return rc;
+    }
+    rows.clear();
+    for (auto &kv : tab) {
+        auto r = kv.second;
+        int best = 0;
+        for (int v = 1; v < 3; v++)
+            if (r[2 + v] < r[2 + best]) best = v;
+        r[5] = sizes[best];
+        stp->fin_tune[kv.first] = sizes[best];
+        rows.push_back(r);
+    }
+    return 0;
+}
+
+void autotune_reset()
+{
+    int rc = 0;
+    DeviceState *stp = get_state(rc);
+    if (!stp) return;
+    std::lock_guard<std::mutex> lk(stp->mu);
+    stp->fin_tune.clear();
 }
 
 void plan_destroy(Plan *P)

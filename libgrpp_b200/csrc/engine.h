@@ -2,7 +2,9 @@
 #pragma once
 
 #include <cstdint>
+#include <array>
 #include <string>
+#include <vector>
 
 #include "../../include/libgrpp_b200.h"
 
@@ -11,6 +13,8 @@ namespace grpp {
 struct RunOptions {
     int radial_mode = LIBGRPP_B200_RADIAL_PLAIN;
     int raw_so = 0;          // spin-orbit output without the 2/(2L+1) factor (libgrpp_spin_orbit_integrals)
+    int fin_nt = 0;          // assembly block size for every task (128, 256, 512); 0: tuning table, else default rule
+    int fin_by_class = 0;    // one assembly launch per class, each timed (autotuning)
 };
 
 struct RunStats {
@@ -42,6 +46,9 @@ void plan_destroy(Plan *P);
 const RunStats *plan_stats(const Plan *P);
 int64_t plan_h2d_bytes(const Plan *P);
 int set_device(int device);
+// per-class block size of the assembly kernel (rows: class key, tasks, ms at 128/256/512, choice)
+int autotune_assembly(const libgrpp_b200_batch_t *b, int radial_mode, std::vector<std::array<double, 6>> &rows);
+void autotune_reset();
 void *host_alloc(size_t bytes);
 void host_free(void *p);
 int measure_fp64_peak(double *tflops);

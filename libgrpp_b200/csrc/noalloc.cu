@@ -145,7 +145,7 @@ int setup(int dev)
     NA_CUDA(cudaGetSymbolAddress(&p, g_scratch));
     g_scratch_ptr[dev] = (unsigned char *)p;
     NA_CUDA(cudaFuncSetAttribute(radial_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-    NA_CUDA(cudaFuncSetAttribute(final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    NA_CUDA(cudaFuncSetAttribute(final_kernel<kFinThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     g_ready[dev] = true;
     return 0;
 }
@@ -447,7 +447,7 @@ int run(const libgrpp_b200_batch_t *b, double *h_arep)
     fs.n_q = fin_nq;
     fs.n_v = std::max(6144, 3 * nabmax);
     const size_t smem = (size_t)(2 * fs.n_rsh + 2 * fs.n_omega + fs.n_q + fs.n_v) * sizeof(double);
-    final_kernel<<<(int)std::min<int64_t>(nt, (int64_t)nsm * 8), kFinThreads, smem>>>(f, fs);
+    final_kernel<kFinThreads><<<(int)std::min<int64_t>(nt, (int64_t)nsm * 8), kFinThreads, smem>>>(f, fs);
     NA_CUDA(cudaGetLastError());
     NA_CUDA(cudaMemcpy(h_arep, P(o_arep), out_tot * sizeof(double), cudaMemcpyDeviceToHost));
     return 0;

@@ -44,12 +44,12 @@ def test_oracle_matches_golden(oracle_lib, name):
 
 def test_oracle_full_kcs_matrices_against_shipped(oracle_lib):
     """The full KCs AREP and SO matrices (54 basis shells, 2 centres, outercore terms) from the
-    oracle against libgrpp's shipped matrices (test/KCs/*.txt); the one element where libgrpp's
-    C path and its shipped Fortran-driver matrix disagree is judged against its binary128 value."""
+    oracle against libgrpp's shipped matrices (test/KCs/*.txt); the elements on which libgrpp keeps
+    few digits (among them the one where libgrpp's C path and its shipped Fortran-driver matrix
+    disagree) are judged against their binary128 values."""
     batch, z = full_system("kcs")
     got = assemble_lower(batch, oracle_lib.driver_full_batch(batch, nthreads=8), int(z["n_shells"]))
     sel = z["truth_idx"]
-    assert len(sel) == 1
     truth = {k: z[k] for k in z.files if k.startswith(("truth_", "refdev_"))}
     for comp, g in zip(COMPS, got):
         ok, rep = truth_parity(g, z["shipped_" + comp], truth, sel, comp)
