@@ -18,9 +18,11 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 
-SOURCES = ["engine.cu", "tables.cpp", "capi.cpp", "fortran_abi.cpp", "noalloc.cu"]
+SOURCES = ["engine.cu", "nofma.cu", "tables.cpp", "capi.cpp", "fortran_abi.cpp", "noalloc.cu"]
+# libgrpp is built without floating-point contraction; the angular sums round as its do
+EXTRA = {"nofma.cu": ["-fmad=false"]}
 HEADERS = ["grpp_common.cuh", "specfunc.cuh", "mmd.cuh", "radial.cuh", "angular.cuh", "level_model.cuh", "gradient.cuh", "tables.h",
-           "engine.h", "onee.cuh", "nucmodel.h"]
+           "engine.h", "onee.cuh", "nucmodel.h", "nofma_launch.h"]
 
 
 def _newer(target, deps):
@@ -40,7 +42,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
         o = os.path.join(BUILD, src + ".o")
         objs.append(o)
         if force or _newer(o, [s] + hdrs):
-            cmd = [NVCC] + ARCH + COMMON + ["-c", s, "-o", o]
+            cmd = [NVCC] + ARCH + COMMON + EXTRA.get(src, []) + ["-c", s, "-o", o]
             if src.endswith(".cu"):
                 cmd += ["-Xptxas", "-v"] if verbose else []
             else:

@@ -58,6 +58,7 @@ __device__ __forceinline__ double usp_integral(int i, int j, int k)
     return 4 * kPi * dfact(i - 1) * dfact(j - 1) * dfact(k - 1) / dfact(i + j + k + 1);
 }
 
+#ifndef GRPP_NO_ANGULAR_KERNELS
 // Atab[abc][slot][mu][m] = sum_uvw sum_rst y_{Lm,uvw} y_{lam mu,rst} I(a+r+u, ...),
 // terms skipped when |y| < 1e-14, accumulated in the reference's order
 // (angular_integrals.c:78-106: uvw outer, rst inner, y_lam * y_L * usp).
@@ -112,6 +113,8 @@ __global__ void atab_kernel(int L, int l, double *out)
     }
 }
 
+#endif  // GRPP_NO_ANGULAR_KERNELS
+
 // ---- outercore spherical projections ---------------------------------------------
 // S_sph[i][m] = sum_icart coef[m][icart] S_cart[i][icart] (outercore_integrals.c:514-525),
 // coef = spherical_to_cartesian_coef(L, m, r, s, t) / ang_norm_factor(r, s, t) (:165-177).
@@ -140,6 +143,7 @@ __device__ inline double sph_coef_oc(int L, int m, int r, int s, int t)
     return y / an;
 }
 
+#ifndef GRPP_NO_ANGULAR_KERNELS
 __global__ void oc_proj_kernel(OcProjArgs a)
 {
     for (int blk = blockIdx.x; blk < a.n; blk += gridDim.x) {
@@ -159,6 +163,7 @@ __global__ void oc_proj_kernel(OcProjArgs a)
         }
     }
 }
+#endif  // GRPP_NO_ANGULAR_KERNELS
 
 // ---- final per-task assembly -----------------------------------------------------
 
@@ -256,6 +261,7 @@ __device__ __forceinline__ double lmat_val(int L, int comp, int m1, int m2)
     return c_tab.lmat[c_tab.lmat_off[L] + comp * d * d + (m1 + L) * d + (m2 + L)];
 }
 
+#ifndef GRPP_NO_ANGULAR_KERNELS
 // Omega tables of one side for every (shell, centre) pair: a CTA per pair computes the
 // real spherical harmonics of the unit vector along k = -2 a (C - S) (a the shell's first
 // exponent) and, for each semilocal potential of the centre's GRPP in order,
@@ -636,13 +642,17 @@ __global__ void __launch_bounds__(NT) final_kernel(FinalArgs a, FinalSmem sm)
                         }
                     }
                     __syncthreads();
+                    // elements whose factored sum is not certified fall back to the term-by-term loop
+                    unsigned tbt = fact ? 0u : ~0u;
                     if (fact) {
+                        // W[j][abc] = sum_def F_B V[abc][def] and Wa[j][abc] = sum_def |F_B| max_c |V[abc][def]|
                         double *W = V + sm.n_v;
                         const int nrow = r1 - r0;
+                        double *Wa = W + nB * nrow * ncomp;
                         for (int e = tid; e < nB * nrow; e += NT) {
                             const int j = e / nrow, ar = e % nrow;
                             const int bx = cB[3 * j], by = cB[3 * j + 1], bz = cB[3 * j + 2];
-                            double w0 = 0.0, w1 = 0.0, w2 = 0.0;
+                            double w0 = 0.0, w1 = 0.0, w2 = 0.0, wa = 0.0;
                             for (int dd = 0; dd <= bx; dd++)
                                 for (int ee = 0; ee <= by; ee++)
                                     for (int ff = 0; ff <= bz; ff++) {
@@ -652,10 +662,13 @@ __global__ void __launch_bounds__(NT) final_kernel(FinalArgs a, FinalSmem sm)
                                         if (fb == 0.0) continue;
                                         const double *vv = V + (ar * nabB + abc_index(lb, dd, ee, ff)) * ncomp;
                                         w0 += fb * vv[0];
+                                        double vm = fabs(vv[0]);
                                         if (so) {
                                             w1 += fb * vv[1];
                                             w2 += fb * vv[2];
+                                            vm = fmax(vm, fmax(fabs(vv[1]), fabs(vv[2])));
                                         }
+                                        wa += fabs(fb) * vm;
                                     }
                             double *ww = W + (j * nrow + ar) * ncomp;
                             ww[0] = w0;
@@ -663,6 +676,7 @@ __global__ void __launch_bounds__(NT) final_kernel(FinalArgs a, FinalSmem sm)
                                 ww[1] = w1;
                                 ww[2] = w2;
                             }
+                            Wa[j * nrow + ar] = wa;
                         }
                         __syncthreads();
 #pragma unroll
@@ -671,7 +685,9 @@ __global__ void __launch_bounds__(NT) final_kernel(FinalArgs a, FinalSmem sm)
                             if (el >= nel) continue;
                             const int i = el / nB, j = el % nB;
                             const int ax = cA[3 * i], ay = cA[3 * i + 1], az = cA[3 * i + 2];
-                            double g0 = gam[0][q], g1 = gam[1][q], g2 = gam[2][q];
+                            const int bx = cB[3 * j], by = cB[3 * j + 1], bz = cB[3 * j + 2];
+                            double g0 = 0.0, g1 = 0.0, g2 = 0.0, ga = 0.0;
+                            int nta = 0;
                             for (int aa = 0; aa <= ax; aa++)
                                 for (int bb = 0; bb <= ay; bb++)
                                     for (int cc = 0; cc <= az; cc++) {
@@ -681,24 +697,39 @@ __global__ void __launch_bounds__(NT) final_kernel(FinalArgs a, FinalSmem sm)
                                                           c_tab.binom[az * kBinN + cc] * powA[0][ax - aa] * powA[1][ay - bb] *
                                                           powA[2][az - cc];
                                         if (fa == 0.0) continue;
+                                        nta++;
                                         const double *ww = W + (j * nrow + abc - r0) * ncomp;
                                         g0 += fa * ww[0];
                                         if (so) {
                                             g1 += fa * ww[1];
                                             g2 += fa * ww[2];
                                         }
+                                        ga += fabs(fa) * Wa[j * nrow + abc - r0];
                                     }
-                            gam[0][q] = g0;
-                            gam[1][q] = g1;
-                            gam[2][q] = g2;
+                            // Both this sum and libgrpp's term-by-term sum of the same terms are within
+                            // (n + 12) u sum|terms| of the exact value, n = the number of terms and 12 u the
+                            // rounding of a term's factors; the two differ by at most twice that. The
+                            // factored result is kept when that bound, scaled by 16 pi^2, is below 1e-12
+                            // absolute or 1e-12 of the partial sum itself (1% of the 1e-10 / 1e-9 comparator);
+                            // otherwise, where the re-centring sum cancels, the element is summed term by
+                            // term in libgrpp's order.
+                            const double nterm = (double)nta * (double)((bx + 1) * (by + 1) * (bz + 1));
+                            const double bound = 2.0 * (nterm + 12.0) * 1.1102230246251565e-16 * ga * (16 * kPi * kPi);
+                            const double gmax = fmax(fabs(g0), fmax(fabs(g1), fabs(g2)));
+                            if (bound <= fmax(1e-12, 1e-12 * gmax * (16 * kPi * kPi))) {
+                                gam[0][q] += g0;
+                                gam[1][q] += g1;
+                                gam[2][q] += g2;
+                            } else {
+                                tbt |= 1u << q;
+                            }
                         }
-                        continue;
                     }
                     // Cartesian pairs: binomial re-centring sums over (a..f) in the reference's loop order
 #pragma unroll
                     for (int q = 0; q < EPT; q++) {
                         const int el = tid + q * NT;
-                        if (el >= nel) continue;
+                        if (el >= nel || !((tbt >> q) & 1u)) continue;
                         const int i = el / nB, j = el % nB;
                         const int ax = cA[3 * i], ay = cA[3 * i + 1], az = cA[3 * i + 2];
                         const int bx = cB[3 * j], by = cB[3 * j + 1], bz = cB[3 * j + 2];
@@ -859,5 +890,6 @@ __global__ void __launch_bounds__(NT) final_kernel(FinalArgs a, FinalSmem sm)
         }
     }
 }
+#endif  // GRPP_NO_ANGULAR_KERNELS
 
 }  // namespace grpp

@@ -26,9 +26,12 @@
 
 #include "grpp_common.cuh"
 #include "specfunc.cuh"
+#define GRPP_NO_RADIAL_TABLE_KERNELS  // ftab_kernel, wu_table_kernel: compiled in nofma.cu
 #include "radial.cuh"
 #include "mmd.cuh"
+#define GRPP_NO_ANGULAR_KERNELS  // the angular kernels are compiled in nofma.cu (no contraction)
 #include "angular.cuh"
+#include "nofma_launch.h"
 #include "level_model.cuh"
 #include "gradient.cuh"
 #include "onee.cuh"
@@ -168,8 +171,10 @@ int init_device_state(DeviceState &st, int device)
     GRPP_CUDA(upload_vec(st, h.lmat_off, &d.lmat_off));
     GRPP_CUDA(upload_vec(st, h.dfact, &d.dfact));
     GRPP_CUDA(upload_vec(st, h.binom, &d.binom));
+    GRPP_CUDA(upload_vec(st, h.grid, &d.grid));
     GRPP_CUDA(upload_vec(st, h.fermi, &st.fermi));
     GRPP_CUDA(cudaMemcpyToSymbol(c_tab, &d, sizeof(d)));
+    GRPP_CUDA(ang_upload_tables(&d, sizeof(d)));
     GRPP_CUDA(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking));
     GRPP_CUDA(cudaStreamCreateWithFlags(&st.copy_stream, cudaStreamNonBlocking));
     for (int k = 0; k < 2; k++) {
@@ -185,9 +190,7 @@ int init_device_state(DeviceState &st, int device)
     GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(mmd_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRPP_CUDA(cudaFuncSetAttribute(radial_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-    GRPP_CUDA(cudaFuncSetAttribute(final_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFinSmemMax));
-    GRPP_CUDA(cudaFuncSetAttribute(final_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFinSmemMax));
-    GRPP_CUDA(cudaFuncSetAttribute(final_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFinSmemMax));
+    GRPP_CUDA(ang_set_final_max_smem((int)kFinSmemMax));
     GRPP_CUDA(cudaFuncSetAttribute(type1_num_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(t1_smem_doubles(kT1MaxLam) * sizeof(double))));
     GRPP_CUDA(cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_train_smem_bytes()));
@@ -344,8 +347,9 @@ static std::vector<int> order_by_cost(const std::vector<double> &cost)
 // Assembly classes and shared-memory layouts. A class is (la, lb, largest semilocal L, spin-orbit
 // terms or not); the layout holds the task's RSH rows, both sides' omega tables, its radial
 // table, the V rows of one potential (all rows when they fit in 6144 values) and W of the
-// factored re-centring sum. W holds ncart(lb) x rows x components values and rows is chosen so
-// that nabB x rows x components fits in V, so a W as large as V always suffices.
+// factored re-centring sum. W holds ncart(lb) x rows x (components + 1) values (the sums and the
+// sums of absolute terms) and rows is chosen so that nabB x rows x components fits in V, so a W
+// twice as large as V always suffices.
 static int fin_class_key(int la, int lb, int Lmax, bool so) { return ((la * 16 + lb) * 16 + Lmax) * 2 + (so ? 1 : 0); }
 
 static int fin_default_nt(int la, int lb)
@@ -363,7 +367,7 @@ static FinalSmem fin_layout(int lam, int n_omega, int n_q, int nabA, int nabB, i
     fs.n_q = n_q;
     fs.n_v = std::min(6144, std::max(nabA * nabB * ncomp, 3 * std::max(nabA, nabB)));
     fs.n_v = std::max(fs.n_v, 3 * std::max(nabA, nabB));
-    fs.n_w = fs.n_v;
+    fs.n_w = 2 * fs.n_v;
     return fs;
 }
 
@@ -499,8 +503,7 @@ int ensure_atab(DeviceState &st, int L, int l)
     double *dst = (double *)st.atab.p + st.atab_used;
     const int threads = 256;
     const int blocks = (int)std::min<int64_t>((sz + threads - 1) / threads, 4096);
-    atab_kernel<<<std::max(blocks, 1), threads, 0, st.stream>>>(L, l, dst);
-    GRPP_CUDA(cudaGetLastError());
+    GRPP_CUDA(ang_launch_atab(std::max(blocks, 1), threads, st.stream, L, l, dst));
     st.atab_off[key] = (int64_t)st.atab_used;
     st.atab_used += sz;
     st.atab_dirty = true;
@@ -1303,9 +1306,7 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         // persistent grid per assembly group over its part of the task queue
         for (auto &G : fin_groups) {
             int occ = 0;
-            if (G.nt == 128) GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, final_kernel<128>, 128, G.smem));
-            else if (G.nt == 256) GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, final_kernel<256>, 256, G.smem));
-            else GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, final_kernel<512>, 512, G.smem));
+            GRPP_CUDA(ang_final_occupancy(G.nt, G.smem, &occ));
             G.blocks = (int)std::min<int64_t>(G.count, (int64_t)nsm * std::max(occ, 1));
         }
         // queue counters of the groups: status words 48..63 (zeroed with the status area before
@@ -1347,8 +1348,7 @@ int plan_launch(Plan &P)
     }
     GRPP_CUDA(cudaEventRecord(ev[1], s));
     if (P.ocp_blocks > 0) {
-        oc_proj_kernel<<<P.ocp_blocks, 64, 0, s>>>(P.ocp);
-        GRPP_CUDA(cudaGetLastError());
+        GRPP_CUDA(ang_launch_oc_proj(P.ocp_blocks, 64, s, &P.ocp, sizeof(P.ocp)));
     }
     if (P.rad_blocks > 0) {
         GRPP_CUDA(cudaMemsetAsync(P.rad.walk, 0, (size_t)P.n_radial, s));
@@ -1377,21 +1377,18 @@ int plan_launch(Plan &P)
             GRPP_CUDA(cudaEventRecord(ev[5], s));
         }
         if (P.wu) {
-            wu_table_kernel<<<P.wu_blocks, 256, 0, s>>>(P.rad, P.wu_grpps, P.wu);
-            GRPP_CUDA(cudaGetLastError());
+            GRPP_CUDA(nofma_launch_wu_table(P.wu_blocks, 256, s, &P.rad, sizeof(P.rad), P.wu_grpps, P.wu));
         }
         if (P.ftab) {
-            ftab_kernel<<<P.ft_blocks, kRadThreads, P.ft_smem, s>>>(P.rad, P.ftab);
-            GRPP_CUDA(cudaGetLastError());
+            GRPP_CUDA(nofma_launch_ftab(P.ft_blocks, kRadThreads, P.ft_smem, s, &P.rad, sizeof(P.rad), P.ftab));
         }
         radial_walk_kernel<<<P.rad_blocks, kRadThreads, P.rad_smem, s>>>(ra);
         GRPP_CUDA(cudaGetLastError());
     }
     GRPP_CUDA(cudaEventRecord(ev[2], s));
     if (P.omtab) {
-        omega_tab_kernel<<<P.om_blocks, kFinThreads, P.om_smem, s>>>(P.fin, P.fin_smem_layout, P.om_shell, P.om_centre,
-                                                                    P.om_pairs, P.omtab);
-        GRPP_CUDA(cudaGetLastError());
+        GRPP_CUDA(ang_launch_omega_tab(P.om_blocks, kFinThreads, P.om_smem, s, &P.fin, sizeof(P.fin), &P.fin_smem_layout,
+                                       sizeof(P.fin_smem_layout), P.om_shell, P.om_centre, P.om_pairs, P.omtab));
     }
     for (size_t gi = 0; gi < P.fin_groups.size(); gi++) {
         const FinGroup &G = P.fin_groups[gi];
@@ -1400,10 +1397,7 @@ int plan_launch(Plan &P)
         f.n_tasks = G.count;
         f.queue = P.fin_queue ? P.fin_queue + gi : nullptr;
         if (P.time_groups) GRPP_CUDA(cudaEventRecord(st.gev[P.set][gi], s));
-        if (G.nt == 128) final_kernel<128><<<G.blocks, 128, G.smem, s>>>(f, G.fs);
-        else if (G.nt == 256) final_kernel<256><<<G.blocks, 256, G.smem, s>>>(f, G.fs);
-        else final_kernel<512><<<G.blocks, 512, G.smem, s>>>(f, G.fs);
-        GRPP_CUDA(cudaGetLastError());
+        GRPP_CUDA(ang_launch_final(G.nt, G.blocks, G.smem, s, &f, sizeof(f), &G.fs, sizeof(G.fs)));
     }
     if (P.time_groups) GRPP_CUDA(cudaEventRecord(st.gev[P.set][P.fin_groups.size()], s));
     GRPP_CUDA(cudaEventRecord(ev[3], s));

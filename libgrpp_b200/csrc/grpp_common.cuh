@@ -26,6 +26,16 @@ constexpr int kBinN = 48;          // binomial table n = 0..kBinN-1
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kZeroThresh = 1e-14;  // LIBGRPP_ZERO_THRESH
 
+// Nested Log3 grid of the type 2 radial integrals: the 8191 points of levels 0..8 in walk
+// order (level 0: points 1..31 of 31; level L >= 1: the odd points of 2^(L+5) - 1). The host
+// tabulates per point, with libgrpp's expressions and C library (radial_type2_integral.c:357-365,
+// 440-441; potential.c:70-81): r, the weight w at the point's own level, r^-1 = pow(r, -1),
+// r^-2 = pow(r, -2) and r^N = pow(r, N) for N = 0..kGridMaxN.
+constexpr int kGridPts = 8191;
+constexpr int kGridMaxN = 24;
+constexpr int kGridRowR = 0, kGridRowW = 1, kGridRowRinv = 2, kGridRowRinv2 = 3, kGridRowPow0 = 4;
+constexpr int kGridRows = kGridRowPow0 + kGridMaxN + 1;
+
 struct DeviceTables {
     const double *bessel;     // [kBesNX][kBesL][5]: value + 4 derivatives
     const double *bessel_p;   // the same values as [kBesNX][kBesL/2][5][2]: orders 2p, 2p+1 side by side
@@ -40,6 +50,7 @@ struct DeviceTables {
     const int *lmat_off;      // [kMaxL+2]
     const double *dfact;      // dfact[n+1] = n!!, n = -1..kDfMax
     const double *binom;      // [kBinN][kBinN]
+    const double *grid;       // [kGridRows][kGridPts] (null: the kernels compute r and w themselves)
 };
 
 __host__ __device__ inline int ncart(int L) { return (L + 1) * (L + 2) / 2; }

@@ -126,6 +126,7 @@ int setup(int dev)
     }
     const ::grpp::HostTables &h = g_host;
     DeviceTables d;
+    d.grid = nullptr;  // grid points computed by the kernels themselves
     int rc = 0;
     if ((rc = copy_table(g_bessel, h.bessel, kNaBessel, &d.bessel))) return rc;
     if ((rc = copy_table(g_bessel_p, h.bessel_p, kNaBessel, &d.bessel_p))) return rc;

@@ -328,6 +328,7 @@ __device__ __forceinline__ bool scr_prim_flat(int l1, int l2, int n, double CA, 
     return false;
 }
 
+#ifndef GRPP_RADIAL_TABLES_ONLY
 // Screening of every (task, entry) of a batch, one thread per entry over the flattened
 // entry space (entries of one task are consecutive, tasks in item order): no per-task
 // barrier and no ragged last round. A thread follows screening.c:193-220 for its entry:
@@ -470,6 +471,7 @@ __global__ void __launch_bounds__(kRadThreads, GRPP_SCR_MINB) radial_screen_flat
         }
     }
 }
+#endif  // GRPP_RADIAL_TABLES_ONLY
 
 // decode entry index within an item -> (potential, l1, l2, N)
 __device__ __forceinline__ void decode_entry(const RadialShared &sh, int e, int &p, int &l1, int &l2, int &N)
@@ -491,6 +493,27 @@ __device__ __forceinline__ void log3_point(int i, int nr, double &r, double &w)
     const double xi = i / (nr + 1.0), xi3 = xi * xi * xi, ln = log(1 - xi3);
     w = 3 * R3 * xi * xi * ln * ln / ((1 - xi3) * (nr + 1.0));
     r = -R * ln;
+}
+
+// r and w of walk-order point f (point i of the level's nr-point grid): libgrpp's values from
+// the host-built grid table (grpp_common.cuh) when present, else computed here
+__device__ __forceinline__ void grid_point(int f, int i, int nr, double &r, double &w)
+{
+    if (c_tab.grid) {
+        r = __ldg(c_tab.grid + (size_t)kGridRowR * kGridPts + f);
+        w = __ldg(c_tab.grid + (size_t)kGridRowW * kGridPts + f);
+    } else {
+        log3_point(i, nr, r, w);
+    }
+}
+
+// r^(n-2) of a potential term (n = 0, 1, 2) at walk-order point f: pow(r, n-2) from the grid
+// table when present (potential.c:70-81), else 1/r^2, 1/r from the given reciprocals
+__device__ __forceinline__ double grid_rpow_m2(int f, int pw, double ir, double ir2)
+{
+    if (pw == 2) return 1.0;
+    if (c_tab.grid) return __ldg(c_tab.grid + (size_t)(pw == 1 ? kGridRowRinv : kGridRowRinv2) * kGridPts + f);
+    return pw == 1 ? ir : ir2;
 }
 
 
@@ -595,6 +618,7 @@ __device__ double one_centre_entry(const RadialArgs &a, const RadialShared &sh, 
     return v;
 }
 
+#ifndef GRPP_RADIAL_TABLES_ONLY
 __global__ void __launch_bounds__(kRadThreads) radial_screen_kernel(RadialArgs a)
 {
     __shared__ RadialShared sh;
@@ -676,6 +700,7 @@ __global__ void __launch_bounds__(kRadThreads) radial_screen_kernel(RadialArgs a
         }
     }
 }
+#endif  // GRPP_RADIAL_TABLES_ONLY
 
 // dst[l * stride] += e * M_l(x) for l = 0..lmax, one table row (specfunc_scaled_mod_sph_bessel.c:72-122)
 __device__ __forceinline__ void bessel_row_acc(int lmax, double x, double e, double *dst, int stride)
@@ -707,7 +732,7 @@ __device__ __forceinline__ void bessel_row_acc(int lmax, double x, double e, dou
 }
 
 constexpr int kRadRow = kRadThreads + 1;  // padded row stride of the chunk arrays (no bank conflicts)
-constexpr int kRadGridPts = 8191;         // points of levels 0..8 together
+constexpr int kRadGridPts = kGridPts;     // points of levels 0..8 together
 
 // Level of point f of the nested grid in walk order (level 0: f = 0..30; level L >= 1:
 // f = 2^(L+4)-1 .. 2^(L+5)-2), and the point's index i on that level's grid of nr points.
@@ -740,6 +765,7 @@ __device__ __forceinline__ int level_last_point(int L) { return (1 << (L + 5)) -
 // The walk of a task stops at the first chunk boundary after which no entry is active;
 // points evaluated past that are never added. The orders, powers and potentials
 // evaluated per point shrink with the set of active entries.
+#ifndef GRPP_NO_RADIAL_TABLE_KERNELS
 // F_l(r) of every (shell, centre) pair of the batch at every point of the nested grid, one
 // CTA per pair and chunk of 128 points: the same point, distance CS (as load_task forms it),
 // primitives, exact-zero skips and Bessel rows as the walk's own evaluation, so every order
@@ -761,7 +787,7 @@ __global__ void __launch_bounds__(kRadThreads) ftab_kernel(RadialArgs a, double 
         int lev, i, nr;
         walk_point(f, lev, i, nr);
         double r, w;
-        log3_point(i, nr, r, w);
+        grid_point(f, i, nr, r, w);
         for (int l = 0; l <= lmax; l++) cf[l * kRadRow + tid] = 0.0;
         const double d2 = (r - CS) * (r - CS);
         const int np = a.rp_n[s], off = a.rp_off[s];
@@ -795,21 +821,22 @@ __global__ void wu_table_kernel(RadialArgs a, int n_grpps, double *wu)
         int lev, i, nr;
         walk_point(f, lev, i, nr);
         double r, w;
-        log3_point(i, nr, r, w);
+        grid_point(f, i, nr, r, w);
         const double r2 = r * r, ir = 1.0 / r, ir2 = 1.0 / r2;
         double u = 0.0;
         for (int k = 0; k < a.pot_nprim[pot]; k++) {
             const int o = a.pot_prim_off[pot] + k;
             const double ex = exp(-a.pot_alpha[o] * r2);
             if (ex == 0.0) continue;  // the term adds an exact zero
-            const int pw = a.pot_powers[o];
-            const double rp = pw == 2 ? 1.0 : (pw == 1 ? ir : ir2);  // r^(n-2)
+            const double rp = grid_rpow_m2(f, a.pot_powers[o], ir, ir2);  // r^(n-2)
             u += a.pot_coef[o] * rp * ex;
         }
         wu[id] = w * u;
     }
 }
+#endif  // GRPP_NO_RADIAL_TABLE_KERNELS
 
+#ifndef GRPP_RADIAL_TABLES_ONLY
 __global__ void __launch_bounds__(kRadThreads, 5) radial_walk_kernel(RadialArgs a)
 {
     __shared__ RadialShared sh;
@@ -893,7 +920,7 @@ __global__ void __launch_bounds__(kRadThreads, 5) radial_walk_kernel(RadialArgs 
                 int lev, i, nr;
                 walk_point(f0 + tid, lev, i, nr);
                 double r, w;
-                log3_point(i, nr, r, w);
+                grid_point(f0 + tid, i, nr, r, w);
                 const double r2 = r * r, ir = 1.0 / r, ir2 = 1.0 / r2;
                 const double *wug = a.wu ? a.wu + (int64_t)sh.grpp * a.wu_npot * kRadGridPts + f0 + tid : nullptr;
                 for (int pp = 0; pp < npot; pp++) {
@@ -907,8 +934,7 @@ __global__ void __launch_bounds__(kRadThreads, 5) radial_walk_kernel(RadialArgs 
                         const int tk = sh.poff[pp] + k;
                         const double ex = exp(-sh.talpha[tk] * r2);
                         if (ex == 0.0) continue;  // the term adds an exact zero
-                        const int pw = sh.tpow[tk];
-                        const double rp = pw == 2 ? 1.0 : (pw == 1 ? ir : ir2);  // r^(n-2)
+                        const double rp = grid_rpow_m2(f0 + tid, sh.tpow[tk], ir, ir2);  // r^(n-2)
                         u += sh.tcoef[tk] * rp * ex;
                     }
                     cwu[pp * kRadRow + tid] = w * u;
@@ -937,10 +963,16 @@ __global__ void __launch_bounds__(kRadThreads, 5) radial_walk_kernel(RadialArgs 
                         if (e != 0.0) bessel_row_acc(u2, sh.kb[q] * r, e, cf2 + tid, kRadRow);
                     }
                 }
-                double rn = 1.0;
-                for (int n = 0; n <= uN; n++) {
-                    crn[n * kRadRow + tid] = rn;
-                    rn *= r;
+                if (c_tab.grid) {
+                    // r^N = pow(r, N) as libgrpp tabulates it (radial_type2_integral.c:440-441)
+                    const double *gp = c_tab.grid + (size_t)kGridRowPow0 * kGridPts + f0 + tid;
+                    for (int n = 0; n <= uN; n++) crn[n * kRadRow + tid] = __ldg(gp + (size_t)n * kGridPts);
+                } else {
+                    double rn = 1.0;
+                    for (int n = 0; n <= uN; n++) {
+                        crn[n * kRadRow + tid] = rn;
+                        rn *= r;
+                    }
                 }
             }
             __syncthreads();
@@ -1026,5 +1058,6 @@ __global__ void __launch_bounds__(kRadThreads, 5) radial_walk_kernel(RadialArgs 
         }
     }
 }
+#endif  // GRPP_RADIAL_TABLES_ONLY
 
 }  // namespace grpp

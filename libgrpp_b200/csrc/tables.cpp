@@ -167,9 +167,43 @@ const double *fermi_table()
     return tab.data();
 }
 
+// The nested Log3 grid in walk order (grpp_common.cuh), with libgrpp's own expressions and the
+// C library's log and pow, evaluated in this host unit without contraction: r and w of
+// radial_type2_integral.c:357-365 (w at the point's own level nr), r^N = pow(r, N) of :440-441 and
+// r^(n-2) = pow(r, n-2) of potential.c:70-81 for the powers n = 0, 1.
+static void build_grid(std::vector<double> &g)
+{
+    g.assign((size_t)kGridRows * kGridPts, 0.0);
+    const double R = 5.0;
+    const double R3 = R * R * R;
+    for (int f = 0; f < kGridPts; f++) {
+        int level = 0;
+        while ((1 << (level + 5)) - 2 < f) level++;
+        const int nr = (1 << (level + 5)) - 1;
+        const int i = level == 0 ? f + 1 : 2 * (f - ((1 << (level + 4)) - 1)) + 1;
+        const double xi = i / (nr + 1.0);
+        const double xi3 = xi * xi * xi;
+        const double ln_xi = log(1 - xi3);
+        const double wi = 3 * R3 * xi * xi * ln_xi * ln_xi / ((1 - xi3) * (nr + 1.0));
+        const double ri = -R * ln_xi;
+        g[(size_t)kGridRowR * kGridPts + f] = ri;
+        g[(size_t)kGridRowW * kGridPts + f] = wi;
+        // exponents through a volatile so that the compiler calls pow as libgrpp does (its
+        // exponents are data) instead of folding pow(r, -1) into 1 / r
+        volatile double e1 = -1.0, e2 = -2.0;
+        g[(size_t)kGridRowRinv * kGridPts + f] = pow(ri, e1);
+        g[(size_t)kGridRowRinv2 * kGridPts + f] = pow(ri, e2);
+        for (int n = 0; n <= kGridMaxN; n++) {
+            volatile double en = n;
+            g[(size_t)(kGridRowPow0 + n) * kGridPts + f] = pow(ri, en);
+        }
+    }
+}
+
 void build_host_tables(HostTables &t)
 {
     t.fermi.assign(fermi_table(), fermi_table() + (size_t)kFermiNX * kFermiNK);
+    build_grid(t.grid);
     // Bessel values for orders 0..kBesL+4 so that all 4 derivative orders of 0..kBesL-1 are exact
     const int LV = kBesL + 5;
     std::vector<double> v((size_t)kBesNX * LV * 5, 0.0);

@@ -11,6 +11,7 @@
 #include <assert.h>
 #include <math.h>
 #include <stdio.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -108,12 +109,42 @@ void libgrpp_delete_potential(libgrpp_potential_t *p)
     free(p);
 }
 
+/* Rounding model (test infrastructure, off by default). With a nonzero seed, the results of the
+ * transcendental calls of the type 2 radial path -- exp and pow of the potential and of the
+ * contracted integrands, log of the grid, pow of r^N, the scaled Bessel values and the screening
+ * estimate -- are moved by -1, 0 or +1 unit in the last place, chosen by a hash of the seed, the
+ * call site and the argument (so a run does not depend on the thread schedule). Such a run stands
+ * for another implementation of libgrpp's algorithm whose math library and tables differ from
+ * libgrpp's in the last bit, which is what a GPU implementation is; the spread of a few runs
+ * measures how closely libgrpp's double-precision arithmetic determines each element. */
+static uint64_t rm_seed = 0;
+
+void orc_set_rounding_model(uint64_t seed) { rm_seed = seed; }
+
+static double rm(double x, uint64_t site)
+{
+    if (!rm_seed || x == 0.0 || !isfinite(x)) return x;
+    uint64_t h, b;
+    memcpy(&b, &x, sizeof b);
+    h = rm_seed * 0x9E3779B97F4A7C15ull ^ (b + 0x632BE59BD9B4E019ull * (site + 1));
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+    h *= 0x94D049BB133111EBull;
+    h ^= h >> 32;
+    switch (h % 3) {
+    case 0: return nextafter(x, -INFINITY);
+    case 1: return nextafter(x, INFINITY);
+    default: return x;
+    }
+}
+
 /* potential.c:70-81 */
 double libgrpp_potential_value(libgrpp_potential_t *p, double r)
 {
     double v = 0.0, r2 = r * r;
     for (int i = 0; i < p->num_primitives; i++)
-        v += p->coeffs[i] * pow(r, p->powers[i] - 2) * exp(-p->alpha[i] * r2);
+        v += p->coeffs[i] * rm(pow(r, p->powers[i] - 2), 1) * rm(exp(-p->alpha[i] * r2), 2);
     return v;
 }
 
@@ -510,7 +541,7 @@ static double integrand_contracted(double r, int lambda, double CA, libgrpp_shel
     double F = 0.0, d2 = (r - CA) * (r - CA);
     for (int i = 0; i < g->num_primitives; i++) {
         double k = 2.0 * g->alpha[i] * CA;
-        F += g->coeffs[i] * exp(-g->alpha[i] * d2) * orc_bessel_scaled(lambda, k * r);
+        F += g->coeffs[i] * rm(exp(-g->alpha[i] * d2), 3) * rm(orc_bessel_scaled(lambda, k * r), 4);
     }
     return F;
 }
@@ -518,12 +549,12 @@ static double integrand_contracted(double r, int lambda, double CA, libgrpp_shel
 static void r2grid_point(r2grid_t *g, int idx, int i, int nr)
 {
     const double R = 5.0, R3 = R * R * R;
-    double xi = i / (nr + 1.0), xi3 = xi * xi * xi, ln = log(1 - xi3);
+    double xi = i / (nr + 1.0), xi3 = xi * xi * xi, ln = rm(log(1 - xi3), 5);
     double wi = 3 * R3 * xi * xi * ln * ln / ((1 - xi3) * (nr + 1.0)), ri = -R * ln;
     g->r[idx] = ri;
     g->w[idx] = wi;
     g->u[idx] = libgrpp_potential_value(g->pot, ri);
-    for (int n = 0; n <= g->nmax; n++) g->rN[n][idx] = pow(ri, n);
+    for (int n = 0; n <= g->nmax; n++) g->rN[n][idx] = rm(pow(ri, n), 6);
     for (int l = 0; l <= g->l1max; l++) g->F1[l][idx] = integrand_contracted(ri, l, g->CA, g->bra);
     for (int l = 0; l <= g->l2max; l++) g->F2[l][idx] = integrand_contracted(ri, l, g->CB, g->ket);
     orc_stats.grid_points++;
@@ -591,6 +622,7 @@ static int scr_prim(int l1, int l2, int n, double CA2, double CB2, double aA, do
     *val = sqrt(M_PI / p) * pow(r0, n) * orc_bessel_scaled(l1, k1 * r0) * orc_bessel_scaled(l2, k2 * r0) *
            exp(-eta * r0 * r0 - aA * (r0 - CA) * (r0 - CA) - aB * (r0 - CB) * (r0 - CB)) * 0.5 *
            (1 + erf(sqrt(p) * r0));
+    *val = rm(*val, 7);
     return 0;
 }
 

@@ -3,6 +3,7 @@
 Run here, where the reference tree exists:
 
     python tests/golden/make_full.py [--ref-root <libgrpp source tree>]   (default: $LIBGRPP_REFERENCE)
+    python tests/golden/make_full.py --truth-only [--only ThO UO2 KCs]   (redo the truth selection only)
 
 For test/ThO, test/UO2 and test/KCs the molecule, basis and GRPP inputs are read with
 libgrpp_b200.formats (the C driver's shell and centre order, test_libgrpp_c/main.c:196-254)
@@ -17,11 +18,12 @@ ThO and UO2 matrices to 1e-13. The shipped KCs matrices come from libgrpp's Fort
 calls; one of its arep elements sits 2.1e-10 from the C path. On some elements libgrpp
 keeps few digits: i-shell pairs on Th with the O potential 3.7 bohr away carry errors up
 to 8e-7 against the exact value in libgrpp's own result, from cancellation in the binomial
-re-centring sum. Those elements are found by running libgrpp on the inputs and on thirty
-copies moved by a few units in the last place; for each element where a run lands more than
+re-centring sum. Those elements are found by running libgrpp on the inputs and on copies
+moved by a few units in the last place, and the oracle under its rounding model (last-bit
+changes of exp, log, pow and Bessel values); for each element where a run lands more than
 an eighth of the tolerance from the shipped value, the fixture holds the binary128 value
 (oracle/truth_quad.c, summed over the element's tasks) as truth_<comp>[truth_idx], and
-refdev_<comp>, the largest distance from it of the shipped value and of the 31 runs.
+refdev_<comp>, the largest distance from it of the shipped value and of the runs.
 """
 from __future__ import annotations
 
@@ -36,7 +38,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from libgrpp_b200.formats import read_lower_triangle, read_system  # noqa: E402
-from tests.util import (REFDEV_MODES, assemble_lower, full_system, load_ref, perturbed,  # noqa: E402
+from tests.util import (assemble_lower, full_system, load_oracle, load_ref, perturbed, rounding_runs,  # noqa: E402
                         strict_tol, truth_full_batch)
 
 COMPS = ("arep", "so_x", "so_y", "so_z")
@@ -45,8 +47,18 @@ COMPS = ("arep", "so_x", "so_y", "so_z")
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default=os.environ.get("LIBGRPP_REFERENCE", "/root/reference"))
+    ap.add_argument("--truth-only", action="store_true", help="keep the shipped matrices on disk, redo the truth")
+    ap.add_argument("--only", nargs="*", help="subset of ThO UO2 KCs")
     args = ap.parse_args()
-    for name in ("ThO", "UO2", "KCs"):
+    if args.truth_only:
+        for name in args.only or ("ThO", "UO2", "KCs"):
+            out = os.path.join(HERE, f"full_{name.lower()}.npz")
+            z = np.load(out)
+            data = {k: z[k] for k in z.files if not k.startswith(("truth_", "refdev_"))}
+            np.savez_compressed(out, **data)
+            add_truth(out, int(z["n_basis"]))
+        return
+    for name in args.only or ("ThO", "UO2", "KCs"):
         d = os.path.join(args.ref_root, "test", name)
         S = read_system(d)
         b = S.batch(np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32))
@@ -65,19 +77,26 @@ def main():
               f"{os.path.relpath(out, ROOT)} ({os.path.getsize(out) / 1e6:.1f} MB)")
 
 
+FULL_INPUT_MODES = (1, 2, 3, 4)  # input perturbations of libgrpp's runs (tests.util.perturbed)
+
+
 def add_truth(path, n):
-    """Truth for the elements on which libgrpp keeps few digits: those where libgrpp's C path,
-    run on the inputs and on thirty copies moved by a few units in the last place
-    (tests.util.perturbed, REFDEV_MODES), lands more than an eighth of the tolerance from the
-    shipped value."""
+    """Truth for the elements on which libgrpp keeps few digits: those where a run of libgrpp's
+    algorithm lands more than an eighth of the tolerance from the shipped value. The runs are
+    libgrpp's C path on the inputs and on copies moved by a few units in the last place
+    (tests.util.perturbed, FULL_INPUT_MODES), and the oracle under its rounding model (last-bit
+    changes of exp, log, pow and Bessel values: another implementation's arithmetic,
+    tests.util.rounding_runs)."""
     name = os.path.basename(path)[5:-4]
     batch, z = full_system(name)
     ns = int(z["n_shells"])
     lib = load_ref()
     nt = os.cpu_count()
     runs = [assemble_lower(batch, lib.driver_full_batch(batch, nthreads=nt), ns)]
-    for mode in REFDEV_MODES:
+    for mode in FULL_INPUT_MODES:
         runs.append(assemble_lower(batch, lib.driver_full_batch(perturbed(batch, mode), nthreads=nt), ns))
+    for r in rounding_runs(load_oracle(), batch, nt):
+        runs.append(assemble_lower(batch, r, ns))
     sens = np.zeros(len(runs[0][0]), dtype=bool)
     for m, c in enumerate(COMPS):
         tol = strict_tol(z["shipped_" + c])

@@ -1,9 +1,9 @@
-"""Extended-precision truth for the ill-conditioned elements of the synthetic fixtures.
+"""Extended-precision truth for the ill-conditioned elements of the fixtures.
 
 Run here, after make_golden.py (needs oracle/_ref, libgrpp compiled from its sources):
 
     make -C oracle oracle ref
-    python tests/golden/make_truth.py [--only config1 config1_moderate config2 config3]
+    python tests/golden/make_truth.py [--only config1 config1_moderate config2 h2o cs kcs tho uo2 config3]
 
 On the synthetic workloads (exponents up to 5e3 on f..h shells, potential centres
 up to tens of bohr away) libgrpp keeps few or no significant digits on some blocks:
@@ -15,13 +15,17 @@ blocks, the value libgrpp's formulas converge to, with oracle/truth_quad.c
 thresholds), and records how far libgrpp itself is from it.
 
 Per fixture, written to tests/golden/truth_<name>.npz:
-  tasks              fixture task indices evaluated (config1, config2): every task
-                     with an element whose reference spread env exceeds 1/8 of the
-                     strict tolerance max(1e-10, 1e-9 |ref|)
+  tasks              fixture task indices evaluated: every task with an element
+                     whose spread exceeds 1/8 of the strict tolerance
+                     max(1e-10, 1e-9 |ref|), the spread being libgrpp's change under
+                     last-bit input changes (env) or the oracle's under its rounding
+                     model (last-bit changes of exp, log, pow and Bessel values,
+                     tests/util.py rounding_runs); tasks already on disk are kept
   truth_<comp>       binary128 blocks of those tasks, rounded to double
-  refdev_<comp>      max over the reference run and its thirty perturbed re-runs
-                     (tests/util.py REFDEV_MODES) of |ref_p - truth|: how far
-                     libgrpp itself lands from the exact value
+  refdev_<comp>      max of |x - truth| over libgrpp's run, its thirty perturbed
+                     re-runs (tests/util.py REFDEV_MODES) and the oracle's
+                     rounding-model runs: how far implementations of libgrpp's
+                     algorithm in double precision land from the exact value
   truthdev_<comp>    max over two perturbed inputs (modes 3, 4) of
                      |truth_p - truth|: the exact value's own sensitivity to the
                      same input changes (small: the loss of digits is in the
@@ -32,7 +36,7 @@ config3 (density-contracted gradient, all tasks): truth_grad [4, n_atoms, 3] fro
 the binary128 blocks of the differentiated shell pairs (L+1 with 2a N_L/N_{L+1},
 L-1 with N_L/N_{L-1}, libgrpp/diff_gaussian.c:35-63) contracted with D under
 libgrpp's atom and sign rule (libgrpp/grpp_integrals_gradient.c:280-393), and
-refdev_grad, the oracle's own distance from it over the same eleven runs (the
+refdev_grad, the oracle's own distance from it over the same runs and its rounding-model runs (the
 config3 reference values are the oracle's: the compiled libgrpp gradient reads
 outside its L-1 block and can return NaN).
 """
@@ -51,52 +55,92 @@ sys.path.insert(0, ROOT)
 
 from libgrpp_b200.gradient import derivative_batch, gradient_terms  # noqa: E402
 from libgrpp_b200.system import cartesian_list, ncart  # noqa: E402
-from tests.util import (COMPS, ENV_MODES, REFDEV_MODES, fixture_subset, load_fixture, load_oracle, load_ref,  # noqa: E402
-                        perturbed, strict_tol, system_from_fixture, truth_full_batch)
+from tests.util import (COMPS, REFDEV_MODES, fixture_subset, load_fixture, load_oracle, load_ref, perturbed,  # noqa: E402
+                        rounding_runs, strict_tol, system_from_fixture, truth_full_batch)
 
 U = 2.0 ** -53
 
 
-def flagged_tasks(batch, z):
+def flagged_tasks(batch, z, rm_spread):
+    """Tasks with an element on which libgrpp keeps few digits: its input-perturbation spread
+    env, or the spread of the oracle's rounding-model runs, exceeds 1/8 of the strict tolerance."""
     off = batch.block_offsets()
     flag = set()
-    for c in COMPS:
-        bad = np.where(z["env_" + c] > strict_tol(z["ref_" + c]) / 8)[0]
+    for m, c in enumerate(COMPS):
+        tol = strict_tol(z["ref_" + c]) / 8
+        bad = np.where((z["env_" + c] > tol) | (rm_spread[m] > tol))[0]
         flag |= set(int(t) for t in np.searchsorted(off, bad, side="right") - 1)
     return sorted(flag)
 
 
-def make_blocks(name, ref_lib, nthreads, refdev_only=False):
-    """Truth of the flagged tasks of a fixture; with refdev_only, the truth already on disk is
-    kept and only libgrpp's distances from it are recomputed."""
+def sub_elements(batch, idx):
+    off = batch.block_offsets()
+    return np.concatenate([np.arange(off[t], off[t + 1]) for t in idx]).astype(np.int64) if len(idx) else \
+        np.zeros(0, np.int64)
+
+
+def make_blocks(name, ref_lib, orc, nthreads):
+    """Truth of the flagged tasks of a fixture (reusing the truth of tasks already on disk) and
+    libgrpp's distances from it."""
     batch, z = load_fixture(name)
     out = os.path.join(HERE, f"truth_{name}.npz")
-    if refdev_only:
-        old = np.load(out)
-        idx = [int(t) for t in old["tasks"]]
-        sub, _, _ = fixture_subset(batch, z, idx)
-        truth = [old["truth_" + c] for c in COMPS]
-        level, resid = old["level"], old["resid"]
-        truthdev = [old["truthdev_" + c] for c in COMPS]
-    else:
-        idx = flagged_tasks(batch, z)
-        sub, _, _ = fixture_subset(batch, z, idx)
-        t = time.time()
-        truth, level, resid = truth_full_batch(sub, nthreads=nthreads)
-        print(f"{name}: {len(idx)} tasks, truth in {time.time() - t:.0f} s, deepest level {level.max()}, "
-              f"worst residual {resid.max():.1e}")
-        truthdev = [np.zeros_like(x) for x in truth]
+    obase = orc.driver_full_batch(batch, nthreads=nthreads)
+    rm = rounding_runs(orc, batch, nthreads)
+    rm_spread = [np.max([np.abs(r[m] - obase[m]) for r in rm], axis=0) for m in range(4)]
+    idx = flagged_tasks(batch, z, rm_spread)
+    old = np.load(out) if os.path.exists(out) else None
+    have = {int(t): k for k, t in enumerate(old["tasks"])} if old is not None else {}
+    idx = sorted(set(idx) | set(have))
+    if not idx:
+        print(f"{name}: no task with an ill-conditioned element")
+        if os.path.exists(out):
+            os.remove(out)
+        return
+    sub, _, _ = fixture_subset(batch, z, idx)
+    soff = sub.block_offsets()
+    new = [t for t in idx if t not in have]
+    truth = [np.zeros(int(soff[-1])) for _ in range(4)]
+    truthdev = [np.zeros(int(soff[-1])) for _ in range(4)]
+    level = np.zeros(len(idx), np.int32)
+    resid = np.zeros(len(idx))
+    if old is not None:
+        oo = fixture_subset(batch, z, [int(x) for x in old["tasks"]])[0].block_offsets()
+        for t in [t for t in idx if t in have]:
+            k = idx.index(t)
+            o = have[t]
+            for m, c in enumerate(COMPS):
+                truth[m][soff[k]:soff[k + 1]] = old["truth_" + c][oo[o]:oo[o + 1]]
+                truthdev[m][soff[k]:soff[k + 1]] = old["truthdev_" + c][oo[o]:oo[o + 1]]
+            level[k], resid[k] = old["level"][o], old["resid"][o]
+    if new:
+        nsub, _, _ = fixture_subset(batch, z, new)
+        noff = nsub.block_offsets()
+        t0 = time.time()
+        tn, ln, rn = truth_full_batch(nsub, nthreads=nthreads)
+        tds = [np.zeros_like(x) for x in tn]
         for mode in (3, 4):
-            tp, _, _ = truth_full_batch(perturbed(sub, mode), nthreads=nthreads)
+            tp, _, _ = truth_full_batch(perturbed(nsub, mode), nthreads=nthreads)
             for m in range(4):
-                truthdev[m] = np.maximum(truthdev[m], np.abs(tp[m] - truth[m]))
+                tds[m] = np.maximum(tds[m], np.abs(tp[m] - tn[m]))
+        print(f"{name}: truth of {len(new)} new tasks in {time.time() - t0:.0f} s")
+        for j, t in enumerate(new):
+            k = idx.index(t)
+            for m in range(4):
+                truth[m][soff[k]:soff[k + 1]] = tn[m][noff[j]:noff[j + 1]]
+                truthdev[m][soff[k]:soff[k + 1]] = tds[m][noff[j]:noff[j + 1]]
+            level[k], resid[k] = ln[j], rn[j]
     base = ref_lib.driver_full_batch(sub, nthreads=nthreads)
     refdev = [np.abs(base[m] - truth[m]) for m in range(4)]
     for mode in REFDEV_MODES:
         p = ref_lib.driver_full_batch(perturbed(sub, mode), nthreads=nthreads)
         for m in range(4):
             refdev[m] = np.maximum(refdev[m], np.abs(p[m] - truth[m]))
+    el = sub_elements(batch, idx)
+    for r in rm:
+        for m in range(4):
+            refdev[m] = np.maximum(refdev[m], np.abs(r[m][el] - truth[m]))
     data = dict(tasks=np.array(idx, dtype=np.int32), level=level, resid=resid)
+    print(f"{name}: {len(idx)} tasks with an ill-conditioned element, deepest level {level.max()}")
     for m, c in enumerate(COMPS):
         data["truth_" + c] = truth[m]
         data["refdev_" + c] = refdev[m]
@@ -171,6 +215,8 @@ def make_gradient(nthreads, refdev_only=False):
     import copy
     orc = load_oracle()
     refdev = np.abs(orc.driver_grad_contract(S, batch, D, nthreads=nthreads) - g)
+    for r in rounding_runs(orc, batch, nthreads, grad=(S, D)):
+        refdev = np.maximum(refdev, np.abs(r - g))
     for mode in REFDEV_MODES:
         sp = copy.copy(S)
         if mode == 2:
@@ -187,16 +233,17 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*")
     ap.add_argument("--threads", type=int, default=0)
-    ap.add_argument("--refdev-only", action="store_true", help="keep the truth on disk, recompute libgrpp's distances")
+    ap.add_argument("--refdev-only", action="store_true", help="config3: keep the truth on disk, recompute the distances")
     args = ap.parse_args()
     ref = load_ref()
     if ref is None:
         raise SystemExit("oracle/_ref/libgrpp_ref.so is not built (make -C oracle ref)")
-    for name in ("config1", "config1_moderate", "config2"):
+    orc = load_oracle()
+    for name in ("config1", "config1_moderate", "config2", "h2o", "cs", "kcs", "tho", "uo2"):
         if not args.only or name in args.only:
-            make_blocks(name, ref, args.threads, args.refdev_only)
+            make_blocks(name, ref, orc, args.threads or os.cpu_count())
     if not args.only or "config3" in args.only:
-        make_gradient(args.threads, args.refdev_only)
+        make_gradient(args.threads or os.cpu_count(), args.refdev_only)
 
 
 if __name__ == "__main__":

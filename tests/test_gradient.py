@@ -35,21 +35,32 @@ def test_gradient_contract_matches_oracle(gpu_lib, mode):
 
 def test_symmetric_density_folding(gpu_lib):
     """libgrpp_b200_grpp_gradient_contract_symmetric: shell pairs folded onto A <= B and no
-    spin-orbit work. The arep gradient equals the unfolded one (and the truth where the oracle
-    keeps few digits), the spin-orbit gradient is the exact zero the unfolded one approximates."""
+    spin-orbit work. On the config3 fixture (a partial task list) the arep gradient equals the
+    oracle's (and the truth where the oracle keeps few digits) and the spin-orbit gradient
+    receives nothing. On a system with every ordered shell pair listed, the unfolded spin-orbit
+    contractions, whose exact value is zero for a symmetric density (the SO matrices are
+    antisymmetric), are rounding noise, and the folded arep gradient equals the unfolded one."""
     batch, z = load_fixture("config3")
     S = system_from_fixture(z)
     truth = load_truth("config3")
-    full = gpu_lib.grad_contract(S, batch, z["D"])
     sym = gpu_lib.grad_contract(S, batch, z["D"], symmetric=True)
     tr = {"truth_grad": truth["truth_grad"][0].ravel(), "refdev_grad": truth["refdev_grad"][0].ravel()}
     ok, rep = truth_parity(sym[0].ravel(), z["ref_grad"][0].ravel(), tr, np.arange(sym[0].size), "grad")
     assert ok, rep
     assert np.all(sym[1:] == 0.0)
+    S2 = _small_system()
+    b2 = S2.batch()  # every ordered shell pair x every centre
+    n = int(S2.basis_offsets()[-1])
+    D = np.random.default_rng(5).uniform(-1, 1, (n, n))
+    D = 0.5 * (D + D.T)
+    full = gpu_lib.grad_contract(S2, b2, D)
+    sym2 = gpu_lib.grad_contract(S2, b2, D, symmetric=True)
     scale = np.abs(full[0]).max()
-    assert np.all(np.abs(full[1:]) <= 1e-10 * scale)  # the unfolded SO contractions are rounding noise
-    print(f"folded vs unfolded arep gradient: max abs {np.abs(sym[0] - full[0]).max():.2e} (max |g| {scale:.2e}); "
-          f"unfolded SO max {np.abs(full[1:]).max():.2e}")
+    print(f"complete pair list: folded vs unfolded arep gradient max abs {np.abs(sym2[0] - full[0]).max():.2e} "
+          f"(max |g| {scale:.2e}); unfolded SO max {np.abs(full[1:]).max():.2e}")
+    assert np.all(np.abs(full[1:]) <= 1e-10 * scale)
+    assert np.all(sym2[1:] == 0.0)
+    assert np.all(np.abs(sym2[0] - full[0]) <= 1e-10 * scale)
 
 
 def _small_system(shift=None):

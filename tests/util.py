@@ -170,6 +170,33 @@ ENV_MODES = (1, 2) + tuple(range(3, 11))  # two uniform and eight independent ra
 REFDEV_MODES = (1, 2) + tuple(range(3, 31))
 
 
+# seeds of the oracle's rounding model (orc_set_rounding_model in oracle/orc_integrals.c): runs of
+# libgrpp's algorithm whose transcendental results and Bessel values differ from libgrpp's in the
+# last bit, as any other implementation's (a GPU's exp, regenerated tables) do
+ROUNDING_SEEDS = tuple(range(1, 7))
+
+
+def rounding_runs(oracle, batch: BatchArrays, nthreads=0, seeds=ROUNDING_SEEDS, grad=None):
+    """The oracle's full-GRPP blocks (or, with grad=(system, D), its density-contracted gradient)
+    under each seed of the rounding model; the model is switched off afterwards."""
+    import ctypes as ct
+    f = oracle.lib.orc_set_rounding_model
+    f.argtypes = [ct.c_uint64]
+    f.restype = None
+    nthreads = nthreads or os.cpu_count()
+    out = []
+    try:
+        for seed in seeds:
+            f(seed)
+            if grad is None:
+                out.append(oracle.driver_full_batch(batch, nthreads=nthreads))
+            else:
+                out.append(oracle.driver_grad_contract(grad[0], batch, grad[1], nthreads=nthreads))
+    finally:
+        f(0)
+    return out
+
+
 def envelope(lib, batch: BatchArrays, base=None, nthreads=8, modes=ENV_MODES):
     """Per-element sensitivity of a CPU library's result to last-bit input changes:
     max over the perturbations of |result(perturbed) - result|."""
