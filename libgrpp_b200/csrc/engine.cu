@@ -543,7 +543,8 @@ struct Plan {
     OcProjArgs ocp;
     int ocp_blocks = 0;
     RadialArgs rad;
-    int rad_blocks = 0, scr_blocks = 0;
+    int rad_blocks = 0, scr_blocks = 0, scru_blocks = 0;
+    size_t scru_smem = 0;
     double *wu = nullptr;  // w U_p(r) table (scratch), filled by wu_table_kernel before the walk
     int wu_grpps = 0, wu_blocks = 0;
     double *ftab = nullptr;  // F_l(r) tables per (shell, centre) pair (scratch), ftab_kernel
@@ -751,6 +752,11 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         return idx;
     };
     int64_t qtot = 0, utot = 0, rad_list_max = 0;
+    // screening runs: long runs of one (task, potential) to the unit kernel, short ones (and
+    // one-centre tasks) to the flat kernel
+    std::vector<ScrUnit> scr_big, scr_small;
+    std::vector<int64_t> su_off(1, 0);
+    int scr_lw = 2;
     std::vector<int2> ucls((kMaxL + 1) * (kMaxL + 1) * (kMaxL + 1), int2{0, 0});
     std::vector<uint8_t> ucls_set(ucls.size(), 0);
     std::vector<uint16_t> ulist;
@@ -782,9 +788,20 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
             rad_uoff.push_back(utot);
             int e = 0, Lmx = 0;
             int64_t item_used = 0;
+            double CA2 = 0.0, CB2 = 0.0;
+            for (int d = 0; d < 3; d++) {
+                const double u = b->centre_origin[3 * C + d] - b->shell_origin[3 * A + d];
+                const double v = b->centre_origin[3 * C + d] - b->shell_origin[3 * B + d];
+                CA2 += u * u;
+                CB2 += v * v;
+            }
+            const bool one_centre = CA2 < 1e-14 && CB2 < 1e-14;
+            const int item = (int)rad_task.size() - 1;
             for (int i = 0; i < g_sl_n[g]; i++) {
-                const int L = p_L[sl_pot[g_sl_off[g] + i]];
+                const int pot = sl_pot[g_sl_off[g] + i];
+                const int L = p_L[pot];
                 Lmx = std::max(Lmx, L);
+                const int pe = e;
                 e += (L + la + 1) * (L + lb + 1) * (la + lb + 1);
                 const int key = (L * (kMaxL + 1) + la) * (kMaxL + 1) + lb;
                 if (!ucls_set[key]) {
@@ -792,6 +809,17 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
                     ucls[key] = int2{(int)ulist.size(), (int)u.size()};
                     ulist.insert(ulist.end(), u.begin(), u.end());
                     ucls_set[key] = 1;
+                }
+                const int ne = ucls[key].y;
+                if (one_centre || ne < kScrUnitMin) {
+                    if (ne > 0) {
+                        scr_small.push_back(ScrUnit{item, pot, pe, ucls[key].x, ne});
+                        su_off.push_back(su_off.back() + ne);
+                    }
+                } else {
+                    for (int o = 0; o < ne; o += kScrUnitThreads)
+                        scr_big.push_back(ScrUnit{item, pot, pe, ucls[key].x + o, std::min(kScrUnitThreads, ne - o)});
+                    scr_lw = std::max(scr_lw, L + std::max(la, lb) + 1);
                 }
                 utot += ucls[key].y;
                 item_used += ucls[key].y;
@@ -829,6 +857,15 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
                 (side ? proj_b : proj_a)[t] = idx;
             }
         }
+    }
+    // long screening runs, costliest first (entries x primitive triples), so the static
+    // round-robin over blocks ends evenly
+    {
+        auto cost = [&](const ScrUnit &u) {
+            const int t = rad_task[u.item];
+            return (int64_t)u.ne * rp_n[ta[t]] * rp_n[tb[t]] * p_n[u.pot];
+        };
+        std::stable_sort(scr_big.begin(), scr_big.end(), [&](const ScrUnit &x, const ScrUnit &y) { return cost(x) > cost(y); });
     }
     // outercore projection blocks
     std::vector<int> blk_shell, blk_oc;
@@ -1018,7 +1055,8 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     const size_t o_ta = pk.add(ta), o_tb = pk.add(tb), o_tc = pk.add(tc), o_too = pk.add(out_off), o_thul = pk.add(has_ul),
                  o_tqo = pk.add(q_off), o_tpa = pk.add(proj_a), o_tpb = pk.add(proj_b);
     const size_t o_items = pk.add(items), o_rt = pk.add(rad_task), o_rq = pk.add(rad_qoff), o_ru = pk.add(rad_uoff),
-                 o_ucls = pk.add(ucls), o_ulist = pk.add(ulist);
+                 o_ucls = pk.add(ucls), o_ulist = pk.add(ulist), o_sbig = pk.add(scr_big), o_ssmall = pk.add(scr_small),
+                 o_suo = pk.add(su_off);
     const size_t o_bs = pk.add(blk_shell), o_bo = pk.add(blk_oc), o_bco = pk.add(blk_cart_off), o_bso = pk.add(blk_sph_off),
                  o_poffp = pk.add(proj_off), o_msch = pk.add(mmd_sched);
     const size_t o_fps = pk.add(fp_shell), o_fpc = pk.add(fp_centre), o_fpl = pk.add(fp_lmax), o_fpo = pk.add(fp_off),
@@ -1195,6 +1233,13 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         r.n_used = utot;
         r.ucls = at<int2>(ib, o_ucls);
         r.ulist = at<uint16_t>(ib, o_ulist);
+        r.scr_units = at<ScrUnit>(ib, o_sbig);
+        r.n_scr_units = (int)scr_big.size();
+        r.scr_lw = scr_lw;
+        r.su = at<ScrUnit>(ib, o_ssmall);
+        r.su_off = at<int64_t>(ib, o_suo);
+        r.n_su = (int)scr_small.size();
+        r.n_su_entries = su_off.back();
         r.Q = Qd;
         r.S_prev = Spd;
         r.scr = SCd;
@@ -1239,7 +1284,11 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
         P.rad_blocks = (int)std::min<int64_t>((int64_t)rad_task.size(), (int64_t)nsm * 16);
         int scr_occ = 0;
         GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&scr_occ, radial_screen_flat_kernel, kRadThreads, 0));
-        P.scr_blocks = (int)std::min<int64_t>((utot + kRadThreads - 1) / kRadThreads, (int64_t)nsm * std::max(scr_occ, 1));
+        P.scr_blocks = (int)std::min<int64_t>((su_off.back() + kRadThreads - 1) / kRadThreads, (int64_t)nsm * std::max(scr_occ, 1));
+        P.scru_smem = (size_t)2 * kScrChunk * scr_lw * sizeof(double);
+        int scru_occ = 0;
+        GRPP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&scru_occ, radial_screen_unit_kernel, kScrUnitThreads, P.scru_smem));
+        P.scru_blocks = (int)std::min<int64_t>((int64_t)scr_big.size(), (int64_t)nsm * std::max(scru_occ, 1));
         P.rad_smem = smem;
     }
 
@@ -1353,6 +1402,10 @@ int plan_launch(Plan &P)
     if (P.rad_blocks > 0) {
         GRPP_CUDA(cudaMemsetAsync(P.rad.walk, 0, (size_t)P.n_radial, s));
         GRPP_CUDA(cudaMemsetAsync(P.rad.eflag, 0, (size_t)P.n_entries, s));  // unread entries stay inactive
+        if (P.scru_blocks > 0) {
+            radial_screen_unit_kernel<<<P.scru_blocks, kScrUnitThreads, P.scru_smem, s>>>(P.rad);
+            GRPP_CUDA(cudaGetLastError());
+        }
         if (P.scr_blocks > 0) {
             radial_screen_flat_kernel<<<P.scr_blocks, kRadThreads, 0, s>>>(P.rad);
             GRPP_CUDA(cudaGetLastError());

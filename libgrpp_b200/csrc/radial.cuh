@@ -48,6 +48,14 @@ constexpr int kRadMaxEntries = 16384;
 // entry flag bits
 constexpr uint8_t kEntActive = 1, kEntScrOk = 2;
 
+// A run of used entries of one semilocal potential of one task, screened by one block of
+// radial_screen_unit_kernel (or, for short runs, by the flat kernel): item, potential index,
+// offset of the potential's (l1, l2, N) box within the item's table, offset of the run in ulist,
+// number of entries.
+struct ScrUnit {
+    int item, pot, pe, uo, ne;
+};
+
 struct RadialArgs {
     int n_items;
     int64_t n_entries;          // total entries of all items (flat screening)
@@ -89,6 +97,16 @@ struct RadialArgs {
     int64_t n_used;
     const int2 *ucls;
     const uint16_t *ulist;
+    // screening split: runs of at least kScrUnitMin entries go to radial_screen_unit_kernel
+    // (scr_units), the others to the flat kernel through su, with prefix entry offsets su_off
+    // (su_off null: the flat kernel covers every used entry of every item through u_off);
+    // scr_lw: orders 0..scr_lw-1 of the unit kernel's Bessel tables
+    const ScrUnit *scr_units;
+    int n_scr_units, scr_lw;
+    const ScrUnit *su;
+    const int64_t *su_off;
+    int n_su;
+    int64_t n_su_entries;
     double *Q;                  // table values (running sums during the walk)
     double *S_prev, *scr;       // per entry scratch, same indexing as Q
     uint8_t *eflag;             // per entry: kEntActive | kEntScrOk
@@ -263,6 +281,60 @@ __device__ __forceinline__ double bessel_scaled_1r(int n, double x)
     return sum * (0.5 * inv);
 }
 
+// Gaussian integral int_0^inf r^n exp(-p r^2) dr (screening.c:255-265): the
+// screening estimate of two s functions on the centre and the one-centre analytic table
+__device__ __forceinline__ double scr_gaussian_integral(int n, double p)
+{
+    if (n % 2 == 0) {
+        const int k = n / 2;
+        return dfact(2 * k - 1) / (pow(2.0, k + 1) * pow(p, k)) * sqrt(kPi / p);
+    }
+    const int k = (n - 1) / 2;
+    double f = 1.0;
+    for (int q = 2; q <= k; q++) f *= q;
+    return f / (2.0 * pow(p, k + 1));
+}
+
+// The envelope of screening.c:308-318 at the fixed point r0, with sqpi = sqrt(pi / p) and
+// sqp = sqrt(p). Every factor is finite and non-negative: a Gaussian factor that underflowed to
+// exactly 0 makes the product exactly 0, so the other factors are not needed; and 1 + erf(z) is
+// exactly 2 once erfc(z) < 2^-54 (z > 5.9), taken here as p r0^2 > 49 (z > 7). The product keeps
+// libgrpp's order (screening.c:333-338).
+__device__ __forceinline__ double scr_envelope(int l1, int l2, int n, double CA, double CB, double aA, double aB,
+                                               double eta, double p, double k1, double k2, double r0, double sqpi,
+                                               double sqp)
+{
+    const double e1 = r0 - CA, e2 = r0 - CB;
+    const double ex = exp(-eta * r0 * r0 - aA * e1 * e1 - aB * e2 * e2);
+    if (ex == 0.0) return 0.0;
+    const double z2 = p * r0 * r0;
+    const double erf_part = z2 > 49.0 ? 2.0 : 1 + erf(sqp * r0);
+    return sqpi * ipow(r0, n) * bessel_scaled_1r(l1, k1 * r0) * bessel_scaled_1r(l2, k2 * r0) * ex * 0.5 * erf_part;
+}
+
+// The fixed-point update of screening.c:329-362 from the Bessel ratio parts (n1/d1 = M_a/M_b of
+// side A at x1, n2/d2 of side B at x2): r0' = sqrt(s / (2p)),
+// s = M_a1/M_b1 x1 + M_a2/M_b2 x2 + n - (l1 + 1 if l1 > 0) - (l2 + 1 if l2 > 0),
+// the two ratios over one common denominator
+__device__ __forceinline__ double scr_update(int l1, int l2, int n, double n1, double d1, double n2, double d2,
+                                             double x1, double x2, double inv2p)
+{
+    double s = (n1 * x1 * d2 + n2 * x2 * d1) / (d1 * d2) + n;
+    if (l1 > 0) s = s - l1 - 1;
+    if (l2 > 0) s = s - l2 - 1;
+    return sqrt(s * inv2p);
+}
+
+// One fixed-point step from r0
+__device__ __forceinline__ double scr_step(int l1, int l2, int n, double k1, double k2, double inv2p, double r0)
+{
+    const double x1 = k1 * r0, x2 = k2 * r0;
+    double n1, d1, n2, d2;
+    scr_ratio_parts(l1, x1, n1, d1);
+    scr_ratio_parts(l2, x2, n2, d2);
+    return scr_update(l1, l2, n, n1, d1, n2, d2, x1, x2, inv2p);
+}
+
 // Primitive screening estimate (screening.c:243-318) with CA, CB as distances.
 // Returns true on failure (no fixed point in 4 steps). *iters: steps taken, negative
 // (-(steps)-1) when the envelope was evaluated.
@@ -275,17 +347,7 @@ __device__ __forceinline__ bool scr_prim_flat(int l1, int l2, int n, double CA, 
     if (l2 >= 1 && fabs(k2) <= kZeroThresh) return false;
     const double p = aA + aB + eta;
     if (l1 == 0 && l2 == 0 && fabs(k1) <= kZeroThresh && fabs(k2) <= kZeroThresh) {
-        double gi;
-        if (n % 2 == 0) {
-            const int k = n / 2;
-            gi = dfact(2 * k - 1) / (pow(2.0, k + 1) * pow(p, k)) * sqrt(kPi / p);
-        } else {
-            const int k = (n - 1) / 2;
-            double f = 1.0;
-            for (int q = 2; q <= k; q++) f *= q;
-            gi = f / (2.0 * pow(p, k + 1));
-        }
-        *val = exp(-aA * CA * CA - aB * CB * CB) * gi;
+        *val = exp(-aA * CA * CA - aB * CB * CB) * scr_gaussian_integral(n, p);
         return false;
     }
     // one reciprocal of p serves the start point, the fixed-point step and the envelope
@@ -300,57 +362,117 @@ __device__ __forceinline__ bool scr_prim_flat(int l1, int l2, int n, double CA, 
             return true;
         }
         r0p = r0;
-        const double x1 = k1 * r0, x2 = k2 * r0;
-        double n1, d1, n2, d2;
-        scr_ratio_parts(l1, x1, n1, d1);
-        scr_ratio_parts(l2, x2, n2, d2);
-        // M_a1/M_b1 x1 + M_a2/M_b2 x2 over one common denominator
-        double s = (n1 * x1 * d2 + n2 * x2 * d1) / (d1 * d2) + n;
-        if (l1 > 0) s = s - l1 - 1;
-        if (l2 > 0) s = s - l2 - 1;
-        r0 = sqrt(s * inv2p);
+        r0 = scr_step(l1, l2, n, k1, k2, inv2p, r0);
     } while (fabs(r0 - r0p) > 1e-2);
-    const double e1 = r0 - CA, e2 = r0 - CB;
     *iters = -steps - 1;
-    // every factor of the envelope is finite and non-negative: a Gaussian factor that
-    // underflowed to exactly 0 makes the product exactly 0, so the other factors are not
-    // needed; and 1 + erf(z) is exactly 2 once erfc(z) < 2^-54 (z > 5.9), taken here as
-    // p r0^2 > 49 (z > 7). The product keeps libgrpp's order (screening.c:333-338).
-    const double ex = exp(-eta * r0 * r0 - aA * e1 * e1 - aB * e2 * e2);
-    if (ex == 0.0) {
-        *val = 0.0;
-        return false;
-    }
-    const double z2 = p * r0 * r0;
-    const double erf_part = z2 > 49.0 ? 2.0 : 1 + erf(sqrt(p) * r0);
-    *val = sqrt(kPi * inv_p) * ipow(r0, n) * bessel_scaled_1r(l1, k1 * r0) * bessel_scaled_1r(l2, k2 * r0) * ex * 0.5 *
-           erf_part;
+    *val = scr_envelope(l1, l2, n, CA, CB, aA, aB, eta, p, k1, k2, r0, sqrt(kPi * inv_p), sqrt(p));
     return false;
 }
 
+// One-centre entry (CA = CB = 0): libgrpp's analytic table (radial_type2_integral.c:126-155),
+// only l1 = l2 = 0 non-zero
+__device__ double scr_one_centre_entry(const RadialArgs &a, int sa, int sb, int la, int lb, int l1, int l2, int N,
+                                       int nk, int po)
+{
+    if (l1 != 0 || l2 != 0) return 0.0;
+    const int na = __ldg(a.shell_nprim + sa), nb = __ldg(a.shell_nprim + sb);
+    const double *pca = a.prim_coef + __ldg(a.shell_prim_off + sa), *pxa = a.prim_alpha + __ldg(a.shell_prim_off + sa);
+    const double *pcb = a.prim_coef + __ldg(a.shell_prim_off + sb), *pxb = a.prim_alpha + __ldg(a.shell_prim_off + sb);
+    double v = 0.0;
+    for (int i = 0; i < na; i++) {
+        const double ci = __ldg(pca + i) * gaussian_norm(la, __ldg(pxa + i));
+        for (int j = 0; j < nb; j++) {
+            const double cj = __ldg(pcb + j) * gaussian_norm(lb, __ldg(pxb + j));
+            for (int k = 0; k < nk; k++) {
+                const double pp = __ldg(pxa + i) + __ldg(pxb + j) + __ldg(a.pot_alpha + po + k);
+                const double f = ci * cj * __ldg(a.pot_coef + po + k);
+                v += f * scr_gaussian_integral(__ldg(a.pot_powers + po + k) + N, pp);
+            }
+        }
+    }
+    return v;
+}
+
+// libgrpp's decision for a screened entry (radial_type2_integral.c:264-279): an estimate below
+// 1e-16 is the entry's value; otherwise the entry is walked, with forced refinement only when
+// the estimate is valid
+__device__ __forceinline__ void scr_store(const RadialArgs &a, int item, int64_t g, double sum, bool fail)
+{
+    a.scr[g] = sum;
+    if (!fail && fabs(sum) < 1e-16) {
+        a.Q[g] = sum;
+        a.eflag[g] = kEntScrOk;
+    } else {
+        a.Q[g] = 0.0;
+        a.eflag[g] = kEntActive | (fail ? 0 : kEntScrOk);
+        a.walk[item] = 1;
+    }
+}
+
 #ifndef GRPP_RADIAL_TABLES_ONLY
-// Screening of every (task, entry) of a batch, one thread per entry over the flattened
-// entry space (entries of one task are consecutive, tasks in item order): no per-task
-// barrier and no ragged last round. A thread follows screening.c:193-220 for its entry:
-// primitive triples (i, j, k) in libgrpp's order, stopping at the first failure. The
-// outcome per entry is written to Q (value if screened out), scr (estimate) and eflag;
-// walk[item] is set to 1 when any entry of the item needs the grid (walk[] is zeroed
-// by the host before the launch). One-centre tasks get their analytic table.
+// Screening of (task, entry) pairs, one thread per entry over a flattened entry space (entries
+// of one task are consecutive, tasks in item order): no per-task barrier and no ragged last
+// round. With a.su_off the space is the short runs of a.su (the long ones go to
+// radial_screen_unit_kernel); without it, every used entry of every item. A thread follows
+// screening.c:193-220 for its entry: primitive triples (i, j, k) in libgrpp's order, stopping at
+// the first failure. The outcome per entry is written to Q (value if screened out), scr
+// (estimate) and eflag; walk[item] is set to 1 when any entry of the item needs the grid (walk[]
+// is zeroed by the host before the launch). One-centre tasks get their analytic table.
 __global__ void __launch_bounds__(kRadThreads, GRPP_SCR_MINB) radial_screen_flat_kernel(RadialArgs a)
 {
     const int lane = threadIdx.x & 31;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const long long t0 = clock64();
     unsigned long long c_combo = 0, c_iter = 0, c_final = 0;
-    for (int64_t gu = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gu < a.n_used; gu += stride) {
-        int lo = 0, hi = a.n_items - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (__ldg(a.u_off + mid) <= gu) lo = mid;
-            else hi = mid - 1;
+    const int64_t n_flat = a.su_off ? a.n_su_entries : a.n_used;
+    for (int64_t gu = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gu < n_flat; gu += stride) {
+        int item, pot, e;
+        int64_t pe = 0;
+        if (a.su_off) {
+            int lo = 0, hi = a.n_su - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(a.su_off + mid) <= gu) lo = mid;
+                else hi = mid - 1;
+            }
+            const ScrUnit &U = a.su[lo];
+            item = U.item;
+            pot = U.pot;
+            pe = U.pe;
+            e = a.ulist[U.uo + (int)(gu - __ldg(a.su_off + lo))];
+        } else {
+            int lo = 0, hi = a.n_items - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(a.u_off + mid) <= gu) lo = mid;
+                else hi = mid - 1;
+            }
+            item = lo;
+            int ku = (int)(gu - __ldg(a.u_off + item));
+            const int t = __ldg(a.item_task + item);
+            const int sa = __ldg(a.task_a + t), sb = __ldg(a.task_b + t), c = __ldg(a.task_c + t);
+            const int la = __ldg(a.shell_L + sa), lb = __ldg(a.shell_L + sb), dn = la + lb + 1;
+            const int gr = __ldg(a.centre_grpp + c), npot = __ldg(a.grpp_sl_n + gr), slo = __ldg(a.grpp_sl_off + gr);
+            // libgrpp tabulates the whole (l1, l2, N) box of every potential, but its angular sums
+            // read only the entries with N = n1 + n2 (n1 <= la, n2 <= lb), l1 in [max(L-n1,0), L+n1]
+            // of the parity of L+n1, l2 likewise (type2_integrals.c:169-184,
+            // spin_orbit_integrals.c:189-204). Only those are screened and walked: the others cannot
+            // change an output, and every entry's walk and stop level are its own
+            // (radial_type2_integral.c:242-318). The host lists them per class (L, la, lb).
+            pot = -1;
+            e = 0;
+            for (int p = 0; p < npot; p++) {
+                pot = __ldg(a.sl_pot + slo + p);
+                const int Lp = __ldg(a.pot_L + pot);
+                const int2 cls = a.ucls[(Lp * (kMaxL + 1) + la) * (kMaxL + 1) + lb];
+                if (ku < cls.y) {
+                    e = a.ulist[cls.x + ku];
+                    break;
+                }
+                ku -= cls.y;
+                pe += (Lp + la + 1) * (Lp + lb + 1) * dn;
+            }
         }
-        const int item = lo;
-        int ku = (int)(gu - __ldg(a.u_off + item));
         const int t = __ldg(a.item_task + item);
         const int sa = __ldg(a.task_a + t), sb = __ldg(a.task_b + t), c = __ldg(a.task_c + t);
         const double *Ao = a.shell_origin + 3 * sa, *Bo = a.shell_origin + 3 * sb, *Co = a.centre_origin + 3 * c;
@@ -361,61 +483,13 @@ __global__ void __launch_bounds__(kRadThreads, GRPP_SCR_MINB) radial_screen_flat
             CB2 += v * v;
         }
         const int la = __ldg(a.shell_L + sa), lb = __ldg(a.shell_L + sb), dn = la + lb + 1;
-        const int gr = __ldg(a.centre_grpp + c), npot = __ldg(a.grpp_sl_n + gr), slo = __ldg(a.grpp_sl_off + gr);
-        // libgrpp tabulates the whole (l1, l2, N) box of every potential, but its angular sums
-        // read only the entries with N = n1 + n2 (n1 <= la, n2 <= lb), l1 in [max(L-n1,0), L+n1]
-        // of the parity of L+n1, l2 likewise (type2_integrals.c:169-184,
-        // spin_orbit_integrals.c:189-204). Only those are screened and walked: the others cannot
-        // change an output, and every entry's walk and stop level are its own
-        // (radial_type2_integral.c:242-318). The host lists them per class (L, la, lb).
-        int pot = -1, Lp = 0, e = 0;
-        int64_t pe = 0;
-        for (int p = 0; p < npot; p++) {
-            pot = __ldg(a.sl_pot + slo + p);
-            Lp = __ldg(a.pot_L + pot);
-            const int2 cls = a.ucls[(Lp * (kMaxL + 1) + la) * (kMaxL + 1) + lb];
-            if (ku < cls.y) {
-                e = a.ulist[cls.x + ku];
-                break;
-            }
-            ku -= cls.y;
-            pe += (Lp + la + 1) * (Lp + lb + 1) * dn;
-        }
+        const int Lp = __ldg(a.pot_L + pot);
         const int64_t g = __ldg(a.q_off + item) + pe + e;
         const int d2 = Lp + lb + 1;
         const int l1 = e / (d2 * dn), rem = e - l1 * d2 * dn, l2 = rem / dn, N = rem - l2 * dn;
         const int nk = __ldg(a.pot_nprim + pot), po = __ldg(a.pot_prim_off + pot);
         if (CA2 < 1e-14 && CB2 < 1e-14) {
-            // analytic one-centre entry (radial_type2_integral.c:126-155): only l1 = l2 = 0 is non-zero
-            double v = 0.0;
-            if (l1 == 0 && l2 == 0) {
-                const int na = __ldg(a.shell_nprim + sa), nb = __ldg(a.shell_nprim + sb);
-                const double *pca = a.prim_coef + __ldg(a.shell_prim_off + sa), *pxa = a.prim_alpha + __ldg(a.shell_prim_off + sa);
-                const double *pcb = a.prim_coef + __ldg(a.shell_prim_off + sb), *pxb = a.prim_alpha + __ldg(a.shell_prim_off + sb);
-                for (int i = 0; i < na; i++) {
-                    const double ci = __ldg(pca + i) * gaussian_norm(la, __ldg(pxa + i));
-                    for (int j = 0; j < nb; j++) {
-                        const double cj = __ldg(pcb + j) * gaussian_norm(lb, __ldg(pxb + j));
-                        for (int k = 0; k < nk; k++) {
-                            const double pp = __ldg(pxa + i) + __ldg(pxb + j) + __ldg(a.pot_alpha + po + k);
-                            const double f = ci * cj * __ldg(a.pot_coef + po + k);
-                            const int n = __ldg(a.pot_powers + po + k) + N;
-                            double gi;
-                            if (n % 2 == 0) {
-                                const int kk = n / 2;
-                                gi = dfact(2 * kk - 1) / (pow(2.0, kk + 1) * pow(pp, kk)) * sqrt(kPi / pp);
-                            } else {
-                                const int kk = (n - 1) / 2;
-                                double fct = 1.0;
-                                for (int q = 2; q <= kk; q++) fct *= q;
-                                gi = fct / (2.0 * pow(pp, kk + 1));
-                            }
-                            v += f * gi;
-                        }
-                    }
-                }
-            }
-            a.Q[g] = v;
+            a.Q[g] = scr_one_centre_entry(a, sa, sb, la, lb, l1, l2, N, nk, po);
             a.eflag[g] = 0;
             continue;
         }
@@ -449,15 +523,7 @@ __global__ void __launch_bounds__(kRadThreads, GRPP_SCR_MINB) radial_screen_flat
                 }
             }
         }
-        a.scr[g] = sum;
-        if (!fail && fabs(sum) < 1e-16) {
-            a.Q[g] = sum;
-            a.eflag[g] = kEntScrOk;
-        } else {
-            a.Q[g] = 0.0;
-            a.eflag[g] = kEntActive | (fail ? 0 : kEntScrOk);
-            a.walk[item] = 1;
-        }
+        scr_store(a, item, g, sum, fail);
     }
     if (a.counters) {
         unsigned long long v[3] = {c_combo, c_iter, c_final};
@@ -471,6 +537,189 @@ __global__ void __launch_bounds__(kRadThreads, GRPP_SCR_MINB) radial_screen_flat
         }
     }
 }
+
+// ---- screening of long runs: radial_screen_unit_kernel ----------------------------------------
+//
+// A block screens one run of entries of one (task, semilocal potential) (ScrUnit), a thread per
+// entry. Everything of a primitive triple (i, j, k) that does not depend on the entry
+// (l1, l2, N) is formed once per block, a triple per thread, kScrChunk triples at a time, into
+// shared memory: p = a_A + a_B + eta, 1/p, sqrt(pi/p), sqrt(p), k = 2 a C, the fixed point's start
+// r0 = (a_A CA + a_B CB)/p and its arguments x = k r0, and the Bessel parts of the first step for
+// every order 0..lw-1 of both sides (the first step's arguments do not depend on the entry).
+// Every entry then runs libgrpp's per-triple estimate (screening.c:193-220, 243-362) over the
+// staged triples in libgrpp's order, reading its first step from the tables: the same
+// expressions, operands and order as the flat kernel, so the estimates and gate decisions are
+// the same.
+constexpr int kScrUnitThreads = 64;  // threads per block = entries per run at most
+constexpr int kScrUnitMin = 16;      // runs with fewer entries stay in the flat kernel
+constexpr int kScrChunk = 64;        // primitive triples staged per round (one per thread)
+static_assert(kScrChunk == kScrUnitThreads, "one staged triple per thread");
+
+// Bessel parts of orders 0..n-1 at x, as scr_ratio_parts forms them: the value (x <= 16) or, above
+// x = 16, the asymptotic sum without its 1/(2x) factor (it cancels in the ratio of two orders)
+__device__ __forceinline__ void scr_parts_row(int n, double x, double *out)
+{
+    if (x <= 1e-7) {
+        for (int l = 0; l < n; l++) out[l] = bessel_small(l, x);
+    } else if (x <= 16.0) {
+        const int i0 = (int)(round(x * 100) + 1e-5);
+        const double dx = x - i0 * 0.01;
+        const double *row = c_tab.bessel + (size_t)i0 * kBesL * 5;
+        for (int l = 0; l < n; l++) out[l] = taylor4(row + 5 * l, dx);
+    } else {
+        const double ninv = -1.0 / x;
+        for (int l = 0; l < n; l++) {
+            const double *cl = c_tab.rfun + l * kRfunL;
+            double pw = 1.0, sum = 0.0;
+            for (int k = 0; k <= l; k++) {
+                sum += __ldg(cl + k) * pw;
+                pw *= ninv;
+            }
+            out[l] = sum;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kScrUnitThreads, 8) radial_screen_unit_kernel(RadialArgs a)
+{
+    extern __shared__ double ptab[];  // [kScrChunk][2][scr_lw]: Bessel parts, sides A and B
+    __shared__ double t_aA[kScrChunk], t_aB[kScrChunk], t_eta[kScrChunk], t_p[kScrChunk], t_ip[kScrChunk],
+        t_sqpi[kScrChunk], t_sqp[kScrChunk], t_k1[kScrChunk], t_k2[kScrChunk], t_r0[kScrChunk], t_x1[kScrChunk],
+        t_x2[kScrChunk], t_c[kScrChunk];
+    __shared__ int t_pw[kScrChunk];
+    const int tid = threadIdx.x, lane = tid & 31, lw = a.scr_lw;
+    const long long t0 = clock64();
+    unsigned long long c_combo = 0, c_iter = 0, c_final = 0;
+    for (int u = blockIdx.x; u < a.n_scr_units; u += gridDim.x) {
+        const int item = a.scr_units[u].item, pot = a.scr_units[u].pot, ne = a.scr_units[u].ne;
+        const int t = __ldg(a.item_task + item);
+        const int sa = __ldg(a.task_a + t), sb = __ldg(a.task_b + t), c = __ldg(a.task_c + t);
+        const double *Ao = a.shell_origin + 3 * sa, *Bo = a.shell_origin + 3 * sb, *Co = a.centre_origin + 3 * c;
+        double CA2 = 0.0, CB2 = 0.0;
+        for (int d = 0; d < 3; d++) {
+            const double uu = __ldg(Co + d) - __ldg(Ao + d), vv = __ldg(Co + d) - __ldg(Bo + d);
+            CA2 += uu * uu;
+            CB2 += vv * vv;
+        }
+        const int la = __ldg(a.shell_L + sa), lb = __ldg(a.shell_L + sb), dn = la + lb + 1;
+        const int Lp = __ldg(a.pot_L + pot), d2 = Lp + lb + 1;
+        const int nk = __ldg(a.pot_nprim + pot), po = __ldg(a.pot_prim_off + pot);
+        const bool have = tid < ne;
+        int l1 = 0, l2 = 0, N = 0;
+        int64_t g = 0;
+        if (have) {
+            const int e = a.ulist[a.scr_units[u].uo + tid];
+            g = __ldg(a.q_off + item) + a.scr_units[u].pe + e;
+            l1 = e / (d2 * dn);
+            const int rem = e - l1 * d2 * dn;
+            l2 = rem / dn;
+            N = rem - l2 * dn;
+        }
+        if (CA2 < 1e-14 && CB2 < 1e-14) {  // one-centre tasks are the flat kernel's; kept for safety
+            if (have) {
+                a.Q[g] = scr_one_centre_entry(a, sa, sb, la, lb, l1, l2, N, nk, po);
+                a.eflag[g] = 0;
+            }
+            continue;
+        }
+        const double CA = sqrt(CA2), CB = sqrt(CB2);
+        const int na = __ldg(a.rp_n + sa), nb = __ldg(a.rp_n + sb);
+        const double *ca = a.rp_coef + __ldg(a.rp_off + sa), *xa = a.rp_alpha + __ldg(a.rp_off + sa);
+        const double *cb = a.rp_coef + __ldg(a.rp_off + sb), *xb = a.rp_alpha + __ldg(a.rp_off + sb);
+        // orders of the first step's ratios (screening.c:329-346): (1, 0) for l = 0, else (l-1, l)
+        const int oa1 = l1 == 0 ? 1 : l1 - 1, ob1 = l1 == 0 ? 0 : l1, oa2 = l2 == 0 ? 1 : l2 - 1, ob2 = l2 == 0 ? 0 : l2;
+        const int nA = max(2, Lp + la + 1), nB = max(2, Lp + lb + 1);  // orders the run's entries can use
+        double sum = 0.0;
+        bool fail = !have;
+        const int T = na * nb * nk;
+        for (int c0 = 0; c0 < T; c0 += kScrChunk) {
+            const int nc = min(kScrChunk, T - c0);
+            __syncthreads();  // the previous round's tables are consumed
+            if (tid < nc) {
+                const int q = c0 + tid, i = q / (nb * nk), j = (q / nk) % nb, k = q % nk;
+                const double aA = __ldg(xa + i), aB = __ldg(xb + j), eta = __ldg(a.pot_alpha + po + k);
+                const double k1 = 2 * aA * CA, k2 = 2 * aB * CB;
+                const double p = aA + aB + eta, inv_p = 1.0 / p;
+                const double r0 = (aA * CA + aB * CB) * inv_p;
+                const double cij = __ldg(ca + i) * __ldg(cb + j);
+                t_aA[tid] = aA;
+                t_aB[tid] = aB;
+                t_eta[tid] = eta;
+                t_p[tid] = p;
+                t_ip[tid] = inv_p;
+                t_sqpi[tid] = sqrt(kPi * inv_p);
+                t_sqp[tid] = sqrt(p);
+                t_k1[tid] = k1;
+                t_k2[tid] = k2;
+                t_r0[tid] = r0;
+                t_x1[tid] = k1 * r0;
+                t_x2[tid] = k2 * r0;
+                t_c[tid] = cij * __ldg(a.pot_coef + po + k);
+                t_pw[tid] = __ldg(a.pot_powers + po + k);
+                scr_parts_row(nA, k1 * r0, ptab + (size_t)(2 * tid) * lw);
+                scr_parts_row(nB, k2 * r0, ptab + (size_t)(2 * tid + 1) * lw);
+            }
+            __syncthreads();
+            if (fail) continue;
+            for (int q = 0; q < nc; q++) {
+                const double k1 = t_k1[q], k2 = t_k2[q];
+                double v = 0.0;
+                int it = 0;
+                bool f = false;
+                if (!(l1 >= 1 && fabs(k1) <= kZeroThresh) && !(l2 >= 1 && fabs(k2) <= kZeroThresh)) {
+                    const int n = N + t_pw[q];
+                    const double p = t_p[q];
+                    if (l1 == 0 && l2 == 0 && fabs(k1) <= kZeroThresh && fabs(k2) <= kZeroThresh) {
+                        v = exp(-t_aA[q] * CA * CA - t_aB[q] * CB * CB) * scr_gaussian_integral(n, p);
+                    } else {
+                        const double inv2p = 0.5 * t_ip[q];
+                        const double *PA = ptab + (size_t)(2 * q) * lw, *PB = PA + lw;
+                        double r0p = t_r0[q];
+                        double r0 = scr_update(l1, l2, n, PA[oa1], PA[ob1], PB[oa2], PB[ob2], t_x1[q], t_x2[q], inv2p);
+                        int steps = 1;
+                        while (fabs(r0 - r0p) > 1e-2) {
+                            steps++;
+                            if (steps == 5) {
+                                f = true;
+                                break;
+                            }
+                            r0p = r0;
+                            r0 = scr_step(l1, l2, n, k1, k2, inv2p, r0);
+                        }
+                        if (f) {
+                            it = steps - 1;
+                        } else {
+                            it = steps;
+                            c_final++;
+                            v = scr_envelope(l1, l2, n, CA, CB, t_aA[q], t_aB[q], t_eta[q], p, k1, k2, r0, t_sqpi[q],
+                                             t_sqp[q]);
+                        }
+                    }
+                }
+                c_combo++;
+                c_iter += it;
+                if (f) {
+                    fail = true;
+                    break;
+                }
+                sum += t_c[q] * v;
+            }
+        }
+        if (have) scr_store(a, item, g, sum, fail);
+    }
+    if (a.counters) {
+        unsigned long long v[3] = {c_combo, c_iter, c_final};
+        for (int k = 0; k < 3; k++)
+            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+        if (lane == 0) {
+            atomicAdd(a.counters + kRadCntScrCombos, v[0]);
+            atomicAdd(a.counters + kRadCntScrIters, v[1]);
+            atomicAdd(a.counters + kRadCntScrFinal, v[2]);
+            atomicAdd(a.counters + kRadCntScreenCycles, (unsigned long long)(clock64() - t0));
+        }
+    }
+}
+
 #endif  // GRPP_RADIAL_TABLES_ONLY
 
 // decode entry index within an item -> (potential, l1, l2, N)
