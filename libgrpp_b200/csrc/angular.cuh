@@ -709,14 +709,14 @@ __global__ void __launch_bounds__(NT) final_kernel(FinalArgs a, FinalSmem sm)
                             // Both this sum and libgrpp's term-by-term sum of the same terms are within
                             // (n + 12) u sum|terms| of the exact value, n = the number of terms and 12 u the
                             // rounding of a term's factors; the two differ by at most twice that. The
-                            // factored result is kept when that bound, scaled by 16 pi^2, is below 1e-12
-                            // absolute or 1e-12 of the partial sum itself (1% of the 1e-10 / 1e-9 comparator);
-                            // otherwise, where the re-centring sum cancels, the element is summed term by
-                            // term in libgrpp's order.
+                            // factored result is kept when that worst-case bound, scaled by 16 pi^2, is below
+                            // 1e-11 absolute or 1e-10 of the partial sum itself (a tenth of the 1e-10 / 1e-9
+                            // comparator); otherwise, where the re-centring sum cancels, the element is summed
+                            // term by term in libgrpp's order.
                             const double nterm = (double)nta * (double)((bx + 1) * (by + 1) * (bz + 1));
                             const double bound = 2.0 * (nterm + 12.0) * 1.1102230246251565e-16 * ga * (16 * kPi * kPi);
                             const double gmax = fmax(fabs(g0), fmax(fabs(g1), fabs(g2)));
-                            if (bound <= fmax(1e-12, 1e-12 * gmax * (16 * kPi * kPi))) {
+                            if (bound <= fmax(1e-11, 1e-10 * gmax * (16 * kPi * kPi))) {
                                 gam[0][q] += g0;
                                 gam[1][q] += g1;
                                 gam[2][q] += g2;

@@ -348,8 +348,8 @@ static std::vector<int> order_by_cost(const std::vector<double> &cost)
 // terms or not); the layout holds the task's RSH rows, both sides' omega tables, its radial
 // table, the V rows of one potential (all rows when they fit in 6144 values) and W of the
 // factored re-centring sum. W holds ncart(lb) x rows x (components + 1) values (the sums and the
-// sums of absolute terms) and rows is chosen so that nabB x rows x components fits in V, so a W
-// twice as large as V always suffices.
+// sums of absolute terms), rows chosen by the kernel so that nabB x rows x components fits in V;
+// its size is set per launch group from the group's tasks.
 static int fin_class_key(int la, int lb, int Lmax, bool so) { return ((la * 16 + lb) * 16 + Lmax) * 2 + (so ? 1 : 0); }
 
 static int fin_default_nt(int la, int lb)
@@ -367,7 +367,7 @@ static FinalSmem fin_layout(int lam, int n_omega, int n_q, int nabA, int nabB, i
     fs.n_q = n_q;
     fs.n_v = std::min(6144, std::max(nabA * nabB * ncomp, 3 * std::max(nabA, nabB)));
     fs.n_v = std::max(fs.n_v, 3 * std::max(nabA, nabB));
-    fs.n_w = 2 * fs.n_v;
+    fs.n_w = 0;  // set per launch group
     return fs;
 }
 
@@ -448,6 +448,14 @@ std::vector<uint16_t> used_entries(int L, int la, int lb)
                 }
                 if (used) out.push_back((uint16_t)((l1 * d2 + l2) * dn + N));
             }
+    // screening order: the lanes of a warp take consecutive entries, and an entry's work grows
+    // with l1 and with l2 (the Bessel sums of either side); tiles of 2 x 2 orders keep both
+    // ranges narrow within a warp. The order only assigns entries to threads.
+    auto key = [&](uint16_t e) {
+        const int l1 = e / (d2 * dn), l2 = (e / dn) % d2;
+        return ((l1 / 2) * 64 + l2 / 2) * 65536 + e;
+    };
+    std::stable_sort(out.begin(), out.end(), [&](uint16_t x, uint16_t y) { return key(x) < key(y); });
     return out;
 }
 
@@ -992,6 +1000,18 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
             fin_groups[gi].count = (int)m.size();
             fin_order.insert(fin_order.end(), m.begin(), m.end());
             FinalSmem &fs = fin_groups[gi].fs;
+            // W of the factored re-centring sum: ncart(lb) x rows x (components + 1) values per
+            // potential, rows as the kernel takes them from the group's V size
+            int need = 0;
+            for (int t : m) {
+                const int la = sh_L[ta[t]], lb = sh_L[tb[t]];
+                const bool so = b->grpp_n_so[b->centre_grpp[tc[t]]] > 0;
+                for (int ncomp = 1; ncomp <= (so ? 3 : 1); ncomp += 2) {
+                    const int rows = std::max(1, std::min(n_abc(la), fs.n_v / (n_abc(lb) * ncomp)));
+                    need = std::max(need, ncart(lb) * rows * (ncomp + 1));
+                }
+            }
+            fs.n_w = need;
             if (fin_smem_bytes(fs) > kFinSmemMax) fs.n_w = 0;  // term-by-term re-centring only
             CHECK_INPUT(fin_smem_bytes(fs) <= kFinSmemMax, "assembly tables of this batch exceed the shared memory of one block");
             fin_groups[gi].smem = fin_smem_bytes(fs);

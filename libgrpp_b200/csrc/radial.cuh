@@ -580,7 +580,7 @@ __device__ __forceinline__ void scr_parts_row(int n, double x, double *out)
     }
 }
 
-__global__ void __launch_bounds__(kScrUnitThreads, 8) radial_screen_unit_kernel(RadialArgs a)
+__global__ void __launch_bounds__(kScrUnitThreads, 10) radial_screen_unit_kernel(RadialArgs a)
 {
     extern __shared__ double ptab[];  // [kScrChunk][2][scr_lw]: Bessel parts, sides A and B
     __shared__ double t_aA[kScrChunk], t_aB[kScrChunk], t_eta[kScrChunk], t_p[kScrChunk], t_ip[kScrChunk],

@@ -73,24 +73,20 @@ def flagged_tasks(batch, z, rm_spread):
     return sorted(flag)
 
 
-def sub_elements(batch, idx):
-    off = batch.block_offsets()
-    return np.concatenate([np.arange(off[t], off[t + 1]) for t in idx]).astype(np.int64) if len(idx) else \
-        np.zeros(0, np.int64)
-
-
-def make_blocks(name, ref_lib, orc, nthreads):
+def make_blocks(name, ref_lib, orc, nthreads, keep_tasks=False):
     """Truth of the flagged tasks of a fixture (reusing the truth of tasks already on disk) and
-    libgrpp's distances from it."""
+    libgrpp's distances from it. keep_tasks: take the task selection on disk as it is."""
     batch, z = load_fixture(name)
     out = os.path.join(HERE, f"truth_{name}.npz")
-    obase = orc.driver_full_batch(batch, nthreads=nthreads)
-    rm = rounding_runs(orc, batch, nthreads)
-    rm_spread = [np.max([np.abs(r[m] - obase[m]) for r in rm], axis=0) for m in range(4)]
-    idx = flagged_tasks(batch, z, rm_spread)
     old = np.load(out) if os.path.exists(out) else None
     have = {int(t): k for k, t in enumerate(old["tasks"])} if old is not None else {}
-    idx = sorted(set(idx) | set(have))
+    if keep_tasks and old is not None:
+        idx = sorted(have)
+    else:
+        obase = orc.driver_full_batch(batch, nthreads=nthreads)
+        rm = rounding_runs(orc, batch, nthreads)
+        rm_spread = [np.max([np.abs(r[m] - obase[m]) for r in rm], axis=0) for m in range(4)]
+        idx = sorted(set(flagged_tasks(batch, z, rm_spread)) | set(have))
     if not idx:
         print(f"{name}: no task with an ill-conditioned element")
         if os.path.exists(out):
@@ -135,10 +131,9 @@ def make_blocks(name, ref_lib, orc, nthreads):
         p = ref_lib.driver_full_batch(perturbed(sub, mode), nthreads=nthreads)
         for m in range(4):
             refdev[m] = np.maximum(refdev[m], np.abs(p[m] - truth[m]))
-    el = sub_elements(batch, idx)
-    for r in rm:
+    for r in rounding_runs(orc, sub, nthreads):
         for m in range(4):
-            refdev[m] = np.maximum(refdev[m], np.abs(r[m][el] - truth[m]))
+            refdev[m] = np.maximum(refdev[m], np.abs(r[m] - truth[m]))
     data = dict(tasks=np.array(idx, dtype=np.int32), level=level, resid=resid)
     print(f"{name}: {len(idx)} tasks with an ill-conditioned element, deepest level {level.max()}")
     for m, c in enumerate(COMPS):
@@ -234,6 +229,7 @@ def main():
     ap.add_argument("--only", nargs="*")
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--refdev-only", action="store_true", help="config3: keep the truth on disk, recompute the distances")
+    ap.add_argument("--keep-tasks", action="store_true", help="keep each fixture's task selection on disk")
     args = ap.parse_args()
     ref = load_ref()
     if ref is None:
@@ -241,7 +237,7 @@ def main():
     orc = load_oracle()
     for name in ("config1", "config1_moderate", "config2", "h2o", "cs", "kcs", "tho", "uo2"):
         if not args.only or name in args.only:
-            make_blocks(name, ref, orc, args.threads or os.cpu_count())
+            make_blocks(name, ref, orc, args.threads or os.cpu_count(), args.keep_tasks)
     if not args.only or "config3" in args.only:
         make_gradient(args.threads or os.cpu_count(), args.refdev_only)
 
