@@ -22,7 +22,7 @@ SOURCES = ["engine.cu", "nofma.cu", "tables.cpp", "capi.cpp", "fortran_abi.cpp",
 # libgrpp is built without floating-point contraction; the angular sums round as its do
 EXTRA = {"nofma.cu": ["-fmad=false"]}
 HEADERS = ["grpp_common.cuh", "specfunc.cuh", "mmd.cuh", "radial.cuh", "angular.cuh", "level_model.cuh", "gradient.cuh", "tables.h",
-           "engine.h", "onee.cuh", "nucmodel.h", "nofma_launch.h"]
+           "engine.h", "onee.cuh", "nucmodel.h", "nofma_launch.h", "exp_rn.h"]
 
 
 def _newer(target, deps):

@@ -30,6 +30,7 @@
 
 #include "grpp_common.cuh"
 #include "specfunc.cuh"
+#include "exp_rn.h"
 
 namespace grpp {
 
@@ -1043,7 +1044,7 @@ __global__ void __launch_bounds__(kRadThreads) ftab_kernel(RadialArgs a, double 
 #pragma unroll 1
         for (int q = 0; q < np; q++) {
             const double x = a.rp_alpha[off + q];
-            const double e = a.rp_coef[off + q] * exp(-x * d2);
+            const double e = a.rp_coef[off + q] * exp_rn(-x * d2);
             if (e != 0.0) bessel_row_acc(lmax, (2.0 * x * CS) * r, e, cf + tid, kRadRow);
         }
         double *dst = ftab + a.fp_off[pr] + f;
@@ -1075,7 +1076,7 @@ __global__ void wu_table_kernel(RadialArgs a, int n_grpps, double *wu)
         double u = 0.0;
         for (int k = 0; k < a.pot_nprim[pot]; k++) {
             const int o = a.pot_prim_off[pot] + k;
-            const double ex = exp(-a.pot_alpha[o] * r2);
+            const double ex = exp_rn(-a.pot_alpha[o] * r2);
             if (ex == 0.0) continue;  // the term adds an exact zero
             const double rp = grid_rpow_m2(f, a.pot_powers[o], ir, ir2);  // r^(n-2)
             u += a.pot_coef[o] * rp * ex;
@@ -1181,7 +1182,7 @@ __global__ void __launch_bounds__(kRadThreads, 5) radial_walk_kernel(RadialArgs 
                     double u = 0.0;
                     for (int k = 0; k < sh.pn[pp]; k++) {
                         const int tk = sh.poff[pp] + k;
-                        const double ex = exp(-sh.talpha[tk] * r2);
+                        const double ex = exp_rn(-sh.talpha[tk] * r2);
                         if (ex == 0.0) continue;  // the term adds an exact zero
                         const double rp = grid_rpow_m2(f0 + tid, sh.tpow[tk], ir, ir2);  // r^(n-2)
                         u += sh.tcoef[tk] * rp * ex;
@@ -1201,14 +1202,14 @@ __global__ void __launch_bounds__(kRadThreads, 5) radial_walk_kernel(RadialArgs 
                 if (!a.ftab && u1 >= 0) {
 #pragma unroll 1
                     for (int q = 0; q < np_a; q++) {
-                        const double e = sh.ca[q] * exp(-sh.xa[q] * dA2);
+                        const double e = sh.ca[q] * exp_rn(-sh.xa[q] * dA2);
                         if (e != 0.0) bessel_row_acc(u1, sh.ka[q] * r, e, cf1 + tid, kRadRow);
                     }
                 }
                 if (!a.ftab && u2 >= 0) {
 #pragma unroll 1
                     for (int q = 0; q < np_b; q++) {
-                        const double e = sh.cb[q] * exp(-sh.xb[q] * dB2);
+                        const double e = sh.cb[q] * exp_rn(-sh.xb[q] * dB2);
                         if (e != 0.0) bessel_row_acc(u2, sh.kb[q] * r, e, cf2 + tid, kRadRow);
                     }
                 }

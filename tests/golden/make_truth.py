@@ -147,6 +147,27 @@ def make_blocks(name, ref_lib, orc, nthreads, keep_tasks=False):
     print(f"  -> {os.path.relpath(out, ROOT)} ({os.path.getsize(out) / 1e3:.0f} kB)")
 
 
+def add_rounding(name, orc, nthreads):
+    """Widen refdev of the truth on disk by the oracle's rounding-model runs on the same tasks
+    (the truth and the earlier distances are kept)."""
+    batch, z = load_fixture(name)
+    out = os.path.join(HERE, f"truth_{name}.npz")
+    old = np.load(out)
+    data = {k: old[k] for k in old.files}
+    if name == "config3":
+        S = system_from_fixture(z)
+        for r in rounding_runs(orc, batch, nthreads, grad=(S, z["D"])):
+            data["refdev_grad"] = np.maximum(data["refdev_grad"], np.abs(r - data["truth_grad"]))
+        print(f"config3: max refdev {data['refdev_grad'].max():.2e}")
+    else:
+        sub, _, _ = fixture_subset(batch, z, [int(t) for t in old["tasks"]])
+        for r in rounding_runs(orc, sub, nthreads):
+            for m, c in enumerate(COMPS):
+                data["refdev_" + c] = np.maximum(data["refdev_" + c], np.abs(r[m] - data["truth_" + c]))
+        print(f"{name}: " + ", ".join(f"{c} max refdev {data['refdev_' + c].max():.2e}" for c in COMPS))
+    np.savez_compressed(out, **data)
+
+
 # ---------------------------------------------------------------- gradient
 
 def truth_gradient(system, batch, D, nthreads):
@@ -230,11 +251,17 @@ def main():
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--refdev-only", action="store_true", help="config3: keep the truth on disk, recompute the distances")
     ap.add_argument("--keep-tasks", action="store_true", help="keep each fixture's task selection on disk")
+    ap.add_argument("--add-rounding", action="store_true",
+                    help="keep the truth files on disk and widen their refdev by the oracle's rounding-model runs")
     args = ap.parse_args()
     ref = load_ref()
     if ref is None:
         raise SystemExit("oracle/_ref/libgrpp_ref.so is not built (make -C oracle ref)")
     orc = load_oracle()
+    if args.add_rounding:
+        for name in args.only or ("config1", "config1_moderate", "config2", "config3"):
+            add_rounding(name, orc, args.threads or os.cpu_count())
+        return
     for name in ("config1", "config1_moderate", "config2", "h2o", "cs", "kcs", "tho", "uo2"):
         if not args.only or name in args.only:
             make_blocks(name, ref, orc, args.threads or os.cpu_count(), args.keep_tasks)

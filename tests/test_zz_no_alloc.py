@@ -1,13 +1,13 @@
 """The allocation-free entry point libgrpp_b200_type2_batch_noalloc.
 
-It exists for callers that must not trigger device allocations (code inside
-CUDA graph capture, processes whose device memory belongs to a pool or a
-framework allocator, services with a fixed device footprint): all its device
-data sit in static device arrays, with a 32 MiB scratch array shared by all
-calls. Its output must equal the arep blocks of the regular batched entry
-point (libgrpp_b200_full_grpp_batch) for GRPPs made of averaged (AREP)
-potentials only, call after call, even though the scratch array keeps the
-previous call's contents.
+It exists for callers that must not trigger device allocations (processes whose
+device memory belongs to a pool or a framework allocator, services with a fixed
+device footprint): all its device data sit in static device arrays, with a
+32 MiB scratch array shared by all calls. Its output must equal the arep blocks
+of the regular batched entry point (libgrpp_b200_full_grpp_batch) for GRPPs
+made of averaged (AREP) potentials only, call after call, even though the
+scratch array keeps the previous call's contents, and the oracle's on the same
+tasks.
 
 This file is collected last, so that a run stopping at the first failure has
 already run every other test; it also passes alone in a fresh process.
@@ -58,6 +58,27 @@ def test_noalloc_matches_batched_entry_point(gpu_lib):
             ok, ab, rel, _ = parity(got, want)
             assert ok, (ab, rel)
         assert np.array_equal(first, second)
+
+
+def test_noalloc_mixed_batch_against_oracle(gpu_lib, oracle_lib):
+    """One-centre tasks (both shells on the potential's atom) and a centre whose GRPP has no
+    AREP potential (its blocks are zero) in one batch, against the batched entry point element
+    by element and against the oracle at the tolerance of record."""
+    from libgrpp_b200.system import GRPP
+    S = _arep_only(_moderate_system())
+    S.grpps.append(GRPP())
+    S.centres.append((np.array([0.6, -1.3, 2.0]), len(S.grpps) - 1))
+    batch = S.batch()
+    want = gpu_lib.full_grpp_batch(batch)[0]
+    got = gpu_lib.type2_batch_noalloc(batch)
+    ok, ab, rel, _ = parity(got, want)
+    assert ok, (ab, rel)
+    ref = oracle_lib.driver_full_batch(batch, nthreads=8)[0]
+    ok, ab, rel, _ = parity(got, ref)
+    assert ok, (ab, rel)
+    off = batch.block_offsets()
+    empty = [t for t in range(len(batch.task_c)) if batch.task_c[t] == len(S.centres) - 1]
+    assert empty and all(np.all(got[off[t]:off[t + 1]] == 0.0) for t in empty)
 
 
 def test_noalloc_rejects_oversized_batch(gpu_lib):

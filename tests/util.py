@@ -173,7 +173,7 @@ REFDEV_MODES = (1, 2) + tuple(range(3, 31))
 # seeds of the oracle's rounding model (orc_set_rounding_model in oracle/orc_integrals.c): runs of
 # libgrpp's algorithm whose transcendental results and Bessel values differ from libgrpp's in the
 # last bit, as any other implementation's (a GPU's exp, regenerated tables) do
-ROUNDING_SEEDS = tuple(range(1, 7))
+ROUNDING_SEEDS = tuple(range(1, 13))
 
 
 def rounding_runs(oracle, batch: BatchArrays, nthreads=0, seeds=ROUNDING_SEEDS, grad=None):
