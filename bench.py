@@ -436,9 +436,10 @@ def run_ours(args, rank, world, local):
 
 # DRAM bytes per task of the dominant kernel, from one ncu capture of it (dram__bytes_read.sum +
 # dram__bytes_write.sum over the captured launch / its tasks); see profiles/
-TRAFFIC_PER_TASK = {"ms_screen": (19.929856e6 + 19.016704e6) / 4096}
-TRAFFIC_SOURCE = ("ncu --set full of radial_screen_flat_kernel on 4096 tasks of the first config-1 step: 38.95 MB "
-                  "DRAM read+write, scaled to the step's tasks (profiles/screen_kernel_full_4096tasks.md)")
+TRAFFIC_PER_TASK = {"ms_screen": (15.772672e6 + 14.599936e6) / 4096}
+TRAFFIC_SOURCE = ("ncu --set full of radial_screen_unit_kernel (the screening of the long runs, about 85% of the "
+                  "screening time) on 4096 tasks of the first config-1 step: 30.37 MB DRAM read+write, scaled to "
+                  "the step's tasks (profiles/screen_unit_kernel_full_4096tasks.md)")
 
 # FLOP model of the radial path (count of FP64 add/mul, FMA = 2, each exp/pow/sqrt/log/erf = 1,
 # per operation of libgrpp's algorithm, libgrpp/radial_type2_integral.c and screening.c):

@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(kRadThreads, GRPP_SCR_MINB) radial_screen_flat
 // expressions, operands and order as the flat kernel, so the estimates and gate decisions are
 // the same.
 constexpr int kScrUnitThreads = 64;  // threads per block = entries per run at most
-constexpr int kScrUnitMin = 16;      // runs with fewer entries stay in the flat kernel
+constexpr int kScrUnitMin = 32;      // runs with fewer entries stay in the flat kernel
 constexpr int kScrChunk = 64;        // primitive triples staged per round (one per thread)
 static_assert(kScrChunk == kScrUnitThreads, "one staged triple per thread");
 
