@@ -22,6 +22,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "grpp_common.cuh"
@@ -732,10 +733,11 @@ int plan_build(DeviceState &st, const libgrpp_b200_batch_t *b, const RunOptions 
     std::vector<int> rad_task;
     std::vector<int64_t> rad_qoff, rad_uoff;
     // (shell, centre) pairs of the radial items, for the F_l(r) tables (ftab_kernel)
-    // pair index per (shell, centre): a flat array when it is small, else a map
+    // pair index per (shell, centre): a flat array when it is small next to the chunk (filling
+    // it costs n_shells x n_centres per chunk), else a hash map
     const int64_t n_sc = (int64_t)b->n_shells * b->n_centres;
-    std::vector<int> fpair_flat(n_sc <= (int64_t(1) << 24) ? n_sc : 0, -1);
-    std::map<int64_t, int> fpair_of;
+    std::vector<int> fpair_flat(n_sc <= std::max<int64_t>(8 * nt, 4096) ? n_sc : 0, -1);
+    std::unordered_map<int64_t, int> fpair_of;
     std::vector<int> fp_shell, fp_centre, fp_lmax, item_fa, item_fb;
     std::vector<int> task_fpa(nt, -1), task_fpb(nt, -1);
     auto fpair = [&](int shell, int centre, int lmax) {
