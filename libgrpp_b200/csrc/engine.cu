@@ -107,6 +107,7 @@ struct PinBuf {
 // prepares and uploads chunk c+1 and downloads chunk c-1 while the GPU runs chunk c.
 struct DeviceState {
     int device = -1;
+    int nsm = 148;                       // multiprocessors of the device (set at initialisation)
     bool ready = false;
     cudaStream_t stream = nullptr;       // all kernels and uploads
     cudaStream_t copy_stream = nullptr;  // downloads of finished chunks
@@ -195,6 +196,7 @@ int init_device_state(DeviceState &st, int device)
     GRPP_CUDA(cudaFuncSetAttribute(type1_num_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(t1_smem_doubles(kT1MaxLam) * sizeof(double))));
     GRPP_CUDA(cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_train_smem_bytes()));
+    GRPP_CUDA(cudaDeviceGetAttribute(&st.nsm, cudaDevAttrMultiProcessorCount, device));
     st.device = device;
     st.ready = true;
     return 0;
@@ -1442,7 +1444,7 @@ int plan_launch(Plan &P)
             // predict every walked task's level, order deepest first, walk from the queue
             GRPP_CUDA(cudaMemsetAsync(P.lm_ctl, 0, 16 * sizeof(int), s));
             LevelModelDev lm{st.lm_norm, st.lm_w};
-            const int pblocks = (int)std::min<int64_t>((P.n_radial + 3) / 4, 148 * 16);
+            const int pblocks = (int)std::min<int64_t>((P.n_radial + 3) / 4, (int64_t)st.nsm * 16);
             level_predict_kernel<<<pblocks, 128, 0, s>>>(P.rad, lm, P.pred_level);
             GRPP_CUDA(cudaGetLastError());
             level_order_kernel<<<1, 256, 0, s>>>((int)P.n_radial, P.pred_level, P.order, P.lm_ctl, P.lm_ctl + 2);
@@ -1954,7 +1956,7 @@ int mlp_predict(const float *params, const float *X, int64_t n, int8_t *pred)
     int8_t *pd = nullptr;
     GRPP_CUDA(cudaMalloc(&pd, (size_t)n));
     LevelModelDev lm{d.norm, d.wb};
-    mlp_predict_kernel<<<(int)std::min<int64_t>((n + 3) / 4, 148 * 16), 128, 0, s>>>(lm, d.X, (int)n, pd);
+    mlp_predict_kernel<<<(int)std::min<int64_t>((n + 3) / 4, (int64_t)stp->nsm * 16), 128, 0, s>>>(lm, d.X, (int)n, pd);
     GRPP_CUDA(cudaGetLastError());
     GRPP_CUDA(cudaMemcpyAsync(pred, pd, (size_t)n, cudaMemcpyDeviceToHost, s));
     GRPP_CUDA(cudaStreamSynchronize(s));
@@ -2008,7 +2010,7 @@ int run_grad_contract(const libgrpp_b200_batch_t *sub, const RunOptions &opt, co
     ga.D = Dd;
     ga.n_bf = n_bf;
     ga.g = gd;
-    grad_contract_kernel<<<(int)std::min<int64_t>((n_tasks + 3) / 4, 148 * 32), 128, 0, s>>>(ga);
+    grad_contract_kernel<<<(int)std::min<int64_t>((n_tasks + 3) / 4, (int64_t)stp->nsm * 32), 128, 0, s>>>(ga);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(out24, gd, (size_t)n_tasks * 24 * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -2146,7 +2148,7 @@ int run_onee_batch(const libgrpp_b200_batch_t *b, int kind, double *h0, double *
     a.out0 = u.at<double>(oout);
     a.out1 = a.out0 + nout;
     a.out2 = a.out1 + nout;
-    const int blocks = (int)std::min<int64_t>((nt + kOneeWarps - 1) / kOneeWarps, 148 * 16);
+    const int blocks = (int)std::min<int64_t>((nt + kOneeWarps - 1) / kOneeWarps, (int64_t)stp->nsm * 16);
     onee_os_kernel<<<blocks, 32 * kOneeWarps, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
     double *hs[3] = {h0, h1, h2};
@@ -2248,7 +2250,7 @@ int run_type1_numeric_batch(const libgrpp_b200_batch_t *b, int model, const doub
     a.pair_skip = pair_skip;
     a.out = u.at<double>(oout);
     const size_t smem = (size_t)t1_smem_doubles(Lt) * sizeof(double);
-    type1_num_kernel<<<(int)std::min<int64_t>(nt, 148 * 8), kT1Threads, smem, s>>>(a);
+    type1_num_kernel<<<(int)std::min<int64_t>(nt, (int64_t)stp->nsm * 8), kT1Threads, smem, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_out, a.out, nout * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
