@@ -36,7 +36,7 @@ namespace grpp {
 
 constexpr int kRadThreads = 128;
 #ifndef GRPP_SCR_MINB
-#define GRPP_SCR_MINB 6  // resident 128-thread blocks per SM asked of the flat screening kernel
+#define GRPP_SCR_MINB 5  // resident 128-thread blocks per SM asked of the flat screening kernel
 #endif
 constexpr int kRadMaxPrims = 64;     // primitives per shell on the radial path
 constexpr int kRadMaxPots = 24;      // semilocal potentials per centre
